@@ -1,0 +1,95 @@
+"""ctypes binding of the C-ABI library ``_lib/libebsd_b200.so``.
+
+Every function declared in ``include/ebsd_b200.h`` is bound here with its
+exact argument types. ``call(name, *args)`` raises ``ValueError`` for argument
+errors (status > 0) and ``RuntimeError`` for CUDA errors (status < 0), with
+the library's own message. There is no fallback: if the library is missing,
+importing the package's GPU entry points fails loudly.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libebsd_b200.so")
+
+vp, i32, i64, f32, sz = C.c_void_p, C.c_int, C.c_int64, C.c_float, C.c_size_t
+
+# name -> (restype, argtypes); mirrors include/ebsd_b200.h
+SIGNATURES = {
+    "ebsd_version": (i32, []),
+    "ebsd_last_error": (i32, [C.c_char_p, sz]),
+    "ebsd_device_check": (i32, [i32]),
+    "ebsd_grid_workspace_bytes": (sz, [i32]),
+    "ebsd_grid_fz_count": (i32, [i32, i32, vp, sz, vp, vp]),
+    "ebsd_grid_fz_write": (i32, [i32, i32, vp, sz, vp, vp, vp]),
+    "ebsd_gather_rows": (i32, [vp, i64, i32, vp, i64, vp, vp]),
+    "ebsd_project_dictionary": (i32, [vp, i32, i32, vp, i32, vp, i64, i32, vp, i64, vp, i32, i64, vp, vp, vp]),
+    "ebsd_prep_patterns": (i32, [vp, i64, i32, i32, i64, i32, vp, i32, i32, vp, i64, vp, i32, i64, vp, vp, vp]),
+    "ebsd_sample_master_pattern": (i32, [vp, i32, i32, vp, i64, i32, vp, vp]),
+    "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
+    "ebsd_match_auto_splits": (i32, [i64, i64]),
+    "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
+    "ebsd_merge_rescore": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
+                                 vp, vp, vp, vp, vp]),
+    "ebsd_gemm_nt": (i32, [vp, i64, vp, i64, i64, i32, f32, i32, vp, i64, i64, i64, vp, vp]),
+    "ebsd_col_mean": (i32, [vp, i64, i32, i64, vp, vp]),
+    "ebsd_split3_bf16": (i32, [vp, i64, i32, i64, vp, i32, i32, vp, i64, i64, vp]),
+    "ebsd_disori_angle": (i32, [vp, vp, i64, i32, vp, vp]),
+}
+
+DT_F32, DT_BF16, DT_E4M3 = 0, 1, 2
+SIM_DOT, SIM_COSINE = 0, 1
+DEVICE_TIMEOUT = 0x7001
+
+_lib = None
+_lock = threading.Lock()
+
+
+def load() -> C.CDLL:
+    """Load (once) and return the library; raises ImportError if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} not found: build it with `python -m ebsdtorch_b200.build` "
+                    "(CUDA toolkit with sm_100a support required)"
+                )
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def last_error() -> str:
+    lib = load()
+    buf = C.create_string_buffer(2048)
+    lib.ebsd_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def call(name: str, *args) -> int:
+    """Call an int-status entry point; raise on failure."""
+    fn = getattr(load(), name)
+    rc = fn(*args)
+    if rc > 0:
+        raise ValueError(f"{name}: {last_error()}")
+    if rc < 0:
+        raise RuntimeError(f"{name}: {last_error()} (cudaError {-rc})")
+    return rc
+
+
+def ptr(t) -> int | None:
+    """Device pointer of a tensor, or None for a missing optional buffer."""
+    if t is None:
+        return None
+    return t.data_ptr()

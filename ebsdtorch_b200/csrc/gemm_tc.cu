@@ -1,0 +1,525 @@
+// K3: pattern x dictionary contraction on the 5th-generation tensor cores
+// (tcgen05) with a fused streaming top-k epilogue, and the same main loop
+// with a plain FP32 store epilogue (PCA covariance and projections).
+//
+// Replaces knn_batch (ebsdtorch/utils/knn.py:80-103: `query @ data.t()` then
+// torch.topk) and the ChunkedKNN running merge (knn.py:219-266); the store
+// variant replaces the einsum in update_covmat (pca_covmat.py:53-91) and the
+// PCA projections (indexing.py:401, 421, 452).
+//
+// Structure (one CTA per SM, 192 threads):
+//   warp 0      TMA producer: A tile (128 rows x 128 B) and B tile
+//               (256 rows x 128 B) per stage, 128-byte swizzle, 4 stages.
+//   warp 1      allocates 512 TMEM columns (two 128x256 FP32 accumulators)
+//               and issues tcgen05.mma (M=128, N=256, 32 B of K each).
+//   warps 2-5   epilogue: tcgen05.ld of the accumulator rows; each thread
+//               owns one query row and keeps its best candidates sorted in
+//               registers across all dictionary tiles of its range.
+// A unit of work is (query tile, dictionary range); the epilogue of tile t
+// overlaps the MMAs of tile t+1 through the second accumulator.
+// Every wait is bounded (common.cuh); a timeout is reported in *status.
+#include <algorithm>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace ebsd {
+
+constexpr int BM = 128;
+constexpr int BN = 256;
+constexpr int BKB = 128;  // bytes of K per stage and row (one 128-byte swizzle atom)
+constexpr int STAGES = 4;
+constexpr int A_BYTES = BM * BKB;
+constexpr int B_BYTES = BN * BKB;
+constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+constexpr int EPI_THREADS = 128;
+constexpr int THREADS = 64 + EPI_THREADS;
+constexpr int SCRATCH_BYTES = 32 * EPI_THREADS * 4;
+constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 1) + 16;
+constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + BAR_BYTES;
+constexpr uint32_t TMEM_COLS = 2 * BN;
+
+static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+
+struct GemmParams {
+  int n_tiles;
+  int splits;
+  int k_iters;
+  int64_t n_valid;
+  const float* col_scale;
+  float* part_val;
+  int32_t* part_idx;
+  int part_slots;
+  int slot_base;
+  int32_t index_base;
+  float* C;
+  int64_t ldc;
+  int64_t m_valid;
+  float alpha;
+  int accumulate;
+  int* status;
+};
+
+template <int KIND>
+__host__ __device__ constexpr uint32_t make_idesc() {
+  // c_format F32 (bit 4); a/b format bits 7-9 / 10-12 (kind::f16: 1 = BF16;
+  // kind::f8f6f4: 0 = E4M3); K-major A and B; N >> 3 at bit 17; M >> 4 at bit 24.
+  return (1u << 4) | (KIND == 0 ? ((1u << 7) | (1u << 10)) : 0u) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+
+template <int KC>
+__device__ __forceinline__ void topk_insert(float (&bv)[KC], int (&bi)[KC], float v, int idx) {
+  bv[KC - 1] = v;
+  bi[KC - 1] = idx;
+#pragma unroll
+  for (int j = KC - 1; j > 0; --j) {
+    const bool sw = bv[j] > bv[j - 1];
+    const float a = bv[j], b = bv[j - 1];
+    const int ia = bi[j], ib = bi[j - 1];
+    bv[j - 1] = sw ? a : b;
+    bv[j] = sw ? b : a;
+    bi[j - 1] = sw ? ia : ib;
+    bi[j] = sw ? ib : ia;
+  }
+}
+
+__device__ __forceinline__ void report_timeout(const GemmParams& p, volatile int* abort_flag) {
+  *abort_flag = 1;
+  atomicExch(p.status, EBSD_DEVICE_TIMEOUT);
+}
+
+// MODE 0: top-k epilogue. MODE 1: store epilogue.
+template <int KIND, int MODE, int KC>
+__global__ void __launch_bounds__(THREADS, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+              const GemmParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_s = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
+  const uint32_t sbase = smem_u32(smem);
+  float* scratch = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+  auto accf_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
+  auto acce_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
+  const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m_tile = blockIdx.x / p.splits;
+  const int split = blockIdx.x - m_tile * p.splits;
+  const int n_begin = (int)((int64_t)split * p.n_tiles / p.splits);
+  const int n_end = (int)((int64_t)(split + 1) * p.n_tiles / p.splits);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(accf_bar(a), 1);
+      mbar_init(acce_bar(a), EPI_THREADS);
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      int64_t issued = 0;
+      bool ok = true;
+      const int a_row = m_tile * BM;
+      for (int n = n_begin; n < n_end && ok; ++n) {
+        for (int k = 0; k < p.k_iters; ++k) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+            ok = false;
+            break;
+          }
+          const uint32_t a_dst = sbase + stage * STAGE_BYTES;
+          mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
+          const int kx = k * (KIND == 0 ? BKB / 2 : BKB);  // element coordinate
+          tma_load_2d(a_dst, &tmA, kx, a_row, full_bar(stage));
+          tma_load_2d(a_dst + A_BYTES, &tmB, kx, n * BN, full_bar(stage));
+          ++issued;
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (!ok) {
+        report_timeout(p, abort_flag);
+        // let the copies already in flight land before the CTA exits
+        const int64_t inflight = issued < STAGES ? issued : (int64_t)STAGES;
+        uint32_t s = stage, ph = phase;
+        for (int64_t i = 0; i < inflight; ++i) {
+          if (s == 0) {
+            s = STAGES - 1;
+            ph ^= 1u;
+          } else {
+            --s;
+          }
+          volatile int never = 0;
+          mbar_wait(full_bar(s), ph, &never);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      int acc = 0;
+      uint32_t acc_phase = 0;
+      bool ok = true, any = false;
+      constexpr uint32_t idesc = make_idesc<KIND>();
+      for (int n = n_begin; n < n_end && ok; ++n) {
+        if (!mbar_wait(acce_bar(acc), acc_phase ^ 1u, abort_flag)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+        for (int k = 0; k < p.k_iters; ++k) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_addr = sbase + stage * STAGE_BYTES;
+          const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BKB / 32; ++kk) {
+            tc_mma<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32),
+                         idesc, (k | kk) != 0 ? 1u : 0u);
+          }
+          any = true;
+          tc_commit(empty_bar(stage));
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        tc_commit(accf_bar(acc));
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1u;
+        }
+      }
+      if (!ok) {
+        report_timeout(p, abort_flag);
+        if (any) {
+          // wait for the MMAs already issued before TMEM is released
+          tc_commit(drain_bar);
+          volatile int never = 0;
+          mbar_wait(drain_bar, 0, &never);
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue ----------------
+    const int wq = warp & 3;              // TMEM lane quarter this warp may access
+    const int etid = threadIdx.x - 64;    // 0..127, scratch column
+    const int row = wq * 32 + lane;       // row of the 128-row tile
+    const uint32_t lane_addr = (uint32_t)(wq * 32) << 16;
+    float bv[KC];
+    int bi[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      bv[j] = -INFINITY;
+      bi[j] = -1;
+    }
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    for (int n = n_begin; n < n_end; ++n) {
+      bool got = mbar_wait(accf_bar(acc), acc_phase, abort_flag);
+      got = __all_sync(0xffffffffu, got);
+      if (!got) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t tile_col = (int64_t)n * BN;
+#pragma unroll 1
+      for (int c = 0; c < BN / 32; ++c) {
+        __syncwarp();
+        float v[32];
+        tmem_ld32(tmem_base + lane_addr + (uint32_t)(acc * BN + c * 32), v);
+        const int64_t col0 = tile_col + c * 32;
+        if constexpr (MODE == 0) {
+          uint32_t mask = 0;
+          const float thr = bv[KC - 1];
+          if (col0 + 32 <= p.n_valid) {
+            if (p.col_scale) {
+              const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
+#pragma unroll
+              for (int j4 = 0; j4 < 8; ++j4) {
+                const float4 s4 = __ldg(cs + j4);
+                v[4 * j4 + 0] *= s4.x;
+                v[4 * j4 + 1] *= s4.y;
+                v[4 * j4 + 2] *= s4.z;
+                v[4 * j4 + 3] *= s4.w;
+              }
+            }
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const bool valid = col0 + j < p.n_valid;
+              const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
+              v[j] = valid ? v[j] * sc : -INFINITY;
+            }
+          }
+#pragma unroll
+          for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
+          if (mask) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) scratch[j * EPI_THREADS + etid] = v[j];
+            while (mask) {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1u;
+              const float sc = scratch[j * EPI_THREADS + etid];
+              if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
+            }
+          }
+        } else {
+          const int64_t grow = (int64_t)m_tile * BM + row;
+          if (grow < p.m_valid) {
+            float* dst = p.C + grow * p.ldc;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int64_t col = col0 + j;
+              if (col < p.n_valid) {
+                const float r = p.alpha * v[j];
+                dst[col] = p.accumulate ? dst[col] + r : r;
+              }
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acce_bar(acc));
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1u;
+      }
+    }
+    if (!ok) {
+      if (lane == 0) report_timeout(p, abort_flag);
+    } else if constexpr (MODE == 0) {
+      const int64_t q = (int64_t)m_tile * BM + row;
+      const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        p.part_val[base + j] = bv[j];
+        p.part_idx[base + j] = bi[j];
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(ptr);
+  });
+  return fn;
+}
+
+static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t rows, int64_t k_pad,
+                     int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable from the CUDA driver");
+    return EBSD_ERR_UNSUPPORTED;
+  }
+  const int esz = lp_dtype == EBSD_DT_BF16 ? 2 : 1;
+  cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(k_pad * esz)};
+  cuuint32_t box[2] = {(cuuint32_t)(BKB / esz), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map,
+                   lp_dtype == EBSD_DT_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16
+                                            : CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                   2, const_cast<void*>(ptr), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (CUresult %d) for rows=%lld k=%lld", (int)r,
+              (long long)rows, (long long)k_pad);
+    return EBSD_ERR_ARG;
+  }
+  return 0;
+}
+
+template <int KIND, int MODE, int KC>
+static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
+                  cudaStream_t s) {
+  auto kern = k_tc_gemm<KIND, MODE, KC>;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, b, p);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int KIND>
+static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
+                       int grid, cudaStream_t s) {
+  switch (kc) {
+    case 1: return launch<KIND, 0, 1>(a, b, p, grid, s);
+    case 2: return launch<KIND, 0, 2>(a, b, p, grid, s);
+    case 4: return launch<KIND, 0, 4>(a, b, p, grid, s);
+    case 8: return launch<KIND, 0, 8>(a, b, p, grid, s);
+    case 16: return launch<KIND, 0, 16>(a, b, p, grid, s);
+    case 32: return launch<KIND, 0, 32>(a, b, p, grid, s);
+    case 64: return launch<KIND, 0, 64>(a, b, p, grid, s);
+  }
+  set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
+  return EBSD_ERR_ARG;
+}
+
+static int check_operands(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
+                          int lp_dtype, int* status) {
+  EBSD_ARG_CHECK(A && B && status, "null operand or status pointer");
+  EBSD_ARG_CHECK(lp_dtype == EBSD_DT_BF16 || lp_dtype == EBSD_DT_E4M3,
+                 "lp_dtype must be EBSD_DT_BF16 or EBSD_DT_E4M3");
+  const int kmul = lp_dtype == EBSD_DT_BF16 ? 64 : 128;
+  EBSD_ARG_CHECK(k_pad > 0 && k_pad % kmul == 0, "k_pad %lld must be a positive multiple of %d",
+                 (long long)k_pad, kmul);
+  EBSD_ARG_CHECK(m_pad > 0 && m_pad % BM == 0, "row count %lld must be a positive multiple of %d",
+                 (long long)m_pad, BM);
+  EBSD_ARG_CHECK(n_pad > 0 && n_pad % BN == 0, "row count %lld must be a positive multiple of %d",
+                 (long long)n_pad, BN);
+  EBSD_ARG_CHECK(((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0,
+                 "operands must be 16-byte aligned");
+  EBSD_ARG_CHECK(m_pad / BM < (1 << 20) && n_pad / BN < (1 << 22), "operand too large");
+  return 0;
+}
+
+}  // namespace ebsd
+
+using namespace ebsd;
+
+extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
+  const int m_tiles = (int)std::max<int64_t>(1, n_queries_pad / BM);
+  const int n_tiles = (int)std::max<int64_t>(1, n_dict_pad / BN);
+  const int sms = device_sm_count();
+  // Enough units for ~4 waves, and at least 8 dictionary ranges when the
+  // query side is large, so concurrently running units share B tiles in L2.
+  int splits = (int)((4LL * sms + m_tiles - 1) / m_tiles);
+  splits = std::max(splits, 8);
+  splits = std::min(splits, n_tiles);
+  return std::max(splits, 1);
+}
+
+extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
+                               int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad,
+                               int lp_dtype, const float* col_scale, int n_cand, int splits,
+                               float* part_val, int32_t* part_idx, int part_slots, int slot_base,
+                               int32_t index_base, int* d_status, void* stream) {
+  if (int rc = check_operands(queries_lp, n_queries_pad, dict_lp, n_dict_pad, k_pad, lp_dtype,
+                              d_status))
+    return rc;
+  EBSD_ARG_CHECK(part_val && part_idx, "null partial-result buffers");
+  EBSD_ARG_CHECK(n_dict_valid > 0 && n_dict_valid <= n_dict_pad, "n_dict_valid out of range");
+  EBSD_ARG_CHECK((int64_t)index_base + n_dict_valid <= INT32_MAX, "dictionary index overflow");
+  EBSD_ARG_CHECK(!col_scale || ((uintptr_t)col_scale & 15) == 0, "col_scale must be 16-byte aligned");
+  const int n_tiles = (int)(n_dict_pad / BN);
+  if (splits <= 0) splits = ebsd_match_auto_splits(n_queries_pad, n_dict_pad);
+  EBSD_ARG_CHECK(splits <= n_tiles, "splits (%d) > dictionary tiles (%d)", splits, n_tiles);
+  EBSD_ARG_CHECK(slot_base >= 0 && slot_base + splits <= part_slots,
+                 "part_slots (%d) < slot_base (%d) + splits (%d)", part_slots, slot_base, splits);
+  const int64_t m_tiles = n_queries_pad / BM;
+  EBSD_ARG_CHECK(m_tiles * splits < INT32_MAX, "too many work units");
+  CUtensorMap ta, tb;
+  if (int rc = make_tmap(&ta, queries_lp, lp_dtype, n_queries_pad, k_pad, BM)) return rc;
+  if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, BN)) return rc;
+  GemmParams p{};
+  p.n_tiles = n_tiles;
+  p.splits = splits;
+  p.k_iters = (int)(k_pad * (lp_dtype == EBSD_DT_BF16 ? 2 : 1) / BKB);
+  p.n_valid = n_dict_valid;
+  p.col_scale = col_scale;
+  p.part_val = part_val;
+  p.part_idx = part_idx;
+  p.part_slots = part_slots;
+  p.slot_base = slot_base;
+  p.index_base = index_base;
+  p.status = d_status;
+  const int grid = (int)(m_tiles * splits);
+  cudaStream_t s = as_stream(stream);
+  return lp_dtype == EBSD_DT_BF16 ? launch_topk<0>(n_cand, ta, tb, p, grid, s)
+                                  : launch_topk<1>(n_cand, ta, tb, p, grid, s);
+}
+
+extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad,
+                            int64_t k_pad, int lp_dtype, float alpha, int accumulate, float* C,
+                            int64_t ldc, int64_t m_valid, int64_t n_valid, int* d_status,
+                            void* stream) {
+  if (int rc = check_operands(A, m_pad, B, n_pad, k_pad, lp_dtype, d_status)) return rc;
+  EBSD_ARG_CHECK(C != nullptr, "null output");
+  EBSD_ARG_CHECK(m_valid > 0 && m_valid <= m_pad && n_valid > 0 && n_valid <= n_pad,
+                 "valid extents out of range");
+  EBSD_ARG_CHECK(ldc >= n_valid, "ldc < n_valid");
+  CUtensorMap ta, tb;
+  if (int rc = make_tmap(&ta, A, lp_dtype, m_pad, k_pad, BM)) return rc;
+  if (int rc = make_tmap(&tb, B, lp_dtype, n_pad, k_pad, BN)) return rc;
+  GemmParams p{};
+  p.n_tiles = (int)(n_pad / BN);
+  // one dictionary tile per unit keeps all SMs busy for small outputs
+  p.splits = p.n_tiles;
+  p.k_iters = (int)(k_pad * (lp_dtype == EBSD_DT_BF16 ? 2 : 1) / BKB);
+  p.n_valid = n_valid;
+  p.C = C;
+  p.ldc = ldc;
+  p.m_valid = m_valid;
+  p.alpha = alpha;
+  p.accumulate = accumulate;
+  p.status = d_status;
+  const int64_t m_tiles = m_pad / BM;
+  EBSD_ARG_CHECK(m_tiles * p.splits < INT32_MAX, "too many work units");
+  const int grid = (int)(m_tiles * p.splits);
+  cudaStream_t s = as_stream(stream);
+  return lp_dtype == EBSD_DT_BF16 ? launch<0, 1, 1>(ta, tb, p, grid, s)
+                                  : launch<1, 1, 1>(ta, tb, p, grid, s);
+}

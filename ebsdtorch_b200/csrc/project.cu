@@ -1,0 +1,285 @@
+// K1: dictionary projector and K2: pattern preparation.
+//
+// K1 follows ebsdtorch/ebsd/indexing.py:117-143: rotate each unit detector
+// ray by the orientation (qu_apply, quaternions.py:186-213), map it to the
+// side-by-side square Lambert projection (rosca_lambert_side_by_side,
+// sphere.py:145-185), sample the (H, 2W) master pattern bilinearly with
+// grid_sample semantics (align_corners=False, padding_mode="border";
+// master_pattern.py:197-206), then subtract the row mean.
+// K2 follows experiment_pats.py:318-346 (avg-pool binning) and
+// indexing.py:175-187 (mask select, row mean subtraction).
+//
+// Both end in the same row finaliser: the zero-mean FP32 row, its L2 norm, and
+// a unit-norm copy in the low-precision matching type (bf16, or e4m3 with a
+// per-row absmax scale), zero padded to the GEMM row length.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace ebsd {
+
+constexpr int kRowThreads = 256;
+constexpr int kMaxRowPix = 57344;  // 224 KiB of fp32 in shared memory
+
+__device__ __forceinline__ float2 lambert_side_by_side(float x, float y, float z) {
+  const float fac = sqrtf(fmaxf(2.0f * (1.0f - fabsf(z)), 0.0f));
+  const bool cond = fabsf(y) <= fabsf(x);
+  const float big = cond ? x : y;
+  const float sml = cond ? y : x;
+  const float sgn = big < 0.0f ? -1.0f : 1.0f;
+  const float simple = sgn * fac * 0.70710678118654752f;  // 2 / sqrt(8)
+  const float arct = sgn * fac * atan2f(sml * sgn, fabsf(big)) * 0.90031631615710607f;  // 2 sqrt2/pi
+  float u = cond ? simple : arct;
+  const float v = cond ? arct : simple;
+  u = u / 2.0f - 0.5f + (z < 0.0f ? 1.0f : 0.0f);
+  return make_float2(u, v);
+}
+
+// grid_sample(bilinear, align_corners=False, padding_mode="border") of one
+// point (u, v) in [-1, 1]^2 on an (h, w) image.
+__device__ __forceinline__ float sample_border(const float* __restrict__ img, int h, int w, float u,
+                                               float v) {
+  float ix = ((u + 1.0f) * (float)w - 1.0f) / 2.0f;
+  float iy = ((v + 1.0f) * (float)h - 1.0f) / 2.0f;
+  ix = fminf(fmaxf(ix, 0.0f), (float)(w - 1));
+  iy = fminf(fmaxf(iy, 0.0f), (float)(h - 1));
+  const float fx0 = floorf(ix), fy0 = floorf(iy);
+  const int x0 = (int)fx0, y0 = (int)fy0;
+  const int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
+  const float wnw = (fx0 + 1.0f - ix) * (fy0 + 1.0f - iy);
+  const float wne = (ix - fx0) * (fy0 + 1.0f - iy);
+  const float wsw = (fx0 + 1.0f - ix) * (iy - fy0);
+  const float wse = (ix - fx0) * (iy - fy0);
+  const float* r0 = img + (int64_t)y0 * w;
+  const float* r1 = img + (int64_t)y1 * w;
+  return __ldg(r0 + x0) * wnw + __ldg(r0 + x1) * wne + __ldg(r1 + x0) * wsw + __ldg(r1 + x1) * wse;
+}
+
+// Rotate v by unit quaternion q = (w, x, y, z): v + w t + q_vec x t,
+// t = 2 q_vec x v (equal to q (0, v) q* for unit q).
+__device__ __forceinline__ float3 rotate(float4 q, float vx, float vy, float vz) {
+  const float tx = 2.0f * (q.z * vz - q.w * vy);
+  const float ty = 2.0f * (q.w * vx - q.y * vz);
+  const float tz = 2.0f * (q.y * vy - q.z * vx);
+  return make_float3(vx + q.x * tx + (q.z * tz - q.w * ty), vy + q.x * ty + (q.w * tx - q.y * tz),
+                     vz + q.x * tz + (q.y * ty - q.z * tx));
+}
+
+struct RowOut {
+  float* f32;
+  int64_t ld_f32;
+  void* lp;
+  int lp_dtype;
+  int64_t ld_lp;
+  float* norm;
+  float* lp_scale;
+};
+
+// Row values are in row[0..n). Finalise and write outputs for `r`.
+__device__ void finalize_row(float* row, int n, int subtract_mean, int64_t r, const RowOut& o,
+                             float* fred, double* dred) {
+  const int tid = threadIdx.x;
+  double mean = 0.0;
+  if (subtract_mean) {
+    float s = 0.0f;
+    for (int p = tid; p < n; p += blockDim.x) s += row[p];
+    mean = block_sum<double>((double)s, dred) / (double)n;
+  }
+  const float meanf = (float)mean;
+  float ss = 0.0f, amax = 0.0f;
+  for (int p = tid; p < n; p += blockDim.x) {
+    const float v = row[p] - meanf;
+    row[p] = v;
+    ss += v * v;
+    amax = fmaxf(amax, fabsf(v));
+  }
+  const double nrm2 = block_sum<double>((double)ss, dred);
+  const float nrm = (float)sqrt(nrm2);
+  const float inv = nrm > 0.0f ? 1.0f / nrm : 0.0f;
+  float qscale = 1.0f;
+  if (o.lp && o.lp_dtype == EBSD_DT_E4M3) {
+    const float m = block_max(amax, fred) * inv;  // absmax of the unit row
+    qscale = m > 0.0f ? m / 448.0f : 1.0f;
+  }
+  if (tid == 0) {
+    if (o.norm) o.norm[r] = nrm;
+    if (o.lp_scale) o.lp_scale[r] = qscale;
+  }
+  if (o.f32) {
+    float* dst = o.f32 + r * o.ld_f32;
+    for (int p = tid; p < n; p += blockDim.x) dst[p] = row[p];
+  }
+  if (o.lp) {
+    if (o.lp_dtype == EBSD_DT_BF16) {
+      __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(o.lp) + r * o.ld_lp;
+      for (int p = tid; p < o.ld_lp; p += blockDim.x)
+        dst[p] = __float2bfloat16_rn(p < n ? row[p] * inv : 0.0f);
+    } else {
+      __nv_fp8_e4m3* dst = reinterpret_cast<__nv_fp8_e4m3*>(o.lp) + r * o.ld_lp;
+      const float s = inv / qscale;
+      for (int p = tid; p < o.ld_lp; p += blockDim.x)
+        dst[p] = __nv_fp8_e4m3(p < n ? row[p] * s : 0.0f);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRowThreads) k_project(
+    const float* __restrict__ mp, int mp_h, int mp_w2, const float* __restrict__ rays, int n_pix,
+    const float4* __restrict__ quats, int64_t n_rows, int subtract_mean, RowOut o) {
+  extern __shared__ float row[];
+  __shared__ float fred[32];
+  __shared__ double dred[32];
+  const float* rx = rays;
+  const float* ry = rays + n_pix;
+  const float* rz = rays + 2 * (int64_t)n_pix;
+  for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
+    const float4 q = quats[r];
+    for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
+      const float3 v = rotate(q, __ldg(rx + p), __ldg(ry + p), __ldg(rz + p));
+      const float2 uv = lambert_side_by_side(v.x, v.y, v.z);
+      row[p] = sample_border(mp, mp_h, mp_w2, uv.x, uv.y);
+    }
+    __syncthreads();
+    finalize_row(row, n_pix, subtract_mean, r, o, fred, dred);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kRowThreads) k_prep(const float* __restrict__ pats, int64_t n_rows,
+                                                      int h, int w, int64_t stride, int b,
+                                                      const int32_t* __restrict__ pix, int n_pix,
+                                                      int subtract_mean, RowOut o) {
+  extern __shared__ float row[];
+  __shared__ float fred[32];
+  __shared__ double dred[32];
+  const int wb = w / b;
+  const float cnt = (float)(b * b);
+  for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
+    const float* img = pats + r * stride;
+    for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
+      const int idx = pix ? __ldg(pix + p) : p;
+      float v;
+      if (b == 1) {
+        v = __ldg(img + idx);
+      } else {
+        const int i = idx / wb, j = idx - i * wb;
+        const float* src = img + (int64_t)(i * b) * w + j * b;
+        float s = 0.0f;
+        for (int a = 0; a < b; ++a)
+          for (int c = 0; c < b; ++c) s += __ldg(src + (int64_t)a * w + c);
+        v = s / cnt;
+      }
+      row[p] = v;
+    }
+    __syncthreads();
+    finalize_row(row, n_pix, subtract_mean, r, o, fred, dred);
+    __syncthreads();
+  }
+}
+
+__global__ void k_sample_points(const float* __restrict__ mp, int mp_h, int mp_w2,
+                                const float* __restrict__ xyz, int64_t n, int normalize,
+                                float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+    if (normalize) {
+      const float nrm = sqrtf(x * x + y * y + z * z);
+      x /= nrm;
+      y /= nrm;
+      z /= nrm;
+    }
+    const float2 uv = lambert_side_by_side(x, y, z);
+    out[i] = sample_border(mp, mp_h, mp_w2, uv.x, uv.y);
+  }
+}
+
+static int check_row_out(const RowOut& o, int n_pix) {
+  EBSD_ARG_CHECK(!o.f32 || o.ld_f32 >= n_pix, "ld_f32 (%lld) < row length (%d)", (long long)o.ld_f32,
+                 n_pix);
+  if (o.lp) {
+    EBSD_ARG_CHECK(o.lp_dtype == EBSD_DT_BF16 || o.lp_dtype == EBSD_DT_E4M3,
+                   "lp_dtype must be EBSD_DT_BF16 or EBSD_DT_E4M3");
+    EBSD_ARG_CHECK(o.ld_lp >= n_pix, "ld_lp (%lld) < row length (%d)", (long long)o.ld_lp, n_pix);
+  }
+  return 0;
+}
+
+static int row_grid(int64_t n_rows, size_t smem, const void* fn) {
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kRowThreads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  const int64_t cap = (int64_t)device_sm_count() * per_sm * 8;
+  return (int)std::min<int64_t>(n_rows, cap);
+}
+
+}  // namespace ebsd
+
+using namespace ebsd;
+
+extern "C" int ebsd_project_dictionary(const float* master_pattern, int mp_h, int mp_w2,
+                                       const float* rays_soa, int n_pix, const float* quats,
+                                       int64_t n_rows, int subtract_mean, float* out_f32,
+                                       int64_t ld_f32, void* out_lp, int lp_dtype, int64_t ld_lp,
+                                       float* out_norm, float* out_lp_scale, void* stream) {
+  EBSD_ARG_CHECK(master_pattern && rays_soa && quats, "ebsd_project_dictionary: null input");
+  EBSD_ARG_CHECK(mp_h >= 1 && mp_w2 >= 1, "master pattern shape (%d, %d) invalid", mp_h, mp_w2);
+  EBSD_ARG_CHECK(n_pix >= 1 && n_pix <= kMaxRowPix, "row length %d outside [1, %d]", n_pix,
+                 kMaxRowPix);
+  EBSD_ARG_CHECK(n_rows >= 0, "n_rows < 0");
+  EBSD_ARG_CHECK((reinterpret_cast<uintptr_t>(quats) & 15) == 0, "quats must be 16-byte aligned");
+  RowOut o{out_f32, ld_f32, out_lp, lp_dtype, ld_lp, out_norm, out_lp_scale};
+  if (int rc = check_row_out(o, n_pix)) return rc;
+  if (n_rows == 0) return 0;
+  const size_t smem = (size_t)n_pix * sizeof(float);
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_project, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+  const int grid = row_grid(n_rows, smem, (const void*)k_project);
+  k_project<<<grid, kRowThreads, smem, as_stream(stream)>>>(
+      master_pattern, mp_h, mp_w2, rays_soa, n_pix, reinterpret_cast<const float4*>(quats), n_rows,
+      subtract_mean, o);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int height, int width,
+                                  int64_t pattern_stride, int binning, const int32_t* pix_index,
+                                  int n_pix, int subtract_mean, float* out_f32, int64_t ld_f32,
+                                  void* out_lp, int lp_dtype, int64_t ld_lp, float* out_norm,
+                                  float* out_lp_scale, void* stream) {
+  EBSD_ARG_CHECK(patterns != nullptr, "ebsd_prep_patterns: null patterns");
+  EBSD_ARG_CHECK(binning >= 1 && height % binning == 0 && width % binning == 0,
+                 "binning %d must divide the pattern shape (%d, %d)", binning, height, width);
+  const int n_binned = (height / binning) * (width / binning);
+  EBSD_ARG_CHECK(n_pix >= 1 && n_pix <= kMaxRowPix, "row length %d outside [1, %d]", n_pix,
+                 kMaxRowPix);
+  EBSD_ARG_CHECK(pix_index || n_pix == n_binned,
+                 "without a pixel index the row length must equal the binned pixel count");
+  EBSD_ARG_CHECK(pattern_stride >= (int64_t)height * width, "pattern_stride too small");
+  RowOut o{out_f32, ld_f32, out_lp, lp_dtype, ld_lp, out_norm, out_lp_scale};
+  if (int rc = check_row_out(o, n_pix)) return rc;
+  if (n_rows == 0) return 0;
+  const size_t smem = (size_t)n_pix * sizeof(float);
+  EBSD_CUDA_CHECK(
+      cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = row_grid(n_rows, smem, (const void*)k_prep);
+  k_prep<<<grid, kRowThreads, smem, as_stream(stream)>>>(patterns, n_rows, height, width,
+                                                        pattern_stride, binning, pix_index, n_pix,
+                                                        subtract_mean, o);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int ebsd_sample_master_pattern(const float* master_pattern, int mp_h, int mp_w2,
+                                          const float* xyz, int64_t n, int normalize, float* out,
+                                          void* stream) {
+  EBSD_ARG_CHECK(master_pattern && xyz && out, "ebsd_sample_master_pattern: null pointer");
+  EBSD_ARG_CHECK(mp_h >= 1 && mp_w2 >= 1 && n >= 0, "ebsd_sample_master_pattern: bad sizes");
+  if (n == 0) return 0;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, (int64_t)device_sm_count() * 16);
+  k_sample_points<<<blocks, 256, 0, as_stream(stream)>>>(master_pattern, mp_h, mp_w2, xyz, n,
+                                                         normalize, out);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}

@@ -1,0 +1,201 @@
+// K4/K6: merge of the per-range candidate lists, FP32 re-score of the best
+// candidates, and the final sorted top-k per query.
+//
+// Replaces ChunkedKNN.retrieve_topk (ebsdtorch/utils/knn.py:268-287; the
+// reference sorts its running top-k with torch.topk(sorted=True)). The exact
+// scores are the reference's metric: the FP32 dot product of the zero-mean
+// query row with the zero-mean dictionary row (knn.py:96-97).
+// One CTA per query; candidates are ordered by (score desc, index asc).
+#include "common.cuh"
+
+namespace ebsd {
+
+constexpr int kMergeThreads = 256;
+constexpr int kMaxCand = 4096;    // part_slots * n_cand per query
+constexpr int kMaxRescore = 128;  // candidates re-scored per query
+constexpr int kMaxKOut = 128;
+static_assert(kMaxRescore + kMaxKOut <= kMergeThreads, "one finalist per thread");
+
+// (v1, i1) ranks before (v2, i2)?
+__device__ __forceinline__ bool ranks_before(float v1, int64_t i1, float v2, int64_t i2) {
+  if (i1 < 0) return false;
+  if (i2 < 0) return true;
+  if (v1 != v2) return v1 > v2;
+  return i1 < i2;
+}
+
+// In-place bitonic sort of n (power of two) entries in shared memory.
+__device__ void bitonic_sort(float* v, int64_t* idx, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      __syncthreads();
+      for (int t = threadIdx.x; t < n / 2; t += blockDim.x) {
+        const int lo = 2 * t - (t & (stride - 1));
+        const int hi = lo + stride;
+        const bool up = ((lo & size) == 0);
+        const bool before = ranks_before(v[lo], idx[lo], v[hi], idx[hi]);
+        // ascending "rank order" in up-segments: element that ranks first goes low
+        if (up != before) {
+          const float tv = v[lo];
+          v[lo] = v[hi];
+          v[hi] = tv;
+          const int64_t ti = idx[lo];
+          idx[lo] = idx[hi];
+          idx[hi] = ti;
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
+    const float* __restrict__ part_val, const int32_t* __restrict__ part_idx, int n_list,
+    const float* __restrict__ q_f32, int64_t ld_q, const float* __restrict__ d_f32, int64_t ld_d,
+    int64_t d_base, int64_t d_rows, int n_pix, const float* __restrict__ q_norm, const float* __restrict__ d_norm,
+    const float* __restrict__ q_lp_scale, int similarity, int n_rescore, int k_out,
+    const float* __restrict__ run_val, const int64_t* __restrict__ run_idx, int sort_n,
+    float* __restrict__ out_val, int64_t* __restrict__ out_idx) {
+  extern __shared__ float dyn[];
+  float* qrow = dyn;                                            // n_pix (re-score only)
+  float* cv = dyn + (d_f32 ? ((n_pix + 3) & ~3) : 0);           // sort_n
+  int64_t* ci = reinterpret_cast<int64_t*>(cv + ((sort_n + 1) & ~1));  // sort_n
+  __shared__ float fin_v[kMaxRescore + kMaxKOut];
+  __shared__ int64_t fin_i[kMaxRescore + kMaxKOut];
+
+  const int64_t q = blockIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+
+  // 1. gather all candidates of this query
+  for (int t = tid; t < sort_n; t += blockDim.x) {
+    if (t < n_list) {
+      const int32_t i = part_idx[q * n_list + t];
+      cv[t] = part_val[q * n_list + t];
+      ci[t] = i;
+    } else {
+      cv[t] = -INFINITY;
+      ci[t] = -1;
+    }
+  }
+  if (d_f32) {
+    const float* src = q_f32 + q * ld_q;
+    for (int p = tid; p < n_pix; p += blockDim.x) qrow[p] = src[p];
+  }
+  bitonic_sort(cv, ci, sort_n);
+
+  // 2. exact FP32 scores of the best n_rescore (or approximate * |q|)
+  const int nr = n_rescore;
+  if (d_f32) {
+    for (int c = wid; c < nr; c += nw) {
+      const int64_t di = (ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
+      float acc = 0.0f;
+      if (di >= 0) {
+        const float* drow = d_f32 + (di - d_base) * ld_d;
+        if ((n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0) {
+          const float4* d4 = reinterpret_cast<const float4*>(drow);
+          const float4* q4 = reinterpret_cast<const float4*>(qrow);
+          for (int p = lane; p < (n_pix >> 2); p += 32) {
+            const float4 a = __ldg(d4 + p), b = q4[p];
+            acc = fmaf(a.x, b.x, acc);
+            acc = fmaf(a.y, b.y, acc);
+            acc = fmaf(a.z, b.z, acc);
+            acc = fmaf(a.w, b.w, acc);
+          }
+        } else {
+          for (int p = lane; p < n_pix; p += 32) acc = fmaf(__ldg(drow + p), qrow[p], acc);
+        }
+      }
+      acc = warp_sum(acc);
+      if (lane == 0) {
+        if (similarity == EBSD_SIM_COSINE && di >= 0) {
+          const float den = q_norm[q] * d_norm[di - d_base];
+          acc = den > 0.0f ? acc / den : 0.0f;
+        }
+        fin_v[c] = di >= 0 ? acc : -INFINITY;
+        fin_i[c] = di;
+      }
+    }
+  } else {
+    float qn = q_lp_scale ? q_lp_scale[q] : 1.0f;
+    if (similarity == EBSD_SIM_DOT && q_norm) qn *= q_norm[q];
+    for (int c = tid; c < nr; c += blockDim.x) {
+      fin_v[c] = ci[c] >= 0 ? cv[c] * qn : -INFINITY;
+      fin_i[c] = ci[c];
+    }
+  }
+  // 3. running results
+  int nf = nr;
+  if (run_val) {
+    for (int c = tid; c < k_out; c += blockDim.x) {
+      fin_v[nr + c] = run_val[q * k_out + c];
+      fin_i[nr + c] = run_idx[q * k_out + c];
+    }
+    nf += k_out;
+  }
+  __syncthreads();
+  // 4. top k_out of the nf finalists by rank selection (nf <= blockDim.x).
+  // Running results and new candidates come from disjoint dictionary ranges.
+  const int valid = (tid < nf && fin_i[tid] >= 0) ? 1 : 0;
+  const int n_valid = __syncthreads_count(valid);
+  if (valid) {
+    const float v = fin_v[tid];
+    const int64_t i = fin_i[tid];
+    int rank = 0;
+    for (int o = 0; o < nf; ++o)
+      if (o != tid && ranks_before(fin_v[o], fin_i[o], v, i)) ++rank;
+    if (rank < k_out) {
+      out_val[q * k_out + rank] = v;
+      out_idx[q * k_out + rank] = i;
+    }
+  }
+  for (int r = n_valid + tid; r < k_out; r += blockDim.x) {
+    out_val[q * k_out + r] = -INFINITY;
+    out_idx[q * k_out + r] = -1;
+  }
+}
+
+}  // namespace ebsd
+
+using namespace ebsd;
+
+extern "C" int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
+                                  int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
+                                  const float* d_f32, int64_t ld_d, int64_t d_index_base,
+                                  int64_t d_rows, int n_pix,
+                                  const float* q_norm, const float* d_norm, const float* q_lp_scale,
+                                  int similarity,
+                                  int n_rescore, int k_out, const float* run_val,
+                                  const int64_t* run_idx, float* out_val, int64_t* out_idx,
+                                  void* stream) {
+  EBSD_ARG_CHECK(part_val && part_idx && out_val && out_idx, "ebsd_merge_rescore: null pointer");
+  EBSD_ARG_CHECK(n_queries >= 0 && part_slots >= 1 && n_cand >= 1, "bad candidate-list sizes");
+  const int n_list = part_slots * n_cand;
+  EBSD_ARG_CHECK(n_list <= kMaxCand, "part_slots * n_cand = %d exceeds %d", n_list, kMaxCand);
+  EBSD_ARG_CHECK(k_out >= 1 && k_out <= kMaxKOut, "k_out %d outside [1, %d]", k_out, kMaxKOut);
+  EBSD_ARG_CHECK(n_rescore >= 1 && n_rescore <= kMaxRescore && n_rescore <= n_list,
+                 "n_rescore %d outside [1, min(%d, %d)]", n_rescore, kMaxRescore, n_list);
+  EBSD_ARG_CHECK(!(run_val == nullptr) == !(run_idx == nullptr), "run_val/run_idx must be given together");
+  EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || similarity == EBSD_SIM_COSINE,
+                 "similarity must be EBSD_SIM_DOT or EBSD_SIM_COSINE");
+  if (d_f32) {
+    EBSD_ARG_CHECK(q_f32 != nullptr, "q_f32 is required for re-scoring");
+    EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || (q_norm && d_norm),
+                   "cosine re-scoring needs q_norm and d_norm");
+    EBSD_ARG_CHECK(n_pix >= 1 && ld_q >= n_pix && ld_d >= n_pix, "bad re-score row length");
+    EBSD_ARG_CHECK(n_pix <= 40960, "re-score row length %d exceeds 40960", n_pix);
+    EBSD_ARG_CHECK(d_rows >= 1 && d_index_base >= 0, "bad dictionary row range");
+  }
+  if (n_queries == 0) return 0;
+  int sort_n = 1;
+  while (sort_n < n_list) sort_n <<= 1;
+  const size_t smem = (d_f32 ? (size_t)((n_pix + 3) & ~3) * 4 : 0) + (size_t)((sort_n + 1) & ~1) * 4 +
+                      (size_t)sort_n * 8 + 16;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_merge_rescore, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+  EBSD_ARG_CHECK(n_queries < INT32_MAX, "too many queries");
+  k_merge_rescore<<<(int)n_queries, kMergeThreads, smem, as_stream(stream)>>>(
+      part_val, part_idx, n_list, q_f32, ld_q, d_f32, ld_d, d_index_base, d_rows, n_pix, q_norm, d_norm, q_lp_scale,
+      similarity, n_rescore, k_out, run_val, run_idx, sort_n, out_val, out_idx);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}

@@ -1,0 +1,192 @@
+"""Dictionary-indexing engine: the GPU pipeline behind the drop-in functions.
+
+Data layout in HBM (one phase):
+  dictionary  lp rows   (D_pad x K_pad)  bf16 / e4m3, unit L2 norm, zero padded
+              f32 rows  (D x P')         zero-mean FP32 rows (the reference's vectors)
+              norm, lp scale (D_pad)     per-row L2 norm, e4m3 dequant scale
+  query chunk the same three for Qc rows, plus candidate lists
+              (Qc_pad x splits x n_cand) and the final (Q x k) results.
+Per query chunk: prepare (K2) -> tcgen05 contraction with streaming top-k
+(K3) -> merge + FP32 re-score (K4). When the dictionary does not fit the
+memory budget it is processed in chunks and each chunk's exact top-k is
+merged into a running result.
+"""
+
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import Callable, Optional
+
+import torch
+
+from . import kernels
+from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT
+from .kernels import LP_DTYPES, LP_KMULT, LP_TORCH, TILE_D, TILE_Q, RowBuffers, round_up
+
+MAX_CAND = 64
+
+
+@dataclass
+class SearchConfig:
+    """precision: element type of the tensor-core contraction ("bf16" | "fp8").
+    rescore_k: candidates per query re-scored in FP32 (0 = report the
+    low-precision score). similarity: "dot" is the reference metric (raw dot of
+    zero-mean rows, knn.py:96-97); "cosine" divides it by both norms.
+    workspace_bytes: device-memory budget (default: 90 % of free memory)."""
+
+    precision: str = "bf16"
+    rescore_k: int = 32
+    similarity: str = "dot"
+    workspace_bytes: Optional[int] = None
+    query_chunk: Optional[int] = None
+    dict_chunk: Optional[int] = None
+
+    def validate(self):
+        if self.precision not in LP_DTYPES:
+            raise ValueError(f"precision must be one of {sorted(LP_DTYPES)}, got {self.precision!r}")
+        if self.similarity not in ("dot", "cosine"):
+            raise ValueError(f"similarity must be 'dot' or 'cosine', got {self.similarity!r}")
+        if not 0 <= self.rescore_k <= 128:
+            raise ValueError("rescore_k must be in [0, 128]")
+
+
+def _pow2_at_least(n: int) -> int:
+    return 1 << max(0, math.ceil(math.log2(max(1, n))))
+
+
+class RowSet:
+    """Low-precision + FP32 rows of a dictionary (or query) block on the GPU."""
+
+    def __init__(self, n_rows: int, n_pix: int, pad_rows: int, lp_dtype: int, keep_f32: bool, device):
+        self.n_rows, self.n_pix, self.lp_dtype = n_rows, n_pix, lp_dtype
+        self.k_pad = round_up(n_pix, LP_KMULT[lp_dtype])
+        rows_pad = round_up(max(n_rows, 1), pad_rows)
+        self.lp = torch.zeros((rows_pad, self.k_pad), dtype=LP_TORCH[lp_dtype], device=device)
+        self.f32 = torch.empty((n_rows, n_pix), dtype=torch.float32, device=device) if keep_f32 else None
+        self.norm = torch.zeros(rows_pad, dtype=torch.float32, device=device)
+        self.lp_scale = torch.ones(rows_pad, dtype=torch.float32, device=device) if lp_dtype != kernels.DT_BF16 else None
+
+    def buffers(self, r0: int, r1: int, with_f32: bool = True) -> RowBuffers:
+        return RowBuffers(
+            f32=self.f32[r0:r1] if (self.f32 is not None and with_f32) else None,
+            lp=self.lp[r0:r1],
+            lp_dtype=self.lp_dtype,
+            norm=self.norm[r0:r1],
+            lp_scale=self.lp_scale[r0:r1] if self.lp_scale is not None else None,
+        )
+
+    @staticmethod
+    def bytes_per_row(n_pix: int, lp_dtype: int, keep_f32: bool) -> int:
+        k_pad = round_up(n_pix, LP_KMULT[lp_dtype])
+        return k_pad * (2 if lp_dtype == kernels.DT_BF16 else 1) + (4 * n_pix if keep_f32 else 0) + 8
+
+
+def _col_scale(rows: RowSet, similarity: str) -> Optional[torch.Tensor]:
+    """Per-dictionary-row factor of the tensor-core score: |d| (dot metric)
+    times the e4m3 dequant scale."""
+    if similarity == "dot":
+        return rows.norm if rows.lp_scale is None else rows.norm * rows.lp_scale
+    return rows.lp_scale
+
+
+def default_budget(device) -> int:
+    free, _ = torch.cuda.mem_get_info(device)
+    return int(free * 0.9)
+
+
+# A query provider fills rows [q0, q1) of a RowSet: fn(q0, q1, buffers)
+QueryFill = Callable[[int, int, RowBuffers], None]
+# A dictionary provider fills rows [d0, d1): fn(d0, d1, buffers)
+DictFill = Callable[[int, int, RowBuffers], None]
+
+
+class Searcher:
+    """Top-k dictionary search for one phase."""
+
+    def __init__(self, n_dict: int, n_queries: int, n_pix: int, k: int, cfg: SearchConfig, device):
+        cfg.validate()
+        if k < 1:
+            raise ValueError("top_k must be >= 1")
+        if k > n_dict:
+            raise ValueError(f"top_k ({k}) exceeds the dictionary size ({n_dict})")
+        if k > MAX_CAND:
+            raise ValueError(f"top_k above {MAX_CAND} is not supported")
+        self.n_dict, self.n_queries, self.n_pix, self.k, self.cfg = n_dict, n_queries, n_pix, k, cfg
+        self.device = torch.device(device)
+        self.lp_dtype = LP_DTYPES[cfg.precision]
+        self.rescore = cfg.rescore_k > 0
+        self.n_cand = min(MAX_CAND, _pow2_at_least(max(k, cfg.rescore_k)))
+        self.n_rescore = max(k, cfg.rescore_k) if self.rescore else k
+        self.sim = SIM_DOT if cfg.similarity == "dot" else SIM_COSINE
+        self._plan()
+
+    def _plan(self):
+        budget = self.cfg.workspace_bytes or default_budget(self.device)
+        drow = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
+        qrow_base = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
+        max_splits = 64
+        qrow = qrow_base + max_splits * self.n_cand * 8 + self.k * 12
+        q_min = min(round_up(self.n_queries, TILE_Q), 16384)
+        if self.cfg.dict_chunk:
+            dchunk = round_up(self.cfg.dict_chunk, TILE_D)
+        elif self.n_dict * drow + q_min * qrow <= budget:
+            dchunk = round_up(self.n_dict, TILE_D)
+        else:
+            dchunk = max(TILE_D, (budget // 2) // drow // TILE_D * TILE_D)
+        self.dict_chunk = min(dchunk, round_up(self.n_dict, TILE_D))
+        left = budget - self.dict_chunk * drow
+        if self.cfg.query_chunk:
+            qchunk = round_up(self.cfg.query_chunk, TILE_Q)
+        else:
+            qchunk = max(TILE_Q, left // qrow // TILE_Q * TILE_Q)
+        self.query_chunk = min(qchunk, round_up(self.n_queries, TILE_Q))
+        if left < self.query_chunk * qrow and not self.cfg.query_chunk:
+            raise MemoryError(
+                f"dictionary indexing needs more device memory than the budget of {budget / 2**30:.1f} GiB")
+
+    def run(self, fill_dict: DictFill, fill_queries: QueryFill, queries_reusable: bool = True):
+        """Search all queries against all dictionary rows.
+        Returns (indices (Q, k) int64, scores (Q, k) float32) on the device."""
+        dev, Q, D, k = self.device, self.n_queries, self.n_dict, self.k
+        out_val = torch.empty((Q, k), dtype=torch.float32, device=dev)
+        out_idx = torch.empty((Q, k), dtype=torch.int64, device=dev)
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
+        qc = self.query_chunk
+        q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.rescore, dev)
+        n_dchunks = (D + self.dict_chunk - 1) // self.dict_chunk
+        for ci, d0 in enumerate(range(0, D, self.dict_chunk)):
+            d1 = min(D, d0 + self.dict_chunk)
+            nd = d1 - d0
+            if nd < dict_rows.n_rows:
+                dict_rows.lp[nd:].zero_()
+                dict_rows.norm[nd:].zero_()
+            fill_dict(d0, d1, dict_rows.buffers(0, nd))
+            col_scale = _col_scale(dict_rows, self.cfg.similarity)
+            nd_pad = round_up(nd, TILE_D)
+            d_lp = dict_rows.lp[:nd_pad]
+            for q0 in range(0, Q, qc):
+                q1 = min(Q, q0 + qc)
+                nq = q1 - q0
+                nq_pad = round_up(nq, TILE_Q)
+                fill_queries(q0, q1, q_rows.buffers(0, nq))
+                splits = kernels.auto_splits(nq_pad, nd_pad)
+                part_val = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.float32, device=dev)
+                part_idx = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.int32, device=dev)
+                kernels.match_topk(q_rows.lp[:nq_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand, splits,
+                                   part_val, part_idx, splits, 0, d0, status)
+                run = ci > 0
+                kernels.merge_rescore(
+                    part_val, part_idx, nq, splits, self.n_cand,
+                    q_rows.f32[:nq] if self.rescore else None,
+                    dict_rows.f32[:nd] if self.rescore else None, d0,
+                    self.n_pix, q_rows.norm, dict_rows.norm, q_rows.lp_scale, self.sim,
+                    min(self.n_rescore, splits * self.n_cand), k,
+                    out_val[q0:q1] if run else None, out_idx[q0:q1] if run else None,
+                    out_val[q0:q1], out_idx[q0:q1])
+        st = int(status.item())
+        if st != 0:
+            code = "device wait timed out" if st == DEVICE_TIMEOUT else f"status {st:#x}"
+            raise RuntimeError(f"dictionary match kernel reported an error: {code}")
+        return out_idx, out_val

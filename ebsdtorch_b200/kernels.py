@@ -1,0 +1,222 @@
+"""Tensor-level wrappers over the C-ABI kernels.
+
+Each function checks devices, dtypes and layouts, allocates outputs with
+PyTorch (the library itself allocates nothing), passes raw pointers plus the
+current CUDA stream to ``libebsd_b200.so`` and returns tensors. All work is
+stream-ordered on ``torch.cuda.current_stream()``; nothing here synchronises
+except ``grid_fz`` (it must read the fundamental-zone point count).
+"""
+
+from __future__ import annotations
+
+from typing import Optional
+
+import torch
+
+from . import _capi
+from ._capi import DT_BF16, DT_E4M3, call, ptr
+
+LP_DTYPES = {"bf16": DT_BF16, "fp8": DT_E4M3}
+LP_TORCH = {DT_BF16: torch.bfloat16, DT_E4M3: torch.float8_e4m3fn}
+LP_KMULT = {DT_BF16: 64, DT_E4M3: 128}
+TILE_Q, TILE_D = 128, 256
+
+
+def round_up(n: int, m: int) -> int:
+    return (n + m - 1) // m * m
+
+
+def _stream(dev: torch.device) -> int:
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def _cuda(t: torch.Tensor, name: str, dtype=None, contiguous=True) -> torch.Tensor:
+    if not isinstance(t, torch.Tensor) or t.device.type != "cuda":
+        raise RuntimeError(f"{name} must be a CUDA tensor (ebsdtorch_b200 runs on sm_100 GPUs only)")
+    if dtype is not None and t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if contiguous and not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    return t
+
+
+# ---------------------------------------------------------------- A1/A2 grid
+
+
+def grid_fz(laue_id: int, edge_length: int, device, want_f64: bool = False):
+    """FZ quaternions of the edge^3 cubochoric grid in reference order.
+    Returns (q_f32 (n, 4), q_f64 (n, 4) or None)."""
+    device = torch.device(device)
+    lib = _capi.load()
+    nbytes = int(lib.ebsd_grid_workspace_bytes(int(edge_length)))
+    if nbytes == 0:
+        raise ValueError(f"grid edge length {edge_length} must be positive")
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=device)
+    s = _stream(device)
+    call("ebsd_grid_fz_count", int(laue_id), int(edge_length), ptr(ws), nbytes, ptr(cnt), s)
+    n = int(cnt.item())
+    q32 = torch.empty((n, 4), dtype=torch.float32, device=device)
+    q64 = torch.empty((n, 4), dtype=torch.float64, device=device) if want_f64 else None
+    if n:
+        call("ebsd_grid_fz_write", int(laue_id), int(edge_length), ptr(ws), nbytes, ptr(q32), ptr(q64), s)
+    return q32, q64
+
+
+def gather_rows(src: torch.Tensor, index: torch.Tensor) -> torch.Tensor:
+    """out[i] = src[index[i]] for float32 rows."""
+    _cuda(src, "src", torch.float32)
+    _cuda(index, "index", torch.int64)
+    src2 = src.reshape(src.shape[0], -1)
+    out = torch.empty((index.numel(), src2.shape[1]), dtype=torch.float32, device=src.device)
+    call("ebsd_gather_rows", ptr(src2), src2.shape[0], src2.shape[1], ptr(index), index.numel(), ptr(out),
+         _stream(src.device))
+    return out.reshape((index.numel(),) + tuple(src.shape[1:]))
+
+
+# ------------------------------------------------------- A4-A8 row producers
+
+
+class RowBuffers:
+    """Destination of the projector / pattern preparation for a block of rows.
+    Any field may be None (not written)."""
+
+    def __init__(self, f32=None, lp=None, lp_dtype=DT_BF16, norm=None, lp_scale=None):
+        self.f32, self.lp, self.lp_dtype, self.norm, self.lp_scale = f32, lp, lp_dtype, norm, lp_scale
+
+    def args(self, n_pix: int):
+        ld_f32 = self.f32.stride(0) if self.f32 is not None else 0
+        ld_lp = self.lp.stride(0) if self.lp is not None else 0
+        return (ptr(self.f32), ld_f32, ptr(self.lp), self.lp_dtype, ld_lp, ptr(self.norm), ptr(self.lp_scale))
+
+
+def project(master_pattern: torch.Tensor, rays_soa: torch.Tensor, quats: torch.Tensor, out: RowBuffers,
+            subtract_mean: bool = True) -> None:
+    """K1: simulated dictionary rows for `quats` into `out` (row i <- quats[i])."""
+    _cuda(master_pattern, "master_pattern", torch.float32)
+    _cuda(rays_soa, "rays_soa", torch.float32)
+    _cuda(quats, "quats", torch.float32)
+    if rays_soa.dim() != 2 or rays_soa.shape[0] != 3:
+        raise ValueError("rays_soa must be (3, n_pix)")
+    n_pix = rays_soa.shape[1]
+    call("ebsd_project_dictionary", ptr(master_pattern), master_pattern.shape[0], master_pattern.shape[1],
+         ptr(rays_soa), n_pix, ptr(quats), quats.shape[0], int(bool(subtract_mean)), *out.args(n_pix),
+         _stream(quats.device))
+
+
+def prep_patterns(patterns: torch.Tensor, out: RowBuffers, binning: int = 1,
+                  pix_index: Optional[torch.Tensor] = None, n_pix: Optional[int] = None,
+                  subtract_mean: bool = True) -> None:
+    """K2: (n, H, W) fp32 patterns (row stride may exceed H*W) -> rows in `out`."""
+    _cuda(patterns, "patterns", torch.float32, contiguous=False)
+    if patterns.dim() == 2:
+        patterns = patterns.unsqueeze(1)
+    n, h, w = patterns.shape
+    if patterns.stride(2) != 1 or patterns.stride(1) != w:
+        raise ValueError("each pattern must be a contiguous (H, W) image")
+    if pix_index is not None:
+        _cuda(pix_index, "pix_index", torch.int32)
+        n_pix = pix_index.numel()
+    elif n_pix is None:
+        n_pix = (h // binning) * (w // binning)
+    call("ebsd_prep_patterns", ptr(patterns), n, h, w, patterns.stride(0), int(binning), ptr(pix_index), int(n_pix),
+         int(bool(subtract_mean)), *out.args(n_pix), _stream(patterns.device))
+
+
+def sample_master_pattern(master_pattern: torch.Tensor, xyz: torch.Tensor, normalize: bool) -> torch.Tensor:
+    _cuda(master_pattern, "master_pattern", torch.float32)
+    _cuda(xyz, "coords", torch.float32)
+    out = torch.empty(xyz.shape[:-1], dtype=torch.float32, device=xyz.device)
+    call("ebsd_sample_master_pattern", ptr(master_pattern), master_pattern.shape[0], master_pattern.shape[1],
+         ptr(xyz), out.numel(), int(bool(normalize)), ptr(out), _stream(xyz.device))
+    return out
+
+
+def avg_pool(x: torch.Tensor, binning: int) -> torch.Tensor:
+    """b x b average pooling over the last two axes."""
+    _cuda(x, "input", torch.float32)
+    h, w = x.shape[-2:]
+    lead = x.shape[:-2]
+    n = x.numel() // (h * w) if x.numel() else 0
+    out = torch.empty(lead + (h // binning, w // binning), dtype=torch.float32, device=x.device)
+    call("ebsd_avg_pool", ptr(x), n, h, w, int(binning), ptr(out), _stream(x.device))
+    return out
+
+
+# ---------------------------------------------------------- A9/A10 matching
+
+
+def auto_splits(n_queries_pad: int, n_dict_pad: int) -> int:
+    return int(_capi.load().ebsd_match_auto_splits(n_queries_pad, n_dict_pad))
+
+
+def match_topk(q_lp, d_lp, n_dict_valid: int, lp_dtype: int, col_scale, n_cand: int, splits: int,
+               part_val, part_idx, part_slots: int, slot_base: int, index_base: int, status) -> None:
+    call("ebsd_match_topk", ptr(q_lp), q_lp.shape[0], ptr(d_lp), d_lp.shape[0], int(n_dict_valid), q_lp.shape[1],
+         lp_dtype, ptr(col_scale), int(n_cand), int(splits), ptr(part_val), ptr(part_idx), int(part_slots),
+         int(slot_base), int(index_base), ptr(status), _stream(q_lp.device))
+
+
+def merge_rescore(part_val, part_idx, n_queries: int, part_slots: int, n_cand: int, q_f32, d_f32, d_index_base: int,
+                  n_pix: int, q_norm, d_norm, q_lp_scale, similarity: int, n_rescore: int, k_out: int, run_val,
+                  run_idx, out_val, out_idx) -> None:
+    call("ebsd_merge_rescore", ptr(part_val), ptr(part_idx), int(n_queries), int(part_slots), int(n_cand),
+         ptr(q_f32), q_f32.stride(0) if q_f32 is not None else 0, ptr(d_f32),
+         d_f32.stride(0) if d_f32 is not None else 0, int(d_index_base),
+         d_f32.shape[0] if d_f32 is not None else 1, int(n_pix), ptr(q_norm), ptr(d_norm),
+         ptr(q_lp_scale),
+         int(similarity), int(n_rescore), int(k_out), ptr(run_val), ptr(run_idx), ptr(out_val), ptr(out_idx),
+         _stream(part_val.device))
+
+
+# ------------------------------------------------------------------ A11/A12
+
+
+def gemm_nt(A, B, out, alpha: float = 1.0, accumulate: bool = False, m_valid=None, n_valid=None, status=None,
+            lp_dtype: int = DT_BF16) -> torch.Tensor:
+    """out[:m_valid, :n_valid] = alpha * A @ B.T (+ out)."""
+    _cuda(A, "A")
+    _cuda(B, "B")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=A.device)
+    m_valid = A.shape[0] if m_valid is None else m_valid
+    n_valid = B.shape[0] if n_valid is None else n_valid
+    call("ebsd_gemm_nt", ptr(A), A.shape[0], ptr(B), B.shape[0], A.shape[1], lp_dtype, float(alpha),
+         int(bool(accumulate)), ptr(out), out.stride(0), int(m_valid), int(n_valid), ptr(status),
+         _stream(A.device))
+    return status
+
+
+def col_mean(X: torch.Tensor) -> torch.Tensor:
+    _cuda(X, "X", torch.float32, contiguous=False)
+    out = torch.empty(X.shape[1], dtype=torch.float32, device=X.device)
+    call("ebsd_col_mean", ptr(X), X.shape[0], X.shape[1], X.stride(0), ptr(out), _stream(X.device))
+    return out
+
+
+def split3(X: torch.Tensor, pattern: int, transpose: bool, seg_len: int, out_rows_pad: int, ld_out: int,
+           shift: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Three-term bf16 split (see ebsd_split3_bf16); returns (out_rows_pad, ld_out) bf16 with
+    rows beyond the data zero-filled."""
+    _cuda(X, "X", torch.float32, contiguous=False)
+    n_rows, n_cols = X.shape
+    rows = n_cols if transpose else n_rows
+    out = torch.empty((out_rows_pad, ld_out), dtype=torch.bfloat16, device=X.device)
+    if out_rows_pad > rows:
+        out[rows:].zero_()
+    call("ebsd_split3_bf16", ptr(X), n_rows, n_cols, X.stride(0), ptr(shift), int(bool(transpose)), int(pattern),
+         ptr(out), ld_out, int(seg_len), _stream(X.device))
+    return out
+
+
+# ---------------------------------------------------------------------- A14
+
+
+def disori_angle(q1: torch.Tensor, q2: torch.Tensor, laue_id: int) -> torch.Tensor:
+    _cuda(q1, "quats1", torch.float32)
+    _cuda(q2, "quats2", torch.float32)
+    if q1.shape != q2.shape or q1.shape[-1] != 4:
+        raise ValueError(f"quats1 and quats2 must have the same (..., 4) shape, got {q1.shape} and {q2.shape}")
+    out = torch.empty(q1.shape[:-1], dtype=torch.float32, device=q1.device)
+    call("ebsd_disori_angle", ptr(q1), ptr(q2), out.numel(), int(laue_id), ptr(out), _stream(q1.device))
+    return out

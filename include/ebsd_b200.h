@@ -1,0 +1,215 @@
+/*
+ * ebsd_b200 — C-ABI of the B200 (sm_100a) dictionary-indexing kernels.
+ *
+ * The reference (ebsdtorch, pure Python/PyTorch) has no native interface; its
+ * dictionary-indexing path is a chain of PyTorch calls inside
+ *   ebsdtorch/ebsd/indexing.py:14-211   dictionary_index_orientations
+ *   ebsdtorch/ebsd/indexing.py:214-476  pca_dictionary_index_orientations
+ * Each entry point below replaces one link of that chain; the comment on it
+ * names the reference code it stands in for. The Python package
+ * ebsdtorch_b200 binds these symbols with ctypes and mirrors the reference's
+ * Python API on top of them.
+ *
+ * Conventions
+ *  - All pointers are device pointers unless stated otherwise; buffers are
+ *    allocated by the caller. The library allocates no device memory.
+ *  - Work is enqueued on `stream` (a cudaStream_t passed as void*); calls are
+ *    asynchronous unless stated otherwise.
+ *  - Return value: 0 success, > 0 argument error (nothing launched),
+ *    < 0 negated cudaError_t. ebsd_last_error() returns the message.
+ *  - Kernels that spin-wait take `int* d_status` (device int, zero before
+ *    the call); a wait that exceeds its limit stores EBSD_DEVICE_TIMEOUT there
+ *    and the kernel returns early instead of hanging.
+ *  - Low-precision row layouts ("lp rows"): row-major, `ld` elements per row,
+ *    ld a multiple of 64 (bf16) or 128 (e4m3), padding zero-filled.
+ */
+#ifndef EBSD_B200_H
+#define EBSD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EBSD_OK 0
+#define EBSD_ERR_ARG 1
+#define EBSD_ERR_UNSUPPORTED 2
+#define EBSD_DEVICE_TIMEOUT 0x7001
+
+/* element types of low-precision rows */
+#define EBSD_DT_F32 0
+#define EBSD_DT_BF16 1
+#define EBSD_DT_E4M3 2
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int ebsd_version(void);
+
+/* Copy the last error message of this host thread into buf (NUL-terminated).
+ * Returns the full message length. */
+int ebsd_last_error(char* buf, size_t n);
+
+/* 0 if `device` is an sm_100 GPU this library can run on. */
+int ebsd_device_check(int device);
+
+/* ---- A1/A2: SO(3) cubochoric grid restricted to a Laue fundamental zone ---
+ * Replaces ebsdtorch/s2_and_so3/laue_fz_ori.py:516-557
+ * (sample_ori_fz_laue_angle: so3_cubochoric_grid sampling.py:179-205,
+ *  cu2qu orientations.py:1136, ori_in_fz_laue laue_fz_ori.py:144-239).
+ * Computed in FP64. The random permutation of the reference (torch.randperm on
+ * the global CPU generator) is applied by the caller with ebsd_gather_rows. */
+
+/* Bytes of workspace needed for an edge^3 grid. */
+size_t ebsd_grid_workspace_bytes(int edge_length);
+
+/* Pass 1: FZ membership of all edge^3 grid points; writes the number of FZ
+ * points to *d_count (device int64). */
+int ebsd_grid_fz_count(int laue_id, int edge_length, void* workspace, size_t workspace_bytes,
+                       int64_t* d_count, void* stream);
+
+/* Pass 2 (after pass 1 on the same workspace): the FZ quaternions (w,x,y,z),
+ * w >= 0, in the reference's grid order, to out_f32 (n x 4) and, if not NULL,
+ * out_f64 (n x 4). */
+int ebsd_grid_fz_write(int laue_id, int edge_length, const void* workspace, size_t workspace_bytes,
+                       float* out_f32, double* out_f64, void* stream);
+
+/* out[i, :] = in[index[i], :] for rows of `width` floats.
+ * Replaces the `so3_samples_fz[torch.randperm(n)]` gather
+ * (laue_fz_ori.py:554-555) and `ori_tensor[matches]` (indexing.py:205). */
+int ebsd_gather_rows(const float* in, int64_t n_in, int width, const int64_t* index, int64_t n_out,
+                     float* out, void* stream);
+
+/* ---- A4-A7: dictionary projector ----------------------------------------
+ * Replaces, per dictionary chunk, indexing.py:117-143 — qu_apply
+ * (quaternions.py:186-213), MasterPattern.interpolate (master_pattern.py:
+ * 141-209: rosca_lambert_side_by_side sphere.py:145-185 then bilinear
+ * grid_sample, align_corners=False, padding_mode="border"), the signal mask
+ * column select and the row mean subtraction.
+ *
+ * master_pattern: (mp_h, mp_w2) fp32, north | south hemispheres side by side.
+ * rays_soa:       3 x n_pix fp32 unit rays (x row, y row, z row), already
+ *                 masked.
+ * quats:          (n_rows, 4) fp32 orientations.
+ * Outputs (each may be NULL):
+ *   out_f32 (n_rows x ld_f32): zero-mean rows (or raw rows if !subtract_mean)
+ *   out_lp  (n_rows x ld_lp) : those rows scaled to unit L2 norm, in lp_dtype;
+ *                              e4m3 rows are further scaled by 1/out_lp_scale
+ *   out_norm (n_rows)        : L2 norm of the zero-mean row
+ *   out_lp_scale (n_rows)    : e4m3 dequantisation scale (absmax/448) */
+int ebsd_project_dictionary(const float* master_pattern, int mp_h, int mp_w2, const float* rays_soa,
+                            int n_pix, const float* quats, int64_t n_rows, int subtract_mean,
+                            float* out_f32, int64_t ld_f32, void* out_lp, int lp_dtype, int64_t ld_lp,
+                            float* out_norm, float* out_lp_scale, void* stream);
+
+/* ---- A8: pattern preparation ----------------------------------------------
+ * Replaces ExperimentPatterns.get_patterns (experiment_pats.py:318-346:
+ * avg_pool2d binning) and indexing.py:175-187 (mask select, row mean
+ * subtraction). patterns: n_rows images of (height, width) fp32, image i at
+ * patterns + i * pattern_stride. pix_index (n_pix int32 indices into the
+ * binned image, row-major) may be NULL for all binned pixels. Outputs as for
+ * ebsd_project_dictionary. Also used with height = 1 to normalise generic
+ * fp32 rows (PCA-projected rows). */
+int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int height, int width,
+                       int64_t pattern_stride, int binning, const int32_t* pix_index, int n_pix,
+                       int subtract_mean, float* out_f32, int64_t ld_f32, void* out_lp, int lp_dtype,
+                       int64_t ld_lp, float* out_norm, float* out_lp_scale, void* stream);
+
+/* Bilinear sample of the side-by-side master pattern at n points on the
+ * sphere (xyz, n x 3 fp32; normalised first when `normalize`), grid_sample
+ * semantics align_corners=False, padding_mode="border".
+ * Replaces MasterPattern.interpolate (master_pattern.py:141-209). */
+int ebsd_sample_master_pattern(const float* master_pattern, int mp_h, int mp_w2, const float* xyz,
+                               int64_t n, int normalize, float* out, void* stream);
+
+/* b x b average pooling of n images (MasterPattern.bin, master_pattern.py:
+ * 94-113). out: n x (height/b) x (width/b). */
+int ebsd_avg_pool(const float* in, int64_t n, int height, int width, int binning, float* out,
+                  void* stream);
+
+/* ---- A9/A10: pattern x dictionary contraction with streaming top-k ------
+ * Replaces knn_batch (ebsdtorch/utils/knn.py:80-103, `query @ data.t()` then
+ * torch.topk) and the ChunkedKNN running merge (knn.py:219-266). One tcgen05
+ * kernel: TMA-fed smem tiles, FP32 accumulators in TMEM, and an epilogue that
+ * keeps each query's best `n_cand` candidates in registers, so the
+ * similarity matrix never reaches HBM.
+ *
+ * queries_lp: (n_queries_pad x k_pad) lp rows, n_queries_pad % 128 == 0.
+ * dict_lp:    (n_dict_pad x k_pad) lp rows,    n_dict_pad % 256 == 0.
+ * score(q, d) = dot(queries_lp[q], dict_lp[d]) * col_scale[d]
+ *               (col_scale NULL means 1); columns d >= n_dict_valid ignored.
+ * n_cand in {1, 2, 4, 8, 16, 32, 64}. splits: number of dictionary ranges
+ * (0 = automatic, see ebsd_match_auto_splits). Each (query tile, range) writes
+ * its best n_cand (score, index + index_base) per query, sorted descending, to
+ *   part_val/part_idx[(q * part_slots + slot_base + range) * n_cand + j].
+ * part_slots >= slot_base + splits. */
+int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad);
+int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
+                    int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
+                    const float* col_scale, int n_cand, int splits, float* part_val,
+                    int32_t* part_idx, int part_slots, int slot_base, int32_t index_base,
+                    int* d_status, void* stream);
+
+/* ---- A10 (final) + FP32 re-score ------------------------------------------
+ * Replaces ChunkedKNN.retrieve_topk (knn.py:268-287). Per query: merge the
+ * part_slots x n_cand candidate lists, take the best n_rescore by the
+ * approximate score, recompute their exact FP32 scores, optionally merge
+ * with a running result (run_val/run_idx, k_out per query, may be NULL; its
+ * indices must not overlap the new candidates'), and write the best k_out
+ * sorted descending (ties: lower index first; missing entries -inf / -1).
+ *   similarity EBSD_SIM_DOT:    exact = q_f32[q] . d_f32[idx - d_index_base]
+ *                               (n_pix terms), the reference metric (knn.py:96-97)
+ *   similarity EBSD_SIM_COSINE: exact = that dot / (q_norm[q] d_norm[idx - d_index_base])
+ * (candidate indices are global; d_f32/d_norm hold rows d_index_base ..
+ * d_index_base + d_rows - 1; a candidate outside that range is dropped)
+ * With d_f32 == NULL nothing is re-scored and the score is
+ *   approx * (q_lp_scale ? q_lp_scale[q] : 1) * (DOT ? q_norm[q] : 1). */
+#define EBSD_SIM_DOT 0
+#define EBSD_SIM_COSINE 1
+int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
+                       int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
+                       const float* d_f32, int64_t ld_d, int64_t d_index_base, int64_t d_rows,
+                       int n_pix,
+                       const float* q_norm, const float* d_norm, const float* q_lp_scale,
+                       int similarity, int n_rescore,
+                       int k_out, const float* run_val, const int64_t* run_idx, float* out_val,
+                       int64_t* out_idx, void* stream);
+
+/* ---- A11/A12: PCA -------------------------------------------------------------
+ * C (m_valid x n_valid, row stride ldc) = alpha * A B^T (+ C if accumulate),
+ * A (m_pad x k_pad), B (n_pad x k_pad) lp rows, m_pad % 128 == 0,
+ * n_pad % 256 == 0. tcgen05 kernel with a store epilogue. Used for the
+ * covariance (pca_covmat.py:53-91 einsum) and the PCA projections
+ * (indexing.py:401, 421, 452 torch.matmul). */
+int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
+                 int lp_dtype, float alpha, int accumulate, float* C, int64_t ldc, int64_t m_valid,
+                 int64_t n_valid, int* d_status, void* stream);
+
+/* Column means of an (n_rows x n_cols) fp32 matrix (row stride ld). */
+int ebsd_col_mean(const float* X, int64_t n_rows, int n_cols, int64_t ld, float* mean, void* stream);
+
+/* Three-term bf16 split of fp32 data so that one bf16 GEMM over a tripled K
+ * reproduces an FP32-accurate product: x = hi + lo, and
+ *   pattern 0 writes [hi | hi | lo], pattern 1 writes [hi | lo | hi]
+ * (segments of seg_len elements, zero padded). transpose = 0: row r of X
+ * (minus shift, if not NULL, per column) becomes row r of out (n_rows x ld_out,
+ * ld_out >= 3 * seg_len, seg_len >= n_cols). transpose = 1: column c becomes
+ * row c of out (n_cols x ld_out, seg_len >= n_rows). */
+int ebsd_split3_bf16(const float* X, int64_t n_rows, int n_cols, int64_t ld, const float* shift,
+                     int transpose, int pattern, void* out, int64_t ld_out, int64_t seg_len,
+                     void* stream);
+
+/* ---- A14: disorientation angle (measurement) --------------------------------
+ * Replaces disori_angle_laue (laue_fz_misori.py:148-203) for one Laue group:
+ * out[i] = min over Laue operators of the rotation angle of q1[i] q2[i]^-1
+ * (radians). */
+int ebsd_disori_angle(const float* q1, const float* q2, int64_t n, int laue_id, float* out,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* EBSD_B200_H */

@@ -1,0 +1,645 @@
+"""CPU oracle for the dictionary-indexing (DI) hot path.
+
+TEST INFRASTRUCTURE ONLY. This module is the checker: the CUDA product path
+never imports, calls or falls back to it. Only ``tests/``,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` use it.
+
+It is a NumPy restatement of ebsdtorch's DI algorithm (reference package
+``ebsdtorch``), written so that every step can run in float64 (the accuracy
+oracle) or float32 (the timed CPU baseline, mirroring the reference's own CPU
+arithmetic width). Each function names the reference file:line it follows.
+
+Parity pins: ``tests/golden/make_golden.py`` runs the reference itself (exec-
+loaded from its source tree, CPU torch) on small seeded cases and commits the
+inputs and outputs as ``tests/golden/*.npz``; ``tests/test_oracle_golden.py``
+checks this module against every one of those fixtures.
+"""
+
+from __future__ import annotations
+
+import math
+from typing import Optional, Tuple
+
+import numpy as np
+
+# --------------------------------------------------------------------------
+# Laue groups
+# --------------------------------------------------------------------------
+
+# Group orders including inversion, ebsdtorch/s2_and_so3/laue_generators.py:14-51
+LAUE_MULT = {1: 2, 2: 4, 3: 8, 4: 8, 5: 16, 6: 6, 7: 12, 8: 12, 9: 24, 10: 24, 11: 48}
+
+
+def laue_mult(laue_id: int) -> int:
+    """Multiplicity of a Laue group (laue_generators.py:14-51)."""
+    if laue_id not in LAUE_MULT:
+        raise ValueError(f"Laue group {laue_id} is not supported")
+    return LAUE_MULT[laue_id]
+
+
+def _qmul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Hamilton product of (w, x, y, z) quaternions (quaternions.py:60-75)."""
+    aw, ax, ay, az = np.moveaxis(a, -1, 0)
+    bw, bx, by, bz = np.moveaxis(b, -1, 0)
+    return np.stack(
+        (
+            aw * bw - ax * bx - ay * by - az * bz,
+            aw * bx + ax * bw + ay * bz - az * by,
+            aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw,
+        ),
+        axis=-1,
+    )
+
+
+def _rot_quat(axis, angle_deg) -> np.ndarray:
+    axis = np.asarray(axis, dtype=np.float64)
+    axis = axis / np.linalg.norm(axis)
+    h = math.radians(angle_deg) / 2.0
+    return np.concatenate(([math.cos(h)], math.sin(h) * axis))
+
+
+def _close_group(gens) -> np.ndarray:
+    """Closure of a set of rotation quaternions under multiplication (w >= 0)."""
+    elems = [np.array([1.0, 0.0, 0.0, 0.0])]
+
+    def canon(q):
+        q = np.where(np.abs(q) < 1e-12, 0.0, q)
+        if q[0] < 0 or (q[0] == 0 and tuple(-q[1:]) > tuple(q[1:])):
+            q = -q
+        return q
+
+    def known(q):
+        return any(abs(abs(float(np.dot(q, e))) - 1.0) < 1e-9 for e in elems)
+
+    frontier = [canon(g) for g in gens]
+    while frontier:
+        nxt = []
+        for g in frontier:
+            if not known(g):
+                elems.append(g)
+                nxt.append(g)
+        new = []
+        for a in list(elems):
+            for b in nxt:
+                for c in (canon(_qmul(a, b)), canon(_qmul(b, a))):
+                    if not known(c):
+                        new.append(c)
+        frontier = new
+    return np.array(elems)
+
+
+def laue_elements(laue_id: int) -> np.ndarray:
+    """Rotation operators of the 11 Laue groups as (n, 4) float64 quaternions.
+
+    Same groups as ebsdtorch/s2_and_so3/laue_generators.py:54-249, built here
+    by closing each group's generators (hexagonal/trigonal axes: c along z,
+    a along x), so the set, not the row order, is what matches.
+    """
+    z4 = _rot_quat((0, 0, 1), 90)
+    z2 = _rot_quat((0, 0, 1), 180)
+    z3 = _rot_quat((0, 0, 1), 120)
+    z6 = _rot_quat((0, 0, 1), 60)
+    x2 = _rot_quat((1, 0, 0), 180)
+    d3 = _rot_quat((1, 1, 1), 120)
+    gens = {
+        1: [],
+        2: [z2],
+        3: [z2, x2],
+        4: [z4],
+        5: [z4, x2],
+        6: [z3],
+        7: [z3, x2],
+        8: [z6],
+        9: [z6, x2],
+        10: [z2, x2, d3],
+        11: [z4, x2, d3],
+    }[laue_id]
+    g = _close_group(gens)
+    assert len(g) == laue_mult(laue_id) // 2
+    return g
+
+
+# --------------------------------------------------------------------------
+# Cubochoric grid -> quaternions (A1)
+# --------------------------------------------------------------------------
+
+CU_HALF_EDGE = 0.5 * math.pi ** (2.0 / 3.0)
+
+
+def cu2ho(cu: np.ndarray) -> np.ndarray:
+    """Cubochoric -> homochoric (orientations.py:293-349).
+
+    Restates the closed-form Rosca et al. (2014) square-to-sphere step used by
+    the reference: per point, the components are ordered by magnitude
+    (s <= m <= b), the magnitudes are mapped, and the signs of the input are
+    copied back. Works in the dtype of ``cu``.
+    """
+    cu = np.asarray(cu)
+    dt = cu.dtype
+    a = np.abs(cu)
+    order = np.argsort(a, axis=-1, kind="stable")
+    srt = np.take_along_axis(a, order, axis=-1)
+    s, m, b = srt[..., 0], srt[..., 1], srt[..., 2]
+    r2 = dt.type(math.sqrt(2.0))
+    pi = dt.type(math.pi)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t = s * pi / (dt.type(12.0) * m)
+        t = np.where(np.isnan(t), dt.type(0.0), t)
+        c = np.cos(t)
+        fac = (
+            dt.type(2.0 ** (1.0 / 12.0) * 3.0 ** (1.0 / 3.0))
+            * m
+            * np.sqrt(
+                (dt.type(4.0) * b * b * (c - r2) + r2 * m * m * (dt.type(-2.0) * r2 * c + dt.type(3.0)))
+                / (c - r2)
+            )
+            / (dt.type(math.pi ** (1.0 / 3.0)) * b * np.sqrt(r2 - c))
+        )
+        hx = fac * np.sin(t)
+        hy = fac * dt.type(2.0 ** -0.5) * (r2 * c - dt.type(1.0))
+        hz = (
+            dt.type(2.0 * 6.0 ** (1.0 / 3.0)) * b * b * (c - r2)
+            + dt.type(2.0 ** (5.0 / 6.0) * 3.0 ** (1.0 / 3.0)) * m * m * (dt.type(-2.0) * r2 * c + dt.type(3.0))
+        ) / (dt.type(2.0 * math.pi ** (1.0 / 3.0)) * b * (c - r2))
+    hs = np.stack((hx, hy, hz), axis=-1)
+    ho = np.empty_like(hs)
+    np.put_along_axis(ho, order, hs, axis=-1)
+    ho = np.where(np.isnan(ho), dt.type(0.0), ho)
+    return np.copysign(ho, cu)
+
+
+def _omega_from_ho_norm(t: np.ndarray) -> np.ndarray:
+    """Rotation angle w from |h| by solving |h|^3 = 3/4 (w - sin w) (float64).
+
+    The reference fits cos(w/2) with a polynomial (orientations.py:419-517);
+    the oracle instead solves the defining equation with Newton's method to
+    float64 accuracy. w - sin w and 1 - cos w use series / half-angle forms to
+    avoid cancellation near 0.
+    """
+    t = np.asarray(t, dtype=np.float64)
+    g = (4.0 / 3.0) * t**3  # = w - sin w
+    w = np.cbrt(6.0 * g)  # small-angle start
+    w = np.minimum(w, math.pi)
+    for _ in range(40):
+        small = w < 0.25
+        w2 = w * w
+        wms_series = w * w2 / 6.0 * (1 - w2 / 20.0 * (1 - w2 / 42.0 * (1 - w2 / 72.0 * (1 - w2 / 110.0))))
+        wms = np.where(small, wms_series, w - np.sin(w))
+        omc = 2.0 * np.sin(0.5 * w) ** 2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            step = np.where(omc > 0, (wms - g) / omc, 0.0)
+        w_new = np.clip(w - step, 0.0, math.pi)
+        if np.all(np.abs(w_new - w) <= 1e-16 * np.maximum(1.0, w)):
+            w = w_new
+            break
+        w = w_new
+    return w
+
+
+# Reference fp32 polynomial for cos(w/2) in |h|^2 (orientations.py:440-456).
+_HO2AX_FP32_POLY = np.array(
+    [
+        1.0000000000000009e00,
+        -4.9999943403867775e-01,
+        -2.5015165060149020e-02,
+        -3.8120131548551729e-03,
+        -1.2106188330642162e-03,
+        4.9329295993155416e-04,
+        -7.0089385526450620e-04,
+        3.0979774923589078e-04,
+        -7.3023474963298843e-05,
+    ]
+)
+
+
+def ho2qu(ho: np.ndarray, mode: str = "exact") -> np.ndarray:
+    """Homochoric -> unit quaternion (w, x, y, z) (ho2ax orientations.py:419-517
+    followed by ax2qu orientations.py:730-746).
+
+    ``mode="exact"`` (float64): w solved from |h| (see _omega_from_ho_norm).
+    ``mode="fp32poly"``: the reference's float32 polynomial for cos(w/2),
+    evaluated in float32 exactly as the reference sums it.
+    Rotations with |h|^2 < 1e-6 become the identity, as in the reference
+    (orientations.py:511-515).
+    """
+    if mode == "exact":
+        ho = np.asarray(ho, dtype=np.float64)
+        n2 = np.sum(ho * ho, axis=-1)
+        t = np.sqrt(n2)
+        w = _omega_from_ho_norm(t)
+        cw, sw = np.cos(0.5 * w), np.sin(0.5 * w)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            axis = ho / t[..., None]
+    elif mode == "fp32poly":
+        ho = np.asarray(ho, dtype=np.float32)
+        n2 = np.sum(ho * ho, axis=-1, dtype=np.float32)
+        s = np.zeros_like(n2)
+        for i, c in enumerate(_HO2AX_FP32_POLY.astype(np.float32)):
+            s = s + c * n2 ** np.float32(i)
+        w = np.float32(2.0) * np.arccos(np.clip(s, -1.0, 1.0))
+        cw = np.cos(w / np.float32(2.0))
+        sw = np.sin(w / np.float32(2.0))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            axis = ho * (np.float32(1.0) / np.sqrt(n2))[..., None]
+    else:
+        raise ValueError(mode)
+    qu = np.concatenate((cw[..., None], axis * sw[..., None]), axis=-1)
+    ident = np.abs(n2) < 1e-6
+    qu[ident] = np.array([1.0, 0.0, 0.0, 0.0], dtype=qu.dtype)
+    return qu
+
+
+def qu_std(qu: np.ndarray) -> np.ndarray:
+    """Make the real part non-negative (quaternions.py:27-38)."""
+    return np.where(qu[..., 0:1] >= 0, qu, -qu)
+
+
+def cu2qu(cu: np.ndarray, mode: str = "exact") -> np.ndarray:
+    """Cubochoric -> quaternion (orientations.py:1136-1147)."""
+    return ho2qu(cu2ho(cu), mode=mode)
+
+
+def grid_edge_length(laue_id: int, angular_resolution_deg: float) -> int:
+    """Cubochoric edge length for a target resolution (laue_fz_ori.py:540-547).
+
+    The empirical fit and the int truncation are the reference's; they set how
+    many grid points exist, so they are kept identical.
+    """
+    n_so3 = (2 * 131.97049 / (angular_resolution_deg - 0.03732) + 1) ** 3
+    return int((n_so3 / (0.5 * laue_mult(laue_id))) ** (1.0 / 3.0) + 1.0)
+
+
+def cubochoric_axis(edge_length: int, dtype=np.float64) -> np.ndarray:
+    """Per-axis grid coordinates (sampling.py:193-200): edge+1 points spanning
+    [-a/2, a/2], the last dropped. Coordinate i is -a/2 + i * a / edge."""
+    i = np.arange(edge_length, dtype=np.float64)
+    return (-CU_HALF_EDGE + i * (2.0 * CU_HALF_EDGE / edge_length)).astype(dtype)
+
+
+def so3_cubochoric_grid(edge_length: int, mode: str = "exact") -> np.ndarray:
+    """All edge^3 grid quaternions in 'ij' meshgrid order (sampling.py:179-205)."""
+    ax = cubochoric_axis(edge_length, np.float64 if mode == "exact" else np.float32)
+    cu = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), axis=-1).reshape(-1, 3)
+    return qu_std(cu2qu(cu, mode=mode))
+
+
+def ori_in_fz_laue(qu: np.ndarray, laue_id: int) -> np.ndarray:
+    """Orientation fundamental-zone membership, inclusive bounds
+    (laue_fz_ori.py:144-239). ``qu`` must have w >= 0."""
+    w = qu[..., 0]
+    x, y, z = np.abs(qu[..., 1]), np.abs(qu[..., 2]), np.abs(qu[..., 3])
+    r2m1 = math.sqrt(2.0) - 1.0
+    r3 = math.sqrt(3.0)
+    if laue_id == 11:
+        return (np.maximum(np.maximum(x, y), z) <= w * r2m1) & (x + y + z <= w)
+    if laue_id == 10:
+        return x + y + z <= w
+    if laue_id == 9:
+        m, n = np.maximum(x, y), np.minimum(x, y)
+        rot = np.where(m > (2 + r3) * n, m, (r3 / 2) * m + 0.5 * n)
+        return (z <= (2 - r3) * w) & (rot <= w)
+    if laue_id == 8:
+        return z <= (2 - r3) * w
+    if laue_id == 7:
+        rot = np.where(x >= y * r3, x, (r3 / 2) * y + 0.5 * x)
+        return (z <= (1.0 / r3) * w) & (rot <= w)
+    if laue_id == 6:
+        return z <= (1.0 / r3) * w
+    if laue_id == 5:
+        m, n = np.maximum(x, y), np.minimum(x, y)
+        rot = np.where(m > (math.sqrt(2.0) + 1) * n, m, (1 / math.sqrt(2.0)) * (m + n))
+        return (z <= r2m1 * w) & (rot <= w)
+    if laue_id == 4:
+        return z <= r2m1 * w
+    if laue_id == 3:
+        return np.maximum(np.maximum(x, y), z) <= w
+    if laue_id == 2:
+        return z <= w
+    if laue_id == 1:
+        return np.ones(qu.shape[:-1], dtype=bool)
+    raise ValueError(f"Laue group {laue_id} is not supported")
+
+
+def sample_ori_fz_laue_angle(
+    laue_id: int,
+    angular_resolution_deg: float,
+    permutation: Optional[np.ndarray] = None,
+    mode: str = "exact",
+) -> np.ndarray:
+    """FZ dictionary (laue_fz_ori.py:516-557): grid, FZ filter, optional
+    permutation (the reference draws it with torch.randperm on the global CPU
+    generator; the caller passes that permutation in)."""
+    edge = grid_edge_length(laue_id, angular_resolution_deg)
+    q = so3_cubochoric_grid(edge, mode=mode)
+    q = q[ori_in_fz_laue(q, laue_id)]
+    if permutation is not None:
+        q = q[permutation]
+    return q
+
+
+# --------------------------------------------------------------------------
+# Detector geometry (A3)
+# --------------------------------------------------------------------------
+
+
+def bruker_geometry_to_SE3(pc, primary_tilt_deg: float, secondary_tilt_deg: float, detector_shape):
+    """Bruker pattern centre -> detector-to-sample rotation and translation
+    (geometry.py:31-92)."""
+    pcx, pcy, pcz = (float(v) for v in pc)
+    rows, cols = float(detector_shape[0]), float(detector_shape[1])
+    d = math.radians(primary_tilt_deg)
+    sx = math.radians(secondary_tilt_deg)
+    sd, cd, ss, cs = math.sin(d), math.cos(d), math.sin(sx), math.cos(sx)
+    rot = np.array(
+        [
+            [-sd, -ss * cd, cs * cd],
+            [0.0, cs, ss],
+            [-cd, ss * sd, -sd * cs],
+        ]
+    )
+    tx = pcx * cols * ss * cd + pcy * rows * sd + pcz * rows * cs * cd - ss * cd / 2 - sd / 2
+    ty = -cols * pcx * cs + pcz * rows * ss + cs / 2
+    tz = -cols * pcx * ss * sd + pcy * rows * cd - pcz * rows * sd * cs + ss * sd / 2 - cd / 2
+    return rot, np.array([tx, ty, tz])
+
+
+def detector_coords_sample_frame(
+    detector_shape: Tuple[int, int],
+    proj_center=(0.5, 0.5, 0.5),
+    tilts_degrees=(0.0, 70.0, 0.0),
+    binning=(1, 1),
+) -> np.ndarray:
+    """Un-normalised sample-frame coordinates of each (binned) detector pixel,
+    (P, 3) float64, row-major over (i, j) (geometry.py:422-503 with
+    project2sample :282-347; the SE(3) correction is the identity)."""
+    h, w = detector_shape
+    if h % binning[0] or w % binning[1]:
+        raise ValueError("binning must evenly divide the detector shape")
+    bh, bw = h // binning[0], w // binning[1]
+    ii = np.linspace(0.5 * (binning[0] - 1), h - 0.5 * (binning[0] - 1), bh)
+    jj = np.linspace(0.5 * (binning[1] - 1), w - 0.5 * (binning[1] - 1), bw)
+    pix = np.stack(np.meshgrid(ii, jj, indexing="ij"), axis=-1).reshape(-1, 2)
+    rot, t = bruker_geometry_to_SE3(
+        proj_center, tilts_degrees[2] - tilts_degrees[1], tilts_degrees[0], detector_shape
+    )
+    p3 = np.concatenate((pix, np.zeros((pix.shape[0], 1))), axis=-1)
+    return p3 @ rot.T + t
+
+
+def unit_rays(coords: np.ndarray) -> np.ndarray:
+    """Normalise rays (indexing.py:106)."""
+    return coords / np.linalg.norm(coords, axis=-1, keepdims=True)
+
+
+# --------------------------------------------------------------------------
+# Projector (A4-A7)
+# --------------------------------------------------------------------------
+
+
+def qu_apply(qu: np.ndarray, v: np.ndarray) -> np.ndarray:
+    """Rotate vectors by unit quaternions, q (0, v) q* (quaternions.py:186-213).
+    Broadcasts (..., 4) against (..., 3)."""
+    w, x, y, z = (qu[..., i] for i in range(4))
+    vx, vy, vz = v[..., 0], v[..., 1], v[..., 2]
+    # t = 2 (q_vec x v); v' = v + w t + q_vec x t  (same rotation, fewer terms)
+    tx = 2.0 * (y * vz - z * vy)
+    ty = 2.0 * (z * vx - x * vz)
+    tz = 2.0 * (x * vy - y * vx)
+    return np.stack(
+        (
+            vx + w * tx + (y * tz - z * ty),
+            vy + w * ty + (z * tx - x * tz),
+            vz + w * tz + (x * ty - y * tx),
+        ),
+        axis=-1,
+    )
+
+
+def rosca_lambert_side_by_side(p: np.ndarray) -> np.ndarray:
+    """Unit sphere -> side-by-side square Lambert coordinates in [-1, 1]^2
+    (sphere.py:145-185). x in [-1, 0] for z >= 0 (north), [0, 1] for z < 0;
+    y in [-1, 1]. Same branch structure and sign conventions as the reference."""
+    x, y, z = p[..., 0], p[..., 1], p[..., 2]
+    dt = p.dtype.type
+    fac = np.sqrt(np.maximum(dt(2.0) * (dt(1.0) - np.abs(z)), dt(0.0)))
+    cond = np.abs(y) <= np.abs(x)
+    big = np.where(cond, x, y)
+    sml = np.where(cond, y, x)
+    sgn = np.where(big < 0, dt(-1.0), dt(1.0))
+    simple = sgn * fac * dt(2.0 / 8.0**0.5)
+    arct = sgn * fac * np.arctan2(sml * sgn, np.abs(big)) * dt(2.0 * 2.0**0.5 / math.pi)
+    u = np.where(cond, simple, arct)
+    v = np.where(cond, arct, simple)
+    u = u / dt(2.0) - dt(0.5) + np.where(z < 0, dt(1.0), dt(0.0))
+    return np.stack((u, v), axis=-1)
+
+
+def grid_sample_border(img: np.ndarray, uv: np.ndarray) -> np.ndarray:
+    """Bilinear sampling of a (H, W) image at normalised (x, y) in [-1, 1],
+    align_corners=False, padding_mode='border' -- the semantics of
+    torch.nn.functional.grid_sample used by master_pattern.py:197-206.
+    Pixel coordinate = ((c + 1) * size - 1) / 2, clamped to [0, size - 1]."""
+    H, W = img.shape
+    dt = uv.dtype.type
+    fx = ((uv[..., 0] + dt(1.0)) * dt(W) - dt(1.0)) / dt(2.0)
+    fy = ((uv[..., 1] + dt(1.0)) * dt(H) - dt(1.0)) / dt(2.0)
+    fx = np.clip(fx, 0, W - 1)
+    fy = np.clip(fy, 0, H - 1)
+    x0 = np.floor(fx).astype(np.int64)
+    y0 = np.floor(fy).astype(np.int64)
+    tx = (fx - x0).astype(uv.dtype)
+    ty = (fy - y0).astype(uv.dtype)
+    x1 = np.minimum(x0 + 1, W - 1)
+    y1 = np.minimum(y0 + 1, H - 1)
+    im = img.astype(uv.dtype, copy=False)
+    v00 = im[y0, x0]
+    v01 = im[y0, x1]
+    v10 = im[y1, x0]
+    v11 = im[y1, x1]
+    return (v00 * (1 - tx) + v01 * tx) * (1 - ty) + (v10 * (1 - tx) + v11 * tx) * ty
+
+
+def avg_pool(img: np.ndarray, b: int) -> np.ndarray:
+    """b x b average pooling with stride b over the last two axes
+    (torch avg_pool2d, master_pattern.py:94-113, experiment_pats.py:338-341)."""
+    if b == 1:
+        return img
+    *lead, H, W = img.shape
+    Hb, Wb = H // b, W // b
+    v = img[..., : Hb * b, : Wb * b].reshape(*lead, Hb, b, Wb, b)
+    return v.mean(axis=(-3, -1))
+
+
+def project_patterns(master_pattern: np.ndarray, rays: np.ndarray, quats: np.ndarray) -> np.ndarray:
+    """Simulated patterns (n, P): rotate unit rays by each orientation, map to
+    the side-by-side Lambert square and bilinearly sample the (H, 2W) master
+    pattern (indexing.py:117-130, master_pattern.py:141-209)."""
+    rot = qu_apply(quats[:, None, :], rays[None, :, :])
+    uv = rosca_lambert_side_by_side(rot)
+    return grid_sample_border(master_pattern, uv)
+
+
+def zero_mean_rows(x: np.ndarray) -> np.ndarray:
+    """Row mean subtraction (indexing.py:139-143)."""
+    return x - x.mean(axis=-1, keepdims=True)
+
+
+# --------------------------------------------------------------------------
+# Matcher (A9, A10)
+# --------------------------------------------------------------------------
+
+
+def topk_dot(queries: np.ndarray, data: np.ndarray, k: int, chunk: int = 4096):
+    """Top-k by raw dot product, sorted descending (knn.py:80-103 angular,
+    ChunkedKNN merge and retrieve_topk :219-287). Ties resolve to the lower
+    dictionary index. Returns (indices int64 (Q, k), values (Q, k))."""
+    Q = queries.shape[0]
+    best_v = np.full((Q, k), -np.inf, dtype=np.result_type(queries, data))
+    best_i = np.zeros((Q, k), dtype=np.int64)
+    for d0 in range(0, data.shape[0], chunk):
+        blk = data[d0 : d0 + chunk]
+        sim = queries @ blk.T
+        kk = min(k, blk.shape[0])
+        part = np.argpartition(-sim, kk - 1, axis=1)[:, :kk]
+        pv = np.take_along_axis(sim, part, axis=1)
+        allv = np.concatenate((best_v, pv), axis=1)
+        alli = np.concatenate((best_i, part + d0), axis=1)
+        # order by (-value, index) so equal values keep the lower index
+        o = np.lexsort((alli, -allv), axis=1)[:, :k]
+        best_v = np.take_along_axis(allv, o, axis=1)
+        best_i = np.take_along_axis(alli, o, axis=1)
+    return best_i, best_v
+
+
+# --------------------------------------------------------------------------
+# End-to-end plain DI (A1-A13)
+# --------------------------------------------------------------------------
+
+
+def prep_patterns(patterns: np.ndarray, binning: int = 1, mask: Optional[np.ndarray] = None,
+                  subtract_mean: bool = True, dtype=np.float64) -> np.ndarray:
+    """Query preparation (indexing.py:175-187, experiment_pats.py:318-346):
+    bin, flatten, mask, zero-mean."""
+    x = avg_pool(np.asarray(patterns, dtype=dtype), binning)
+    x = x.reshape(x.shape[0], -1)
+    if mask is not None:
+        x = x[:, mask.reshape(-1)]
+    if subtract_mean:
+        x = zero_mean_rows(x)
+    return x
+
+
+def dictionary_rows(master_pattern, rays_unit, quats, mask=None, dtype=np.float64, chunk=2048):
+    """Zero-mean simulated dictionary rows (n, P') in ``dtype``."""
+    mp = np.asarray(master_pattern, dtype=dtype)
+    r = rays_unit.astype(dtype)
+    if mask is not None:
+        r = r[mask.reshape(-1)]
+    out = np.empty((quats.shape[0], r.shape[0]), dtype=dtype)
+    for i in range(0, quats.shape[0], chunk):
+        out[i : i + chunk] = zero_mean_rows(project_patterns(mp, r, quats[i : i + chunk].astype(dtype)))
+    return out
+
+
+def dictionary_index(
+    master_pattern: np.ndarray,
+    laue_id: int,
+    patterns: np.ndarray,
+    detector_shape,
+    proj_center=(0.5, 0.5, 0.5),
+    tilts_degrees=(0.0, 70.0, 0.0),
+    resolution_deg: float = 10.0,
+    permutation: Optional[np.ndarray] = None,
+    top_k: int = 1,
+    mask: Optional[np.ndarray] = None,
+    binning: int = 1,
+    dtype=np.float64,
+    dictionary: Optional[np.ndarray] = None,
+):
+    """Plain DI for one phase (indexing.py:14-211). Returns
+    (orientations (Q, k, 4), metrics (Q, k), indices (Q, k), dictionary (D, 4))."""
+    if dictionary is None:
+        dictionary = sample_ori_fz_laue_angle(laue_id, resolution_deg, permutation)
+    mp = avg_pool(np.asarray(master_pattern, dtype=np.float64), binning)
+    coords = detector_coords_sample_frame(detector_shape, proj_center, tilts_degrees, (binning, binning))
+    rays = unit_rays(coords)
+    d = dictionary_rows(mp, rays, dictionary, mask, dtype)
+    q = prep_patterns(patterns, binning, mask, True, dtype)
+    idx, val = topk_dot(q, d, top_k)
+    return dictionary[idx], val, idx, dictionary
+
+
+# --------------------------------------------------------------------------
+# PCA (A11, A12)
+# --------------------------------------------------------------------------
+
+
+def covariance_chan(rows_iter, n_features: int) -> np.ndarray:
+    """Streaming covariance with Chan/Welford batch updates, float64
+    (pca_covmat.py:53-91 update, :139-147 normalisation by obs - 1)."""
+    mean = np.zeros((1, n_features))
+    agg = np.zeros((n_features, n_features))
+    obs = 0
+    for x in rows_iter:
+        x = np.asarray(x, dtype=np.float64)
+        n = x.shape[0]
+        bmean = x.mean(axis=0, keepdims=True)
+        new_mean = (mean * obs + bmean * n) / (obs + n)
+        agg += (x - mean).T @ (x - new_mean)
+        obs += n
+        mean = new_mean
+    return agg / (obs - 1)
+
+
+def pca_components(cov: np.ndarray, n_components: int, slice_mode: str = "top") -> np.ndarray:
+    """Eigenvectors (ascending eigenvalue, pca_covmat.py:149-158) and the
+    component slice. ``slice_mode="reference"`` reproduces indexing.py:355
+    exactly (``[:, -n : -n + 300]``); ``"top"`` keeps the n leading vectors."""
+    _, vecs = np.linalg.eigh(cov)
+    if slice_mode == "reference":
+        return vecs[:, -n_components : (-n_components + 300)]
+    return vecs[:, -n_components:]
+
+
+# --------------------------------------------------------------------------
+# Disorientation (A14)
+# --------------------------------------------------------------------------
+
+
+def disori_angle(q1: np.ndarray, q2: np.ndarray, laue_id: int) -> np.ndarray:
+    """Disorientation angle (rad) under one Laue group
+    (laue_fz_misori.py:148-203): max |w| over g2 (q1 q2*) g1."""
+    g = laue_elements(laue_id)
+    q2c = q2 * np.array([1.0, -1.0, -1.0, -1.0])
+    mis = _qmul(q1, q2c)
+    best = np.zeros(mis.shape[:-1])
+    for a in g:
+        left = _qmul(np.broadcast_to(a, mis.shape), mis)
+        for b in g:
+            w = np.abs(_qmul(left, np.broadcast_to(b, mis.shape))[..., 0])
+            best = np.maximum(best, w)
+    return 2.0 * np.arccos(np.clip(best, -1.0, 1.0))
+
+
+# --------------------------------------------------------------------------
+# Synthetic data (stands in for the reference's kikuchipy demo data)
+# --------------------------------------------------------------------------
+
+
+def inv_rosca_lambert_north(uv: np.ndarray) -> np.ndarray:
+    """Square [-1, 1]^2 -> northern unit hemisphere (sphere.py:95-142)."""
+    pi = math.pi
+    xa = np.abs(uv[..., 0]) * math.sqrt(pi / 2)
+    ya = np.abs(uv[..., 1]) * math.sqrt(pi / 2)
+    cond = xa >= ya
+    xn = np.where(cond, xa, ya)
+    yn = np.where(cond, ya, xa)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ang = np.where(xn > 0, pi * yn / (4 * xn), 0.0)
+    rr = (2 * xn / pi) * np.sqrt(np.maximum(pi - xn * xn, 0.0))
+    xh, yh = rr * np.cos(ang), rr * np.sin(ang)
+    zo = 1 - 2 * xn * xn / pi
+    xo = np.copysign(np.where(cond, xh, yh), uv[..., 0])
+    yo = np.copysign(np.where(cond, yh, xh), uv[..., 1])
+    return np.stack((xo, yo, zo), axis=-1)

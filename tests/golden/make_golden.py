@@ -1,0 +1,260 @@
+"""Generate golden vectors by running the reference ebsdtorch itself (CPU torch).
+
+Run in a container that holds the reference source tree:
+
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_ROOT]
+
+REFERENCE_ROOT defaults to /root/reference. The reference's
+``ebsdtorch/ebsd/indexing.py`` ends in a module-level demo script that imports
+``kikuchipy`` (absent), so the two DI functions are loaded by executing only
+the file's lines 1-477 into a fresh module; nothing in the reference tree is
+modified. The PCA variant is also loaded with line 355's component slice
+``[:, -n : -n + 300]`` replaced by ``[:, -n:]`` (the "top" slice).
+
+Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
+outputs of one case. The files are small (< 1 MB each) and committed.
+"""
+
+from __future__ import annotations
+
+import contextlib
+import io
+import os
+import sys
+import types
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_reference(root: str):
+    sys.path.insert(0, root)
+    import ebsdtorch  # noqa: F401
+
+    path = os.path.join(root, "ebsdtorch", "ebsd", "indexing.py")
+    with open(path) as f:
+        lines = f.readlines()
+    src = "".join(lines[:477])
+    mod = types.ModuleType("ref_indexing")
+    mod.__file__ = path
+    exec(compile(src, path, "exec"), mod.__dict__)
+    shipped_slice = "pca_matrix = eigenvectors[:, -n_pca_components : (-n_pca_components + 300)]"
+    assert shipped_slice in src
+    mod_top = types.ModuleType("ref_indexing_top")
+    mod_top.__file__ = path
+    exec(compile(src.replace(shipped_slice, "pca_matrix = eigenvectors[:, -n_pca_components:]"), path, "exec"),
+         mod_top.__dict__)
+    return mod, mod_top
+
+
+def smooth_master_pattern(seed: int, n: int) -> torch.Tensor:
+    """Seeded smooth random (n, 2n) side-by-side master pattern."""
+    g = torch.Generator().manual_seed(seed)
+    base = torch.rand((1, 1, 2 * n // 4 + 2, 2 * (2 * n // 4) + 2), generator=g)
+    mp = torch.nn.functional.interpolate(base, size=(n, 2 * n), mode="bicubic", align_corners=True)[0, 0]
+    return mp.contiguous().float()
+
+
+def main(root: str = "/root/reference"):
+    ref_idx, ref_idx_top = load_reference(root)
+    from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+    from ebsdtorch.s2_and_so3.orientations import cu2qu, qu2cu
+    from ebsdtorch.s2_and_so3.sphere import rosca_lambert_side_by_side
+    from ebsdtorch.s2_and_so3.sampling import so3_uniform_quat
+    from ebsdtorch.s2_and_so3.laue_fz_misori import disori_angle_laue
+    from ebsdtorch.ebsd.geometry import EBSDGeometry
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.utils.pca_covmat import OnlineCovMatrix
+    from ebsdtorch.preprocessing.radial_mask import get_radial_mask
+
+    cpu = torch.device("cpu")
+    out = {}
+
+    # ---- A1/A2: FZ grids for all 11 Laue groups (unpermuted) ----
+    grids = {}
+    for laue in range(1, 12):
+        for res in (15.0, 7.5):
+            q = sample_ori_fz_laue_angle(laue, res, cpu, permute=False)
+            grids[f"q_{laue}_{res}"] = q.numpy()
+    # counts of the config-sized dictionaries
+    counts = []
+    for laue, res in ((11, 1.0), (11, 0.9), (11, 0.5), (9, 0.6), (5, 0.9), (10, 2.0), (7, 2.0), (3, 3.0)):
+        q = sample_ori_fz_laue_angle(laue, res, cpu, permute=False)
+        counts.append((laue, res, q.shape[0]))
+        if (laue, res) == (11, 1.0):
+            grids["q_11_1.0"] = q.numpy()
+    grids["counts"] = np.array(counts, dtype=np.float64)
+    # permutation convention: one randperm(n) on the global CPU generator
+    torch.manual_seed(1234)
+    q_perm = sample_ori_fz_laue_angle(11, 7.5, cpu, permute=True)
+    grids["q_11_7.5_perm_seed1234"] = q_perm.numpy()
+    np.savez_compressed(os.path.join(HERE, "grid.npz"), **grids)
+
+    # ---- cu2qu / qu2cu ----
+    g = torch.Generator().manual_seed(7)
+    a = 0.5 * np.pi ** (2 / 3)
+    cu = (torch.rand((4000, 3), generator=g) * 2 - 1) * a
+    np.savez_compressed(os.path.join(HERE, "cu2qu.npz"), cu=cu.numpy(), qu=cu2qu(cu).numpy(),
+                        cu64=cu.double().numpy(), qu64=cu2qu(cu.double()).numpy())
+
+    # ---- A3: detector rays ----
+    rays = {}
+    for name, shape, pc, tilts, b in (
+        ("d60", (60, 60), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0), 1),
+        ("d60b2", (60, 60), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0), 2),
+        ("d5", (5, 5), (0.4221, 0.2179, 0.4954), (0.0, 70.0, 0.0), 1),
+        ("d40x32", (40, 32), (0.45, 0.55, 0.7), (3.0, 68.0, 5.0), 1),
+        ("d128", (128, 128), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0), 1),
+    ):
+        geom = EBSDGeometry(shape, tilts_degrees=tilts, proj_center=pc)
+        with torch.no_grad():
+            r = geom.get_coords_sample_frame(binning=(b, b))
+        rays[name] = r.numpy()
+        rays[name + "_meta"] = np.array([shape[0], shape[1], *pc, *tilts, b], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "rays.npz"), **rays)
+
+    # ---- A5: Lambert side-by-side ----
+    g = torch.Generator().manual_seed(11)
+    v = torch.randn((5000, 3), generator=g)
+    v = v / v.norm(dim=-1, keepdim=True)
+    special = torch.tensor([[0, 0, 1.0], [0, 0, -1.0], [1.0, 0, 0], [0, 1.0, 0], [-1.0, 0, 0], [0, -1.0, 0],
+                            [0.6, 0.8, 0.0], [0.6, -0.8, 0.0], [-0.7071, 0.7071, 0.0]])
+    v = torch.cat((v, special))
+    np.savez_compressed(os.path.join(HERE, "lambert.npz"), xyz=v.numpy(), uv=rosca_lambert_side_by_side(v).numpy())
+
+    # ---- A4-A7: projector ----
+    proj = {}
+    torch.manual_seed(3)
+    mp_t = smooth_master_pattern(5, 33)
+    mp = MasterPattern(mp_t, laue_group=11)
+    quats = so3_uniform_quat(64, cpu)
+    quats = torch.where(quats[:, :1] >= 0, quats, -quats)
+    for b in (1, 2):
+        geom = EBSDGeometry((16, 16), tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.45, 0.6))
+        with torch.no_grad():
+            dc = geom.get_coords_sample_frame(binning=(b, b))
+            dc = dc / dc.norm(dim=-1, keepdim=True)
+            rot = __import__("ebsdtorch.s2_and_so3.quaternions", fromlist=["qu_apply"]).qu_apply(
+                quats[:, None, :], dc[None])
+            sims = mp.interpolate(rot, mode="bilinear", align_corners=False, normalize_coords=False,
+                                  virtual_binning=b).squeeze()
+        mp.master_pattern_binned = None
+        proj[f"sims_b{b}"] = sims.reshape(64, -1).numpy()
+        proj[f"rays_b{b}"] = dc.numpy()
+    proj["master_pattern"] = mp_t.numpy()
+    proj["quats"] = quats.numpy()
+    np.savez_compressed(os.path.join(HERE, "projector.npz"), **proj)
+
+    # ---- A1-A13: end-to-end plain DI ----
+    def make_queries(mp_obj, geom, n, seed, b=1):
+        torch.manual_seed(seed)
+        qq = so3_uniform_quat(n, cpu)
+        with torch.no_grad():
+            dc = geom.get_coords_sample_frame(binning=(1, 1))
+            dc = dc / dc.norm(dim=-1, keepdim=True)
+            from ebsdtorch.s2_and_so3.quaternions import qu_apply
+            pats = mp_obj.interpolate(qu_apply(qq[:, None, :], dc[None]), normalize_coords=False).reshape(
+                n, *geom.detector_shape)
+            pats = pats + 0.02 * torch.randn_like(pats)
+        return qq, pats
+
+    cases = [
+        dict(name="di_a", det=(16, 16), pc=(0.5, 0.5, 0.6), res=10.0, Q=24, k=3, mask=False, b=1,
+             ec=4096, dcs=4096, seed=21),
+        dict(name="di_b", det=(20, 20), pc=(0.45, 0.55, 0.62), res=12.0, Q=17, k=4, mask=True, b=2,
+             ec=5, dcs=7, seed=22),
+        dict(name="di_c", det=(12, 16), pc=(0.5, 0.5, 0.55), res=15.0, Q=9, k=1, mask=False, b=1,
+             ec=4, dcs=16, seed=23),
+    ]
+    for c in cases:
+        torch.manual_seed(c["seed"])
+        mp_t = smooth_master_pattern(c["seed"], 41)
+        mp = MasterPattern(mp_t.clone(), laue_group=11)
+        geom = EBSDGeometry(c["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=c["pc"])
+        qq, pats = make_queries(mp, geom, c["Q"], c["seed"] + 100)
+        exp = ExperimentPatterns(pats.clone())
+        mask = get_radial_mask(tuple(c["det"] if c["b"] == 1 else (c["det"][0] // c["b"], c["det"][1] // c["b"])))\
+            if c["mask"] else None
+        torch.manual_seed(c["seed"] + 1000)
+        with contextlib.redirect_stdout(io.StringIO()):
+            ref_idx.dictionary_index_orientations(
+                mp, geom, exp, signal_mask=mask, experiment_chunk_size=c["ec"],
+                dictionary_resolution_degrees=c["res"], dictionary_chunk_size=c["dcs"], virtual_binning=c["b"],
+                top_k_matches=c["k"], match_dtype=torch.float32, quantized_if_x86=False)
+        quats_k, metrics_k = exp.raw_indexing_results[0]
+        torch.manual_seed(c["seed"] + 1000)
+        dict_q = sample_ori_fz_laue_angle(11, c["res"], cpu, permute=True)
+        np.savez_compressed(
+            os.path.join(HERE, f"{c['name']}.npz"),
+            master_pattern=mp_t.numpy(), patterns=pats.numpy(), true_quats=qq.numpy(),
+            mask=(mask.numpy() if mask is not None else np.zeros(0, bool)),
+            meta=np.array([*c["det"], *c["pc"], c["res"], c["Q"], c["k"], c["b"], c["ec"], c["dcs"],
+                           c["seed"] + 1000], dtype=np.float64),
+            quats=quats_k.numpy(), metrics=metrics_k.numpy(), orientations=exp.orientations.numpy(),
+            best_metrics=exp.best_metrics.numpy(), dictionary=dict_q.numpy(),
+        )
+
+    # the reference's own DI test case (tests/test_di.py:9-48), fp32 matching
+    torch.manual_seed(0)
+    geom = EBSDGeometry(detector_shape=(5, 5), proj_center=(0.4221, 0.2179, 0.4954))
+    mp_t = torch.randn((10, 10), dtype=torch.float32)
+    pats = torch.randn((2, 5, 5), dtype=torch.float32)
+    mp = MasterPattern(mp_t.clone(), laue_group=11)
+    exp = ExperimentPatterns(pats.clone())
+    torch.manual_seed(99)
+    with contextlib.redirect_stdout(io.StringIO()):
+        ref_idx.dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=10.0,
+                                              dictionary_chunk_size=4096, experiment_chunk_size=4096,
+                                              match_dtype=torch.float32, quantized_if_x86=False)
+    np.savez_compressed(os.path.join(HERE, "di_reftest.npz"), master_pattern=mp_t.numpy(), patterns=pats.numpy(),
+                        quats=exp.raw_indexing_results[0][0].numpy(),
+                        metrics=exp.raw_indexing_results[0][1].numpy(), seed=np.array([99]))
+
+    # ---- A11/A12: PCA DI (shipped slice and top slice) ----
+    torch.manual_seed(31)
+    mp_t = smooth_master_pattern(31, 41)
+    geom = EBSDGeometry((16, 16), tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+    mp = MasterPattern(mp_t.clone(), laue_group=11)
+    qq, pats = make_queries(mp, geom, 20, 131)
+    pca = dict(master_pattern=mp_t.numpy(), patterns=pats.numpy(), true_quats=qq.numpy())
+    for tag, mod, ncomp in (("top", ref_idx_top, 40), ("shipped", ref_idx, 40), ("shipped_n100", ref_idx, 100)):
+        exp = ExperimentPatterns(pats.clone())
+        torch.manual_seed(777)
+        with contextlib.redirect_stdout(io.StringIO()):
+            mod.pca_dictionary_index_orientations(
+                MasterPattern(mp_t.clone(), laue_group=11), geom, exp, n_pca_components=ncomp,
+                dictionary_resolution_learn_deg=12.0, dictionary_resolution_index_deg=12.0,
+                dictionary_chunk_size=4096, experiment_chunk_size=4096, top_k_matches=2,
+                match_dtype=torch.float32, quantized_via_ao=False)
+        pca[f"quats_{tag}"] = exp.raw_indexing_results[0][0].numpy()
+        pca[f"metrics_{tag}"] = exp.raw_indexing_results[0][1].numpy()
+    torch.manual_seed(777)
+    pca["dictionary"] = sample_ori_fz_laue_angle(11, 12.0, cpu, permute=True).numpy()
+    np.savez_compressed(os.path.join(HERE, "pca_di.npz"), **pca)
+
+    # ---- A11: covariance ----
+    g = torch.Generator().manual_seed(41)
+    x = torch.randn((300, 24), generator=g) @ torch.randn((24, 24), generator=g) + 3.0
+    cov = OnlineCovMatrix(24)
+    for chunk in torch.split(x, 64):
+        cov(chunk)
+    np.savez_compressed(os.path.join(HERE, "covariance.npz"), x=x.numpy(), cov=cov.get_covmat().numpy())
+
+    # ---- A14: disorientation ----
+    dis = {}
+    torch.manual_seed(51)
+    for laue in (11, 9, 5, 3, 1):
+        q1 = so3_uniform_quat(500, cpu, dtype=torch.float64)
+        q2 = so3_uniform_quat(500, cpu, dtype=torch.float64)
+        dis[f"q1_{laue}"] = q1.numpy()
+        dis[f"q2_{laue}"] = q2.numpy()
+        dis[f"ang_{laue}"] = disori_angle_laue(q1, q2, laue, laue).numpy()
+    np.savez_compressed(os.path.join(HERE, "disori.npz"), **dis)
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main(*sys.argv[1:])

@@ -1,0 +1,133 @@
+"""Pins the CPU oracle against golden vectors produced by the reference
+ebsdtorch itself (tests/golden/make_golden.py). CPU only."""
+
+import numpy as np
+import pytest
+
+from oracle import di_oracle as O
+
+
+def _sign_invariant_maxdiff(a, b):
+    return float(np.minimum(np.abs(a - b).max(-1), np.abs(a + b).max(-1)).max())
+
+
+@pytest.mark.parametrize("laue", range(1, 12))
+@pytest.mark.parametrize("res", [15.0, 7.5])
+def test_grid_sets_match_reference(golden, laue, res):
+    ref = golden("grid")[f"q_{laue}_{res}"]
+    mine = O.sample_ori_fz_laue_angle(laue, res)
+    assert mine.shape == ref.shape
+    # same order; q and -q are the same rotation (matters only at w == 0)
+    assert _sign_invariant_maxdiff(mine.astype(np.float32), ref) < 2e-6
+
+
+def test_grid_counts_match_reference(golden):
+    counts = golden("grid")["counts"]
+    for laue, res, n in counts:
+        if n > 100000:  # large grids are checked on the GPU
+            continue
+        assert O.sample_ori_fz_laue_angle(int(laue), float(res)).shape[0] == int(n)
+
+
+def test_grid_edge_length_rule(golden):
+    # 0.5 deg m-3m: edge 199 -> 328,720 FZ points (count checked on the GPU)
+    assert O.grid_edge_length(11, 0.5) == 199
+    assert O.grid_edge_length(11, 1.0) == 96
+
+
+def test_cu2qu_matches_reference(golden):
+    g = golden("cu2qu")
+    q = O.qu_std(O.cu2qu(g["cu64"]))
+    ref = O.qu_std(g["qu64"])
+    # reference float64 uses a 10-term polynomial (error ~5e-10 in cos(w/2))
+    assert _sign_invariant_maxdiff(q, ref) < 5e-7
+    q32 = O.qu_std(O.cu2qu(g["cu"].astype(np.float64)))
+    assert _sign_invariant_maxdiff(q32, O.qu_std(g["qu"])) < 3e-6
+
+
+def test_cu2qu_fp32_poly_mode(golden):
+    g = golden("cu2qu")
+    q = O.qu_std(O.cu2qu(g["cu"], mode="fp32poly"))
+    assert _sign_invariant_maxdiff(q, O.qu_std(g["qu"])) < 3e-6
+
+
+@pytest.mark.parametrize("name", ["d60", "d60b2", "d5", "d40x32", "d128"])
+def test_detector_rays_match_reference(golden, name):
+    r = golden("rays")
+    m = r[name + "_meta"]
+    shape, pc, tilts, b = (int(m[0]), int(m[1])), m[2:5], m[5:8], int(m[8])
+    mine = O.detector_coords_sample_frame(shape, pc, tilts, (b, b))
+    ref = r[name]
+    assert np.abs(mine - ref).max() <= 2e-7 * np.abs(ref).max() * 10
+
+
+def test_lambert_matches_reference(golden):
+    g = golden("lambert")
+    uv = O.rosca_lambert_side_by_side(g["xyz"].astype(np.float64))
+    assert np.abs(uv - g["uv"]).max() < 5e-7
+
+
+@pytest.mark.parametrize("b", [1, 2])
+def test_projector_matches_reference(golden, b):
+    g = golden("projector")
+    mp = O.avg_pool(g["master_pattern"].astype(np.float64), b)
+    sims = O.project_patterns(mp, g[f"rays_b{b}"].astype(np.float64), g["quats"].astype(np.float64))
+    assert np.abs(sims - g[f"sims_b{b}"]).max() < 5e-5
+
+
+@pytest.mark.parametrize("case", ["di_a", "di_b", "di_c"])
+def test_dictionary_index_matches_reference(golden, case):
+    d = golden(case)
+    m = d["meta"]
+    det, pc, res, k, b = (int(m[0]), int(m[1])), m[2:5], m[5], int(m[7]), int(m[8])
+    mask = d["mask"] if d["mask"].size else None
+    oq, ov, oi, _ = O.dictionary_index(d["master_pattern"], 11, d["patterns"], det, pc, (0, 70, 0), res, top_k=k,
+                                       mask=mask, binning=b, dictionary=d["dictionary"].astype(np.float64))
+    assert np.abs(oq - d["quats"]).max() < 1e-6  # identical dictionary entries, same order
+    assert np.abs(ov - d["metrics"]).max() <= 1e-5 * np.abs(d["metrics"]).max()
+
+
+def test_permuted_dictionary_matches_reference(golden):
+    """The reference dictionary of each DI case equals the oracle grid under
+    the permutation torch.randperm draws from the seeded CPU generator."""
+    import torch
+
+    d = golden("di_a")
+    seed = int(d["meta"][-1])
+    base = O.sample_ori_fz_laue_angle(11, float(d["meta"][5]))
+    torch.manual_seed(seed)
+    perm = torch.randperm(base.shape[0]).numpy()
+    assert np.abs(base[perm] - d["dictionary"]).max() < 2e-6
+
+
+def test_covariance_matches_reference(golden):
+    g = golden("covariance")
+    x = g["x"].astype(np.float64)
+    cov = O.covariance_chan((x[i:i + 64] for i in range(0, x.shape[0], 64)), x.shape[1])
+    assert np.abs(cov - g["cov"]).max() <= 1e-4 * np.abs(g["cov"]).max()
+
+
+def test_pca_shipped_slice_semantics():
+    """indexing.py:355 keeps [:, -n : -n + 300]: none for P >= 300 and n < 300."""
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((400, 400))
+    cov = a @ a.T
+    assert O.pca_components(cov, 100, "reference").shape[1] == 0
+    assert O.pca_components(cov, 350, "reference").shape[1] == 300
+    assert O.pca_components(cov, 100, "top").shape[1] == 100
+    small = a[:25, :25] @ a[:25, :25].T
+    assert O.pca_components(small, 100, "reference").shape[1] == 25
+
+
+@pytest.mark.parametrize("laue", [11, 9, 5, 3, 1])
+def test_disorientation_matches_reference(golden, laue):
+    g = golden("disori")
+    ang = O.disori_angle(g[f"q1_{laue}"], g[f"q2_{laue}"], laue)
+    assert np.abs(ang - g[f"ang_{laue}"]).max() < 1e-6
+
+
+@pytest.mark.parametrize("laue", range(1, 12))
+def test_laue_groups_are_groups(laue):
+    g = O.laue_elements(laue)
+    assert g.shape[0] == O.laue_mult(laue) // 2
+    assert np.allclose(np.linalg.norm(g, axis=1), 1.0)
