@@ -1,0 +1,345 @@
+"""Benchmark: patterns indexed per second, plain dictionary indexing.
+
+Workload (default): 128 x 128 detector (16,384 px), PC (0.5, 0.5, 0.6), 70 deg
+tilt; synthetic 2 x 1001 x 1001 modified-Lambert master pattern; m-3m
+dictionary at 0.5 deg = 328,720 orientations projected on the fly; 262,144
+query patterns (a 512 x 512 map) at mean 100 counts; top-8 per pattern.
+A step is one full dictionary_index_orientations call (grid generation,
+projection, pattern preparation, tensor-core match with streaming top-k,
+FP32 re-score of the best 32 candidates, result write-back). Inputs are far
+larger than L2 (17 GB of patterns, 10.8 GB of bf16 dictionary), so no flush
+is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload full|small] [--precision bf16|fp8]
+
+Multi-GPU (torchrun, one rank per GPU): every rank indexes its own full map
+(replicas, weak scaling, no collective on the data path); the timed region
+is bracketed by barriers and the slowest rank's time is reported.
+--impl reference times the reference algorithm's CPU implementation (the
+NumPy port in oracle/, all host threads) on a bounded sample of the same
+workload and reports the rate extrapolated to the full workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "patterns indexed/s (128^2, 333k dict) vs plain FP32 DI; % within 0.5deg misori"
+UNIT = "patterns/s"
+
+WORKLOADS = {
+    "full": dict(name="plain DI 128x128 px, m-3m 0.5deg dictionary (328,720), 262,144 patterns, top-8",
+                 mp=1001, det=(128, 128), res=0.5, Q=262144, k=8, counts=100.0),
+    "small": dict(name="plain DI 60x60 px, m-3m 1.0deg dictionary (36,829), 4,096 patterns, top-1",
+                  mp=257, det=(60, 60), res=1.0, Q=4096, k=1, counts=200.0),
+}
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return p, "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        mhz, maxmhz, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                mhz.append(float(parts[1].split()[0]))
+                maxmhz = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not mhz:
+            return None
+        return {"sm_mhz": statistics.median(mhz), "sm_max_mhz": maxmhz, "reasons": sorted(reasons),
+                "samples": len(mhz)}
+
+
+def _dist():
+    import torch.distributed as dist
+
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and not dist.is_initialized():
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return dist if dist.is_initialized() else None
+
+
+def _max_over_ranks(x: float, dist, device) -> float:
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU port
+
+
+def cpu_rate(wl, sample_dict=1024, sample_q=256, threads=None):
+    """Reference algorithm on the host cores (oracle NumPy port, float32, all
+    BLAS threads): times projection of `sample_dict` dictionary rows, query
+    preparation of `sample_q` patterns and their dot-product top-k, then
+    extrapolates to the full workload (Q patterns against D rows)."""
+    import numpy as np
+
+    from ebsdtorch_b200.synthetic import random_quaternions, synthetic_master_pattern
+    from oracle import di_oracle as O
+
+    rng = np.random.default_rng(0)
+    mp = synthetic_master_pattern(wl["mp"], seed=0).numpy().astype(np.float32)
+    h, w = wl["det"]
+    rays = O.unit_rays(O.detector_coords_sample_frame((h, w), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0))).astype(np.float32)
+    quats = random_quaternions(sample_dict, 7).numpy()
+    pats = rng.standard_normal((sample_q, h, w)).astype(np.float32)
+    t0 = time.perf_counter()
+    d = O.dictionary_rows(mp, rays, quats, dtype=np.float32, chunk=256)
+    t1 = time.perf_counter()
+    q = O.prep_patterns(pats, dtype=np.float32)
+    t2 = time.perf_counter()
+    O.topk_dot(q, d, wl["k"], chunk=sample_dict)
+    t3 = time.perf_counter()
+    D = {0.5: 328720, 1.0: 36829}[wl["res"]]
+    t_row = (t1 - t0) / sample_dict
+    t_q = (t2 - t1) / sample_q
+    t_pair = (t3 - t2) / (sample_q * sample_dict)
+    total = D * t_row + wl["Q"] * t_q + wl["Q"] * D * t_pair
+    return wl["Q"] / total, (t3 - t0), os.cpu_count() if threads is None else threads
+
+
+def run_reference(args, wl):
+    dist = _dist()
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    rates = []
+    for i in range(args.warmup + args.steps):
+        r, secs, cores = cpu_rate(wl)
+        if i >= args.warmup:
+            rates.append(r)
+    v = statistics.median(rates)
+    sample = (f"{wl['name']}: per step 1,024 dictionary rows projected and 256 patterns matched against them "
+              "(oracle NumPy float32 port), rate extrapolated to the full workload")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": wl["Q"] / v * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl["name"], "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU arm
+
+
+def run_ours(args, wl):
+    import torch
+
+    from ebsdtorch_b200 import _capi, engine, synthetic
+    from ebsdtorch_b200.ebsd import EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations
+
+    dist = _dist()
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    _capi.load()
+
+    mp = MasterPattern(synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev), laue_group=11)
+    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+    truth = synthetic.random_quaternions(wl["Q"], 1000 + rank).to(dev)
+    pats = synthetic.synthetic_patterns(mp.master_pattern, geom, truth, mean_counts=wl["counts"], seed=2000 + rank)
+    exp = ExperimentPatterns(pats)
+    kw = dict(dictionary_resolution_degrees=wl["res"], top_k_matches=wl["k"], match_dtype=torch.float32,
+              precision=args.precision, rescore_k=32)
+
+    def step():
+        torch.manual_seed(0)
+        dictionary_index_orientations(mp, geom, exp, **kw)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    # ---- timed region: patterns resident in HBM ----
+    engine.MATCH_TIMERS = []
+    launches0 = _capi.launch_count
+    with ClockSampler(local) as clocks:
+        _barrier(dist)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+        _barrier(dist)
+    launches = (_capi.launch_count - launches0) // args.steps
+    elapsed = e0.elapsed_time(e1) / 1e3
+    t_max = _max_over_ranks(elapsed, dist, dev)
+    n = args.gpus
+    value = n * wl["Q"] * args.steps / t_max
+    timers = engine.MATCH_TIMERS
+    engine.MATCH_TIMERS = None
+    match_ms = [a.elapsed_time(b) for a, b, _ in timers]
+    match_flops = [f for _, _, f in timers]
+    avg_launch_s = sum(match_ms) / len(match_ms) / 1e3
+    achieved_tflops = (sum(match_flops) / len(match_flops)) / avg_launch_s / 1e12
+    match_share = sum(match_ms) / 1e3 / elapsed
+
+    # accuracy vs the true orientations (reported, cheap)
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+
+    ang = disori_angle_laue(exp.orientations.float().contiguous(), truth, 11, 11)
+    within_half = float((ang < torch.deg2rad(torch.tensor(0.5))).float().mean())
+    median_deg = float(torch.rad2deg(torch.median(ang)))
+
+    # ---- end to end: host (pinned) patterns, H2D + D2H inside the timed region ----
+    e2e = None
+    if not args.no_e2e:
+        try:
+            host = torch.empty(pats.shape, dtype=torch.float32, pin_memory=True)
+            host.copy_(pats)
+            pinned = True
+        except RuntimeError:
+            host = pats.cpu()
+            pinned = False
+        del exp
+        exp_h = ExperimentPatterns(host)
+        torch.cuda.synchronize()
+        _barrier(dist)
+        t0 = time.perf_counter()
+        e2e_steps = max(1, args.steps // 2)
+        for _ in range(e2e_steps):
+            torch.manual_seed(0)
+            dictionary_index_orientations(mp, geom, exp_h, **kw)
+            q_out = exp_h.raw_indexing_results[0][0].cpu()
+            m_out = exp_h.raw_indexing_results[0][1].cpu()
+        torch.cuda.synchronize()
+        _barrier(dist)
+        t_e2e = _max_over_ranks(time.perf_counter() - t0, dist, dev)
+        e2e = {"value": n * wl["Q"] * e2e_steps / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": int(host.numel() * 4),
+               "d2h_bytes_per_step": int(q_out.numel() * 4 + m_out.numel() * 4),
+               "host_memory": "pinned" if pinned else "pageable"}
+        del host, exp_h
+
+    peaks, peak_kind = _peaks()
+    peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    if args.precision == "fp8":
+        peak = 2.0 * peak  # no measured fp8 denominator: twice the measured bf16
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_max / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": args.precision, "data": "synthetic",
+        "config": {"workload": wl["name"], "precision": f"{args.precision} match + FP32 re-score of top-32",
+                   "parallelism": f"replicas x{n} (query maps independent)", "l2": "inputs larger than L2"},
+        "e2e": e2e,
+        "gpu_launches": int(launches * args.steps),
+        "roofline": {"bound": "tensor", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved_tflops / peak, "traffic": None,
+                     "kernel": "k_tc_gemm (match + streaming top-k)",
+                     "peak_source": f"{peak_kind} bf16_tflops_sustained" + (" x2 for fp8" if args.precision == "fp8"
+                                                                             else ""),
+                     "share_of_step": match_share},
+        "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        r, secs, cores = cpu_rate(wl)
+        line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": "1,024 dictionary rows projected + 256 patterns matched (oracle NumPy "
+                                          f"float32 port, {secs:.1f} s), extrapolated to the full workload"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="full")
+    ap.add_argument("--precision", choices=["bf16", "fp8"], default="bf16")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, wl)
+    else:
+        run_ours(args, wl)
+
+
+if __name__ == "__main__":
+    main()

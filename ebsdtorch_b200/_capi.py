@@ -45,6 +45,15 @@ DT_F32, DT_BF16, DT_E4M3 = 0, 1, 2
 SIM_DOT, SIM_COSINE = 0, 1
 DEVICE_TIMEOUT = 0x7001
 
+# kernels launched by one successful call of each entry point
+LAUNCHES_PER_CALL = {
+    "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
+    "ebsd_prep_patterns": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1, "ebsd_match_topk": 1,
+    "ebsd_merge_rescore": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
+    "ebsd_disori_angle": 1,
+}
+launch_count = 0  # running total of kernels launched through call()
+
 _lib = None
 _lock = threading.Lock()
 
@@ -79,8 +88,11 @@ def last_error() -> str:
 
 def call(name: str, *args) -> int:
     """Call an int-status entry point; raise on failure."""
+    global launch_count
     fn = getattr(load(), name)
     rc = fn(*args)
+    if rc == 0:
+        launch_count += LAUNCHES_PER_CALL.get(name, 0)
     if rc > 0:
         raise ValueError(f"{name}: {last_error()}")
     if rc < 0:

@@ -23,6 +23,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
          "-Xptxas", "-warn-spills"]
+# per-file extra flags: the FP64 grid must round like the CPU oracle
+FILE_FLAGS = {"grid.cu": ["-fmad=false"]}
 
 
 def _nvcc() -> str:
@@ -51,7 +53,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
 
     def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc, *ARCH, *FLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj]
+        cmd = [nvcc, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), *extra, "-I", INCLUDE, "-c", src,
+               "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {os.path.basename(src)}:\n{r.stderr}")

@@ -117,14 +117,19 @@ __device__ __forceinline__ bool in_fz(const double q[4], int laue) {
   }
 }
 
+// Grid coordinate i of `edge` along each axis: the edge + 1 points spanning
+// [-a/2, a/2] with the last dropped, i.e. a/2 * (2i - edge) / edge. This form
+// is exactly 0 at i = edge / 2 and exactly antisymmetric, as the reference's
+// symmetric linspace is; the FZ test of 180-degree rotations about in-plane
+// axes (z exactly 0) depends on that. grid.cu is compiled without FMA
+// contraction so the FP64 arithmetic rounds like the CPU oracle.
 __device__ __forceinline__ void grid_point(int64_t i, int edge, double c[3]) {
   const double kHalf = 1.0725146985555127;  // 0.5 * pi^(2/3)
-  const double step = 2.0 * kHalf / (double)edge;
   const int64_t e2 = (int64_t)edge * edge;
   const int ia = (int)(i / e2), ib = (int)((i / edge) % edge), ic = (int)(i % edge);
-  c[0] = -kHalf + ia * step;
-  c[1] = -kHalf + ib * step;
-  c[2] = -kHalf + ic * step;
+  c[0] = kHalf * (double)(2 * ia - edge) / (double)edge;
+  c[1] = kHalf * (double)(2 * ib - edge) / (double)edge;
+  c[2] = kHalf * (double)(2 * ic - edge) / (double)edge;
 }
 
 __global__ void __launch_bounds__(kGridBlock) k_grid_count(int laue, int edge, int64_t n_total,

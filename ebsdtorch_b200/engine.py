@@ -26,6 +26,10 @@ from .kernels import LP_DTYPES, LP_KMULT, LP_TORCH, TILE_D, TILE_Q, RowBuffers, 
 
 MAX_CAND = 64
 
+# When set to a list, Searcher.run appends (start, end, flops) CUDA-event
+# triples around every tensor-core match launch (measurement only).
+MATCH_TIMERS: Optional[list] = None
+
 
 @dataclass
 class SearchConfig:
@@ -174,8 +178,16 @@ class Searcher:
                 splits = kernels.auto_splits(nq_pad, nd_pad)
                 part_val = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.float32, device=dev)
                 part_idx = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.int32, device=dev)
+                timers = MATCH_TIMERS
+                if timers is not None:
+                    ev0 = torch.cuda.Event(enable_timing=True)
+                    ev1 = torch.cuda.Event(enable_timing=True)
+                    ev0.record()
                 kernels.match_topk(q_rows.lp[:nq_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand, splits,
                                    part_val, part_idx, splits, 0, d0, status)
+                if timers is not None:
+                    ev1.record()
+                    timers.append((ev0, ev1, 2.0 * nq * nd * self.n_pix))
                 run = ci > 0
                 kernels.merge_rescore(
                     part_val, part_idx, nq, splits, self.n_cand,

@@ -272,9 +272,11 @@ def grid_edge_length(laue_id: int, angular_resolution_deg: float) -> int:
 
 def cubochoric_axis(edge_length: int, dtype=np.float64) -> np.ndarray:
     """Per-axis grid coordinates (sampling.py:193-200): edge+1 points spanning
-    [-a/2, a/2], the last dropped. Coordinate i is -a/2 + i * a / edge."""
+    [-a/2, a/2], the last dropped. Coordinate i is a/2 * (2i - edge) / edge:
+    exactly 0 at the centre and antisymmetric, like the reference's
+    symmetric linspace (the FZ test of 180-degree rotations needs the exact 0)."""
     i = np.arange(edge_length, dtype=np.float64)
-    return (-CU_HALF_EDGE + i * (2.0 * CU_HALF_EDGE / edge_length)).astype(dtype)
+    return (CU_HALF_EDGE * (2.0 * i - edge_length) / edge_length).astype(dtype)
 
 
 def so3_cubochoric_grid(edge_length: int, mode: str = "exact") -> np.ndarray:
@@ -600,6 +602,33 @@ def pca_components(cov: np.ndarray, n_components: int, slice_mode: str = "top") 
     if slice_mode == "reference":
         return vecs[:, -n_components : (-n_components + 300)]
     return vecs[:, -n_components:]
+
+
+def pca_dictionary_index(
+    master_pattern: np.ndarray,
+    patterns: np.ndarray,
+    detector_shape,
+    proj_center,
+    learn_dictionary: np.ndarray,
+    index_dictionary: np.ndarray,
+    n_components: int,
+    slice_mode: str = "top",
+    top_k: int = 1,
+    tilts_degrees=(0.0, 70.0, 0.0),
+    chunk: int = 4096,
+):
+    """PCA DI for one phase, float64 (indexing.py:214-476): Chan covariance of
+    the zero-mean learn patterns, eigenvectors, slice, projection of the
+    zero-mean dictionary and query rows, top-k by the projected dot.
+    Returns (orientations (Q, k, 4), metrics (Q, k), indices (Q, k))."""
+    rays = unit_rays(detector_coords_sample_frame(detector_shape, proj_center, tilts_degrees))
+    learn = dictionary_rows(master_pattern, rays, learn_dictionary)
+    cov = covariance_chan((learn[i:i + chunk] for i in range(0, learn.shape[0], chunk)), learn.shape[1])
+    V = pca_components(cov, n_components, slice_mode)
+    d = dictionary_rows(master_pattern, rays, index_dictionary) @ V
+    q = prep_patterns(patterns) @ V
+    idx, val = topk_dot(q, d, top_k)
+    return index_dictionary[idx], val, idx
 
 
 # --------------------------------------------------------------------------

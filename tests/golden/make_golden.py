@@ -214,25 +214,31 @@ def main(root: str = "/root/reference"):
                         metrics=exp.raw_indexing_results[0][1].numpy(), seed=np.array([99]))
 
     # ---- A11/A12: PCA DI (shipped slice and top slice) ----
+    # learn on 5 deg (296 orientations > 256 pixels, full-rank covariance),
+    # index on 8 deg; n = 24 (both slices give the top 24 for P < 300) and
+    # n = 100 with the shipped slice (components 57-100).
     torch.manual_seed(31)
     mp_t = smooth_master_pattern(31, 41)
     geom = EBSDGeometry((16, 16), tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
     mp = MasterPattern(mp_t.clone(), laue_group=11)
     qq, pats = make_queries(mp, geom, 20, 131)
-    pca = dict(master_pattern=mp_t.numpy(), patterns=pats.numpy(), true_quats=qq.numpy())
-    for tag, mod, ncomp in (("top", ref_idx_top, 40), ("shipped", ref_idx, 40), ("shipped_n100", ref_idx, 100)):
+    pca = dict(master_pattern=mp_t.numpy(), patterns=pats.numpy(), true_quats=qq.numpy(),
+               meta=np.array([5.0, 8.0, 777], dtype=np.float64))
+    for tag, mod, ncomp in (("top", ref_idx_top, 24), ("shipped", ref_idx, 24), ("shipped_n100", ref_idx, 100)):
         exp = ExperimentPatterns(pats.clone())
         torch.manual_seed(777)
         with contextlib.redirect_stdout(io.StringIO()):
             mod.pca_dictionary_index_orientations(
                 MasterPattern(mp_t.clone(), laue_group=11), geom, exp, n_pca_components=ncomp,
-                dictionary_resolution_learn_deg=12.0, dictionary_resolution_index_deg=12.0,
+                dictionary_resolution_learn_deg=5.0, dictionary_resolution_index_deg=8.0,
                 dictionary_chunk_size=4096, experiment_chunk_size=4096, top_k_matches=2,
                 match_dtype=torch.float32, quantized_via_ao=False)
         pca[f"quats_{tag}"] = exp.raw_indexing_results[0][0].numpy()
         pca[f"metrics_{tag}"] = exp.raw_indexing_results[0][1].numpy()
+        pca[f"ncomp_{tag}"] = np.array([ncomp])
     torch.manual_seed(777)
-    pca["dictionary"] = sample_ori_fz_laue_angle(11, 12.0, cpu, permute=True).numpy()
+    pca["learn_dictionary"] = sample_ori_fz_laue_angle(11, 5.0, cpu, permute=True).numpy()
+    pca["dictionary"] = sample_ori_fz_laue_angle(11, 8.0, cpu, permute=True).numpy()
     np.savez_compressed(os.path.join(HERE, "pca_di.npz"), **pca)
 
     # ---- A11: covariance ----

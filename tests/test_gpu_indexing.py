@@ -103,11 +103,12 @@ def test_cosine_similarity_mode(golden):
     assert np.abs(exp.raw_indexing_results[0][1].cpu().numpy() - rv).max() < 1e-5
 
 
-@pytest.mark.parametrize("tag,ncomp,slice_mode", [("top", 40, "top"), ("shipped", 40, "reference")])
-def test_pca_dictionary_index_matches_reference(golden, tag, ncomp, slice_mode):
-    """PCA DI: top-1 orientations agree with the reference; the metric is the
-    dot of projected patterns (within the tolerance of an eigenvector basis
-    computed by a different covariance summation)."""
+@pytest.mark.parametrize("tag,slice_mode", [("top", "top"), ("shipped", "reference"),
+                                            ("shipped_n100", "reference")])
+def test_pca_dictionary_index_matches_reference(golden, tag, slice_mode):
+    """PCA DI (learn on 5 deg, index on 8 deg) against the reference's output:
+    same dictionary, same top-1 orientations, metric within FP32-class
+    tolerance of the reference's eigenvector basis."""
     from ebsdtorch_b200.ebsd import (EBSDGeometry, ExperimentPatterns, MasterPattern,
                                      pca_dictionary_index_orientations)
 
@@ -116,16 +117,16 @@ def test_pca_dictionary_index_matches_reference(golden, tag, ncomp, slice_mode):
     mp = MasterPattern(torch.from_numpy(d["master_pattern"]), laue_group=11).to(DEV)
     exp = ExperimentPatterns(torch.from_numpy(d["patterns"]).to(DEV))
     torch.manual_seed(777)
-    pca_dictionary_index_orientations(mp, geom, exp, n_pca_components=ncomp,
-                                      dictionary_resolution_learn_deg=12.0, dictionary_resolution_index_deg=12.0,
+    pca_dictionary_index_orientations(mp, geom, exp, n_pca_components=int(d[f"ncomp_{tag}"][0]),
+                                      dictionary_resolution_learn_deg=5.0, dictionary_resolution_index_deg=8.0,
                                       top_k_matches=2, match_dtype=torch.float32, component_slice=slice_mode)
     q = exp.raw_indexing_results[0][0].cpu().numpy()
     assert np.abs(exp.dictionaries[0].cpu().numpy() - d["dictionary"]).max() < 2e-6
     top1 = np.abs(q[:, 0] - d[f"quats_{tag}"][:, 0]).max(-1) < 1e-5
-    assert top1.mean() >= 0.9
-    ref_m = d[f"metrics_{tag}"][:, 0]
-    got = exp.raw_indexing_results[0][1].cpu().numpy()[:, 0]
-    assert np.abs(got[top1] - ref_m[top1]).max() <= 5e-3 * np.abs(ref_m).max()
+    assert top1.mean() == 1.0
+    ref = d[f"metrics_{tag}"]
+    got = exp.raw_indexing_results[0][1].cpu().numpy()
+    assert np.abs(got[:, 0] - ref[:, 0]).max() <= 1e-3 * np.abs(ref).max()
 
 
 def test_pca_shipped_slice_empty_raises(golden):
@@ -159,9 +160,10 @@ def test_argument_errors_are_loud():
         dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=15, virtual_binning=3)
 
 
-def test_synthetic_small_config_accuracy():
-    """Config-0 style synthetic case at reduced size: indexed orientations
-    are within the dictionary resolution of the true ones."""
+def test_synthetic_small_config_parity_and_accuracy():
+    """Config-0 style synthetic case at reduced size: the GPU result equals the
+    exact FP64 oracle DI on the same dictionary and patterns, and the indexed
+    orientations are near the true ones."""
     from ebsdtorch_b200 import synthetic
     from ebsdtorch_b200.ebsd import dictionary_index_orientations
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
@@ -169,5 +171,13 @@ def test_synthetic_small_config_accuracy():
     mp, geom, exp, truth = synthetic.make_case(129, (40, 40), 256, seed=4)
     dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=2.0, top_k_matches=2,
                                   match_dtype=torch.float32)
+    dic = exp.dictionaries[0].cpu().numpy().astype(np.float64)
+    rays = O.unit_rays(O.detector_coords_sample_frame((40, 40), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0)))
+    d = O.dictionary_rows(mp.master_pattern.cpu().numpy(), rays, dic)
+    ri, rv = O.topk_dot(O.prep_patterns(exp.patterns.cpu().numpy()), d, 2)
+    assert (exp.raw_indexing_indices[0].cpu().numpy()[:, 0] == ri[:, 0]).mean() >= 0.99
+    got = exp.raw_indexing_results[0][1].cpu().numpy()
+    assert np.abs(got - rv).max() <= 1e-4 * np.abs(rv).max()
     ang = disori_angle_laue(exp.orientations.float().contiguous(), truth, 11, 11)
-    assert torch.quantile(ang, 0.9).item() < np.deg2rad(3.0)
+    # 2 deg grid on a coarse 40 x 40 detector: nearest grid point ~1-2 deg away
+    assert torch.median(ang).item() < np.deg2rad(4.0)

@@ -133,7 +133,7 @@ def test_projector_row_outputs(lp):
     scale = torch.empty(37, device=DEV)
     kernels.project(mp, rays, quats, RowBuffers(f32=f32, lp=low, lp_dtype=dt, norm=norm, lp_scale=scale))
     ref = O.dictionary_rows(mp.cpu().numpy(), rays64, quats.cpu().numpy().astype(np.float64))
-    assert np.abs(f32.cpu().numpy() - ref).max() < 2e-5
+    assert np.abs(f32.cpu().numpy() - ref).max() < 5e-5
     assert np.allclose(norm.cpu().numpy(), np.linalg.norm(ref, axis=1), rtol=1e-5)
     unit = low.float()[:, :300] * (scale[:, None] if lp == "fp8" else 1.0)
     tol = 2 ** -8 if lp == "bf16" else 2 ** -3

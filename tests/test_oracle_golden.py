@@ -131,3 +131,16 @@ def test_laue_groups_are_groups(laue):
     g = O.laue_elements(laue)
     assert g.shape[0] == O.laue_mult(laue) // 2
     assert np.allclose(np.linalg.norm(g, axis=1), 1.0)
+
+
+@pytest.mark.parametrize("tag", ["top", "shipped", "shipped_n100"])
+def test_pca_dictionary_index_matches_reference(golden, tag):
+    d = golden("pca_di")
+    mode = "top" if tag == "top" else "reference"
+    oq, ov, oi = O.pca_dictionary_index(d["master_pattern"], d["patterns"], (16, 16), (0.5, 0.5, 0.6),
+                                        d["learn_dictionary"].astype(np.float64),
+                                        d["dictionary"].astype(np.float64), int(d[f"ncomp_{tag}"][0]), mode, 2)
+    top1 = np.abs(oq[:, 0] - d[f"quats_{tag}"][:, 0]).max(-1) < 1e-5
+    assert top1.mean() == 1.0
+    ref = d[f"metrics_{tag}"]
+    assert np.abs(ov - ref).max() <= 1e-4 * np.abs(ref).max()
