@@ -43,6 +43,9 @@ WORKLOADS = {
                  mp=1001, det=(128, 128), res=0.5, Q=262144, k=8, counts=100.0),
     "small": dict(name="plain DI 60x60 px, m-3m 1.0deg dictionary (36,829), 4,096 patterns, top-1",
                   mp=257, det=(60, 60), res=1.0, Q=4096, k=1, counts=200.0),
+    # profiling case: the full-size kernels' shapes at a few GB of device memory
+    "profile": dict(name="plain DI 128x128 px, m-3m 1.0deg dictionary (36,829), 8,192 patterns, top-8",
+                    mp=1001, det=(128, 128), res=1.0, Q=8192, k=8, counts=100.0),
 }
 
 
@@ -197,6 +200,68 @@ def run_reference(args, wl):
 # ---------------------------------------------------------------- GPU arm
 
 
+def _reference_rows_torch(mp, rays, quats):
+    """Dictionary rows exactly as the reference builds them, in torch eager
+    ops: qu_apply (quaternions.py:186-213), rosca_lambert_side_by_side
+    (sphere.py:145-185), grid_sample bilinear / border / align_corners=False
+    (master_pattern.py:197-206), row mean subtraction (indexing.py:139-143)."""
+    import math
+
+    import torch
+
+    w, x, y, z = (quats[:, None, i] for i in range(4))
+    vx, vy, vz = rays[0][None], rays[1][None], rays[2][None]
+    iw = w - x * vx - y * vy - z * vz
+    ix = w * vx + x + y * vz - z * vy
+    iy = w * vy - x * vz + y + z * vx
+    iz = w * vz + x * vy - y * vx + z
+    ox = -iw * x + ix * w - iy * z + iz * y
+    oy = -iw * y + ix * z + iy * w - iz * x
+    oz = -iw * z - ix * y + iy * x + iz * w
+    fac = torch.sqrt(torch.clamp(2.0 * (1.0 - oz.abs()), min=0.0))
+    cond = oy.abs() <= ox.abs()
+    big, sml = torch.where(cond, ox, oy), torch.where(cond, oy, ox)
+    sgn = torch.where(big < 0, -1.0, 1.0)
+    simple = sgn * fac * (2.0 / 8.0 ** 0.5)
+    arct = sgn * fac * torch.atan2(sml * sgn, big.abs()) * (2.0 * 2.0 ** 0.5 / math.pi)
+    u = torch.where(cond, simple, arct) / 2.0 - 0.5 + torch.where(oz < 0, 1.0, 0.0)
+    v = torch.where(cond, arct, simple)
+    grid = torch.stack((u, v), dim=-1)[None]
+    out = torch.nn.functional.grid_sample(mp[None, None], grid, mode="bilinear", padding_mode="border",
+                                          align_corners=False)[0, 0]
+    return out - out.mean(dim=-1, keepdim=True)
+
+
+def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192):
+    """The reference's plain FP32 DI loop on the GPU (torch eager, TF32 off):
+    per dictionary chunk, project it, then query @ chunk.T in FP32, chunk
+    top-k and a running top-k merge (knn.py:80-103, 219-266). Returns
+    (indices (Q, k), seconds spent projecting, seconds spent matching)."""
+    import torch
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    Q = queries_f32.shape[0]
+    best_v = torch.full((Q, k), -float("inf"), device=queries_f32.device)
+    best_i = torch.zeros((Q, k), dtype=torch.int64, device=queries_f32.device)
+    t_proj = t_match = 0.0
+    for d0 in range(0, dictionary.shape[0], chunk):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rows = _reference_rows_torch(mp, rays, dictionary[d0:d0 + chunk])
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        sim = queries_f32 @ rows.t()
+        v, i = torch.topk(sim, min(k, rows.shape[0]), dim=1, largest=True, sorted=False)
+        allv, alli = torch.cat((best_v, v), 1), torch.cat((best_i, i + d0), 1)
+        sel = torch.topk(allv, k, dim=1, largest=True, sorted=False)[1]
+        best_v, best_i = torch.gather(allv, 1, sel), torch.gather(alli, 1, sel)
+        torch.cuda.synchronize()
+        t_proj += t1 - t0
+        t_match += time.perf_counter() - t1
+    order = torch.topk(best_v, k, dim=1, largest=True, sorted=True)[1]
+    return torch.gather(best_i, 1, order), t_proj, t_match
+
+
 def run_ours(args, wl):
     import torch
 
@@ -260,6 +325,32 @@ def run_ours(args, wl):
     within_half = float((ang < torch.deg2rad(torch.tensor(0.5))).float().mean())
     median_deg = float(torch.rad2deg(torch.median(ang)))
 
+    # plain FP32 GPU DI (the reference algorithm in torch eager) on a query
+    # subset: agreement of our top-1 with it, and its extrapolated rate
+    fp32_cmp = None
+    if not args.no_fp32_compare:
+        from ebsdtorch_b200 import kernels
+        from ebsdtorch_b200.ebsd.indexing import _unit_rays_soa
+        from ebsdtorch_b200.kernels import RowBuffers
+
+        n_sub = min(wl["Q"], args.fp32_subset)
+        ori = exp.dictionaries[0]
+        rays = _unit_rays_soa(geom, 1, None, dev)
+        q_sub = torch.empty((n_sub, rays.shape[1]), dtype=torch.float32, device=dev)
+        kernels.prep_patterns(pats[:n_sub], RowBuffers(f32=q_sub))
+        ref_idx, t_proj, t_match = plain_fp32_gpu_di(wl, mp.master_pattern, rays, ori, q_sub, 1)
+        ours = exp.raw_indexing_results[0][0][:n_sub, 0].float().contiguous()
+        theirs = ori[ref_idx[:, 0]].contiguous()
+        a = disori_angle_laue(ours, theirs, 11, 11)
+        agree = float((a < torch.deg2rad(torch.tensor(0.5))).float().mean())
+        same_idx = float((exp.raw_indexing_indices[0][:n_sub, 0] == ref_idx[:, 0]).float().mean())
+        fp32_rate = wl["Q"] / (t_proj + t_match * wl["Q"] / n_sub)
+        fp32_cmp = {"within_0.5deg_of_plain_fp32_di": agree, "same_top1_index": same_idx, "subset": n_sub,
+                    "plain_fp32_gpu_di_rate": fp32_rate, "speedup_vs_plain_fp32_gpu_di": value / n / fp32_rate,
+                    "how": "reference algorithm restated in torch eager ops (FP32, TF32 off), dictionary chunks "
+                           "of 8192, timed on the same GPU for a query subset and extrapolated"}
+        del q_sub
+
     # ---- end to end: host (pinned) patterns, H2D + D2H inside the timed region ----
     e2e = None
     if not args.no_e2e:
@@ -310,6 +401,7 @@ def run_ours(args, wl):
                                                                              else ""),
                      "share_of_step": match_share},
         "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
+        "plain_fp32_di": fp32_cmp,
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -333,6 +425,8 @@ def main():
     ap.add_argument("--precision", choices=["bf16", "fp8"], default="bf16")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32-compare", action="store_true")
+    ap.add_argument("--fp32-subset", type=int, default=4096)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -1,0 +1,50 @@
+"""The C-ABI library builds for sm_100a, loads without a GPU, and exports every
+function declared in include/ebsd_b200.h with the binding's signature. CPU only:
+no compute entry point is called here."""
+
+import os
+import re
+
+from ebsdtorch_b200 import _capi
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "ebsd_b200.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ebsd_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    assert "ebsd_match_topk" in names and "ebsd_project_dictionary" in names
+    assert len(names) >= 19
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _capi.load()
+    for name in _declared():
+        assert hasattr(lib, name), name
+
+
+def test_bindings_cover_header():
+    assert set(_declared()) == set(_capi.SIGNATURES)
+
+
+def test_version_and_error_channel():
+    lib = _capi.load()
+    assert lib.ebsd_version() >= 100
+    assert isinstance(_capi.last_error(), str)
+
+
+def test_argument_errors_need_no_gpu():
+    """Argument checks run on the host before any CUDA call."""
+    import pytest
+
+    with pytest.raises(ValueError, match="Laue group"):
+        _capi.call("ebsd_grid_fz_count", 12, 10, 1, 1 << 20, 1, None)
+    with pytest.raises(ValueError, match="n_cand|multiple"):
+        _capi.call("ebsd_match_topk", 16, 100, 16, 256, 256, 64, _capi.DT_BF16, None, 8, 1, 16, 16, 1, 0, 0, 16,
+                   None)
+    assert _capi.load().ebsd_grid_workspace_bytes(199) > 199**3 // 1024 * 12
