@@ -39,6 +39,7 @@ SIGNATURES = {
     "ebsd_col_mean": (i32, [vp, i64, i32, i64, vp, vp]),
     "ebsd_split3_bf16": (i32, [vp, i64, i32, i64, vp, i32, i32, vp, i64, i64, vp]),
     "ebsd_disori_angle": (i32, [vp, vp, i64, i32, vp, vp]),
+    "ebsd_match_topk_noalloc": (i32, [vp, i64, i64, vp, i64, i64, i64, i32, vp, vp, i32, vp, vp, vp, vp]),
 }
 
 DT_F32, DT_BF16, DT_E4M3 = 0, 1, 2
@@ -50,7 +51,7 @@ LAUNCHES_PER_CALL = {
     "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
     "ebsd_prep_patterns": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1, "ebsd_match_topk": 1,
     "ebsd_merge_rescore": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
-    "ebsd_disori_angle": 1,
+    "ebsd_disori_angle": 1, "ebsd_match_topk_noalloc": 2,
 }
 launch_count = 0  # running total of kernels launched through call()
 

@@ -177,6 +177,32 @@ int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n
                        int k_out, const float* run_val, const int64_t* run_idx, float* out_val,
                        int64_t* out_idx, void* stream);
 
+/* ---- allocation-free match ------------------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that
+ * cannot call cudaMalloc where they index patterns -- e.g. a detector
+ * acquisition callback that must never block (cudaMalloc / cudaFree can
+ * synchronise the device), or a host application that owns all device memory
+ * and forbids its plugins to allocate. Same result as ebsd_match_topk followed
+ * by ebsd_merge_rescore without re-scoring: per query the best k_out
+ * (1..64) candidates by dot(queries_lp[q], dict_lp[d]) * col_scale[d] *
+ * (q_scale ? q_scale[q] : 1), sorted descending, into out_val / out_idx
+ * (n_queries x k_out); if out_status is not NULL the device status word
+ * (0 or EBSD_DEVICE_TIMEOUT) is copied there.
+ * The candidate-list scratch is a fixed 32 MiB device array inside the library
+ * (held by every GPU that loads it until the process exits), so
+ * n_queries_pad * next_pow2(k_out) * 8 bytes must not exceed 32 MiB - 256 B;
+ * larger calls are rejected with EBSD_ERR_ARG. No cudaMalloc, cudaFree or
+ * allocating library routine is called. The first call on each device looks
+ * up the array's device address (cudaGetSymbolAddress, with that device
+ * current); make that first call before any stream capture. All calls share
+ * the array and it keeps the last call's contents: calls that overlap on the
+ * GPU race and must be serialised by the caller. */
+int ebsd_match_topk_noalloc(const void* queries_lp, int64_t n_queries, int64_t n_queries_pad,
+                            const void* dict_lp, int64_t n_dict_pad, int64_t n_dict_valid,
+                            int64_t k_pad, int lp_dtype, const float* col_scale,
+                            const float* q_scale, int k_out, float* out_val, int64_t* out_idx,
+                            int* out_status, void* stream);
+
 /* ---- A11/A12: PCA -------------------------------------------------------------
  * C (m_valid x n_valid, row stride ldc) = alpha * A B^T (+ C if accumulate),
  * A (m_pad x k_pad), B (n_pad x k_pad) lp rows, m_pad % 128 == 0,
