@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     uint32_t acc_phase = 0;
     bool ok = true;
     for (int n = n_begin; n < n_end; ++n) {
-      bool got = mbar_wait(accf_bar(acc), acc_phase, abort_flag);
+      bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag);
       got = __all_sync(0xffffffffu, got);
       if (!got) {
         ok = false;
@@ -441,15 +441,17 @@ static int check_operands(const void* A, int64_t m_pad, const void* B, int64_t n
 using namespace ebsd;
 
 extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
-  const int m_tiles = (int)std::max<int64_t>(1, n_queries_pad / BM);
-  const int n_tiles = (int)std::max<int64_t>(1, n_dict_pad / BN);
-  const int sms = device_sm_count();
-  // Enough units for ~4 waves, and at least 8 dictionary ranges when the
-  // query side is large, so concurrently running units share B tiles in L2.
-  int splits = (int)((4LL * sms + m_tiles - 1) / m_tiles);
-  splits = std::max(splits, 8);
+  // One wave: query tiles x dictionary ranges ~= number of SMs, so all units
+  // start and finish together. Measured on B200 at 128^2 px x 328,720 rows:
+  // one-wave shapes with 16-37 query tiles x 4-9 ranges run at ~1.26 PFLOP/s
+  // and ~1.3 GHz under the power cap; multi-wave or 1-range shapes that keep
+  // many more operand tiles in flight settle at 0.68-1.1 PFLOP/s.
+  const int64_t m_tiles = std::max<int64_t>(1, n_queries_pad / BM);
+  const int64_t n_tiles = std::max<int64_t>(1, n_dict_pad / BN);
+  const int64_t sms = device_sm_count();
+  int64_t splits = std::max<int64_t>(1, sms / m_tiles);
   splits = std::min(splits, n_tiles);
-  return std::max(splits, 1);
+  return (int)splits;
 }
 
 extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,

@@ -25,6 +25,7 @@ from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT
 from .kernels import LP_DTYPES, LP_KMULT, LP_TORCH, TILE_D, TILE_Q, RowBuffers, round_up
 
 MAX_CAND = 64
+MAX_MERGE_CANDIDATES = 4096  # per query, ebsd_merge_rescore's limit
 
 # When set to a list, Searcher.run appends (start, end, flops) CUDA-event
 # triples around every tensor-core match launch (measurement only).
@@ -94,6 +95,14 @@ def _col_scale(rows: RowSet, similarity: str) -> Optional[torch.Tensor]:
     return rows.lp_scale
 
 
+def wave_query_tiles(device) -> int:
+    """Query tiles per match launch: a quarter of the SMs, so that with the
+    automatic dictionary ranges (SMs / tiles, i.e. 4) one launch is exactly one
+    wave of one-CTA-per-SM units (37 tiles x 4 ranges on a 148-SM B200)."""
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    return max(1, sms // 4)
+
+
 def default_budget(device) -> int:
     free, _ = torch.cuda.mem_get_info(device)
     return int(free * 0.9)
@@ -129,8 +138,7 @@ class Searcher:
         budget = self.cfg.workspace_bytes or default_budget(self.device)
         drow = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
         qrow_base = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
-        max_splits = 64
-        qrow = qrow_base + max_splits * self.n_cand * 8 + self.k * 12
+        qrow = qrow_base + self.k * 12
         q_min = min(round_up(self.n_queries, TILE_Q), 16384)
         if self.cfg.dict_chunk:
             dchunk = round_up(self.cfg.dict_chunk, TILE_D)
@@ -159,6 +167,12 @@ class Searcher:
         dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
         qc = self.query_chunk
         q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.rescore, dev)
+        # match launches cover one wave of (query tile, dictionary range) units
+        qm = wave_query_tiles(dev) * TILE_Q
+        max_splits = max(1, torch.cuda.get_device_properties(dev).multi_processor_count)
+        part_val = torch.empty((min(qm, round_up(qc, TILE_Q)) * max_splits * self.n_cand,), dtype=torch.float32,
+                               device=dev)
+        part_idx = torch.empty(part_val.shape, dtype=torch.int32, device=dev)
         n_dchunks = (D + self.dict_chunk - 1) // self.dict_chunk
         for ci, d0 in enumerate(range(0, D, self.dict_chunk)):
             d1 = min(D, d0 + self.dict_chunk)
@@ -173,30 +187,33 @@ class Searcher:
             for q0 in range(0, Q, qc):
                 q1 = min(Q, q0 + qc)
                 nq = q1 - q0
-                nq_pad = round_up(nq, TILE_Q)
                 fill_queries(q0, q1, q_rows.buffers(0, nq))
-                splits = kernels.auto_splits(nq_pad, nd_pad)
-                part_val = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.float32, device=dev)
-                part_idx = torch.empty((nq_pad, splits, self.n_cand), dtype=torch.int32, device=dev)
-                timers = MATCH_TIMERS
-                if timers is not None:
-                    ev0 = torch.cuda.Event(enable_timing=True)
-                    ev1 = torch.cuda.Event(enable_timing=True)
-                    ev0.record()
-                kernels.match_topk(q_rows.lp[:nq_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand, splits,
-                                   part_val, part_idx, splits, 0, d0, status)
-                if timers is not None:
-                    ev1.record()
-                    timers.append((ev0, ev1, 2.0 * nq * nd * self.n_pix))
-                run = ci > 0
-                kernels.merge_rescore(
-                    part_val, part_idx, nq, splits, self.n_cand,
-                    q_rows.f32[:nq] if self.rescore else None,
-                    dict_rows.f32[:nd] if self.rescore else None, d0,
-                    self.n_pix, q_rows.norm, dict_rows.norm, q_rows.lp_scale, self.sim,
-                    min(self.n_rescore, splits * self.n_cand), k,
-                    out_val[q0:q1] if run else None, out_idx[q0:q1] if run else None,
-                    out_val[q0:q1], out_idx[q0:q1])
+                for s0 in range(0, nq, qm):
+                    s1 = min(nq, s0 + qm)
+                    ns = s1 - s0
+                    ns_pad = round_up(ns, TILE_Q)
+                    splits = min(kernels.auto_splits(ns_pad, nd_pad), MAX_MERGE_CANDIDATES // self.n_cand)
+                    timers = MATCH_TIMERS
+                    if timers is not None:
+                        ev0 = torch.cuda.Event(enable_timing=True)
+                        ev1 = torch.cuda.Event(enable_timing=True)
+                        ev0.record()
+                    kernels.match_topk(q_rows.lp[s0:s0 + ns_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand,
+                                       splits, part_val, part_idx, splits, 0, d0, status)
+                    if timers is not None:
+                        ev1.record()
+                        timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))
+                    run = ci > 0
+                    g0, g1 = q0 + s0, q0 + s1
+                    kernels.merge_rescore(
+                        part_val, part_idx, ns, splits, self.n_cand,
+                        q_rows.f32[s0:s1] if self.rescore else None,
+                        dict_rows.f32[:nd] if self.rescore else None, d0,
+                        self.n_pix, q_rows.norm[s0:], dict_rows.norm,
+                        q_rows.lp_scale[s0:] if q_rows.lp_scale is not None else None, self.sim,
+                        min(self.n_rescore, splits * self.n_cand), k,
+                        out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
+                        out_val[g0:g1], out_idx[g0:g1])
         st = int(status.item())
         if st != 0:
             code = "device wait timed out" if st == DEVICE_TIMEOUT else f"status {st:#x}"
