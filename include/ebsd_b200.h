@@ -234,6 +234,38 @@ int ebsd_split3_bf16(const float* X, int64_t n_rows, int n_cols, int64_t ld, con
 int ebsd_disori_angle(const float* q1, const float* q2, int64_t n, int laue_id, float* out,
                       void* stream);
 
+/* ---- A15: 6-D rotation representation and the learned proposal ------------
+ * 6-D (Zhou et al.) -> quaternion (orientations.py:986-1005 zh2qu: Gram-Schmidt
+ * rows b1, b2, b3 then om2qu), optional rotation matrices (n x 9). */
+int ebsd_zh_to_qu(const float* zh, int64_t n, float* out_qu, float* out_om, void* stream);
+/* quaternion -> 6-D, the first two matrix rows (orientations.py:1008-1020). */
+int ebsd_qu_to_zh(const float* qu, int64_t n, float* out_zh, void* stream);
+/* Training objective of the orientation-proposal network (no counterpart in
+ * the reference): loss[i] = min over the Laue operators g of
+ * ||zh2om(zh[i]) - om(q_true[i] g)||_F^2 and grad = grad_scale * dloss/dzh. */
+int ebsd_rot6d_sym_loss(const float* zh, const float* q_true, int64_t n, int laue_id, float grad_scale,
+                        float* out_loss, float* out_grad, void* stream);
+
+/* CNN building blocks (3x3 / stride 2 / pad 1 convolutions on NHWC bf16
+ * activations as im2col + ebsd_gemm_nt; FP32 dense head; Adam). */
+int ebsd_cnn_im2col(const void* x, int B, int H, int W, int C, int64_t m_pad, int ld, void* cols, void* stream);
+int ebsd_cnn_col2im(const float* dcols, int64_t ld, int B, int H, int W, int C, float* dx, void* stream);
+int ebsd_cnn_bias_act(const float* y, int64_t ldy, const float* bias, int64_t M, int C, int relu, void* out,
+                      int64_t ld_out, float* out32, void* stream);
+int ebsd_cnn_relu_grad(const float* dy, int64_t ldy, const void* act, int64_t lda, int64_t M, int C, float* g32,
+                       void* g16, int64_t ld_out, void* stream);
+int ebsd_cnn_col_sum(const float* g, int64_t M, int C, float* db, void* stream);
+int ebsd_cnn_transpose(const void* in, int in_is_f32, int64_t rows, int64_t cols, int64_t ld_in, void* out,
+                       int64_t out_rows, int64_t ld_out, void* stream);
+int ebsd_cnn_scale_cast(const float* x, int64_t n, float scale, void* out, void* stream);
+int ebsd_cnn_dense_fwd(const float* x, int64_t ldx, const float* w, const float* b, int M, int N, int K, int relu,
+                       float* y, void* y16, void* stream);
+int ebsd_cnn_dense_bwd(const float* dy, const float* x, int64_t ldx, const float* w, int M, int N, int K,
+                       float* dw, float* db, float* dx, void* stream);
+int ebsd_cnn_adam(float* w, float* m, float* v, const float* g, int64_t rows, int cols, float lr, float b1,
+                  float b2, float eps, int step, float weight_decay, void* w16, int64_t ld16, void* w16t,
+                  int64_t ld16t, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -652,6 +652,182 @@ def disori_angle(q1: np.ndarray, q2: np.ndarray, laue_id: int) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------
+# 6-D rotation representation (A15)
+# --------------------------------------------------------------------------
+
+
+def zh2om(zh: np.ndarray) -> np.ndarray:
+    """6-D (Zhou et al. 2019) -> rotation matrix with Gram-Schmidt rows
+    b1, b2, b3 (orientations.py:940-963)."""
+    a1, a2 = zh[..., :3], zh[..., 3:]
+    b1 = a1 / np.linalg.norm(a1, axis=-1, keepdims=True)
+    b2 = a2 - np.sum(b1 * a2, axis=-1, keepdims=True) * b1
+    b2 = b2 / np.linalg.norm(b2, axis=-1, keepdims=True)
+    b3 = np.cross(b1, b2)
+    b3 = b3 / np.linalg.norm(b3, axis=-1, keepdims=True)
+    return np.stack((b1, b2, b3), axis=-2)
+
+
+def qu2om(qu: np.ndarray) -> np.ndarray:
+    """Quaternion (w, x, y, z) -> rotation matrix (orientations.py:913-937)."""
+    w, x, y, z = (qu[..., i] for i in range(4))
+    qb = w * w - (x * x + y * y + z * z)
+    m = np.empty(qu.shape[:-1] + (3, 3))
+    m[..., 0, 0] = qb + 2 * x * x
+    m[..., 0, 1] = 2 * (x * y - w * z)
+    m[..., 0, 2] = 2 * (x * z + w * y)
+    m[..., 1, 0] = 2 * (y * x + w * z)
+    m[..., 1, 1] = qb + 2 * y * y
+    m[..., 1, 2] = 2 * (y * z - w * x)
+    m[..., 2, 0] = 2 * (z * x - w * y)
+    m[..., 2, 1] = 2 * (z * y + w * x)
+    m[..., 2, 2] = qb + 2 * z * z
+    return m
+
+
+def om2qu(m: np.ndarray) -> np.ndarray:
+    """Rotation matrix -> quaternion with w >= 0 (orientations.py:52-132):
+    the largest-diagonal branch of Farrell's method, then the axis signs from
+    the antisymmetric part."""
+    m00, m11, m22 = m[..., 0, 0], m[..., 1, 1], m[..., 2, 2]
+    m01, m02, m10, m12, m20, m21 = m[..., 0, 1], m[..., 0, 2], m[..., 1, 0], m[..., 1, 2], m[..., 2, 0], m[..., 2, 1]
+    q = np.empty(m.shape[:-2] + (4,))
+    b1 = (m22 < 0) & (m00 > m11)
+    b2 = (m22 < 0) & ~(m00 > m11)
+    b3 = ~(m22 < 0) & (m00 < -m11)
+    b4 = ~(m22 < 0) & ~(m00 < -m11)
+    for br, t, comp in (
+        (b1, 1 + m00 - m11 - m22, (m12 - m21, None, m01 + m10, m20 + m02)),
+        (b2, 1 - m00 + m11 - m22, (m20 - m02, m01 + m10, None, m12 + m21)),
+        (b3, 1 - m00 - m11 + m22, (m01 - m10, m20 + m02, m12 + m21, None)),
+        (b4, 1 + m00 + m11 + m22, (None, m12 - m21, m20 - m02, m01 - m10)),
+    ):
+        r = 0.5 / np.sqrt(np.where(br, t, 1.0))
+        for i, c in enumerate(comp):
+            val = t * r if c is None else c * r
+            q[..., i] = np.where(br, val, q[..., i])
+    q[..., 0] = np.abs(q[..., 0])
+    q[..., 1] = np.copysign(q[..., 1], m21 - m12)
+    q[..., 2] = np.copysign(q[..., 2], m02 - m20)
+    q[..., 3] = np.copysign(q[..., 3], m10 - m01)
+    return q
+
+
+def zh2qu(zh: np.ndarray) -> np.ndarray:
+    return om2qu(zh2om(zh))
+
+
+def qu2zh(qu: np.ndarray) -> np.ndarray:
+    """First two rows of the rotation matrix (orientations.py:1008-1020)."""
+    return qu2om(qu)[..., :2, :].reshape(qu.shape[:-1] + (6,))
+
+
+def rot6d_sym_loss(zh: np.ndarray, q_true: np.ndarray, laue_id: int):
+    """Per-sample loss min over Laue operators g of ||zh2om(zh) - om(q_true g)||_F^2
+    and its gradient with respect to zh (Gram-Schmidt backward), float64.
+    The CNN head's training objective (a new part: the reference has no
+    learned indexer)."""
+    g = laue_elements(laue_id)
+    R = zh2om(zh)
+    best = np.full(zh.shape[0], np.inf)
+    target = np.zeros_like(R)
+    for op in g:
+        Rt = qu2om(_qmul(q_true, np.broadcast_to(op, q_true.shape)))
+        d = np.sum((R - Rt) ** 2, axis=(-2, -1))
+        sel = d < best
+        best = np.where(sel, d, best)
+        target[sel] = Rt[sel]
+    gR = 2.0 * (R - target)
+    a1, a2 = zh[:, :3], zh[:, 3:]
+    n1 = np.linalg.norm(a1, axis=1, keepdims=True)
+    b1 = a1 / n1
+    u = a2 - np.sum(b1 * a2, axis=1, keepdims=True) * b1
+    n2 = np.linalg.norm(u, axis=1, keepdims=True)
+    b2 = u / n2
+    c = np.cross(b1, b2)
+    nc = np.linalg.norm(c, axis=1, keepdims=True)
+    b3 = c / nc
+    gb1, gb2, gb3 = gR[:, 0], gR[:, 1], gR[:, 2]
+    gc = (gb3 - np.sum(gb3 * b3, axis=1, keepdims=True) * b3) / nc
+    gb1 = gb1 + np.cross(b2, gc)
+    gb2 = gb2 + np.cross(gc, b1)
+    gu = (gb2 - np.sum(gb2 * b2, axis=1, keepdims=True) * b2) / n2
+    gub1 = np.sum(gu * b1, axis=1, keepdims=True)
+    ga2 = gu - gub1 * b1
+    gb1 = gb1 - gub1 * a2 - np.sum(b1 * a2, axis=1, keepdims=True) * gu
+    ga1 = (gb1 - np.sum(gb1 * b1, axis=1, keepdims=True) * b1) / n1
+    return best, np.concatenate((ga1, ga2), axis=1)
+
+
+# --------------------------------------------------------------------------
+# Orientation-proposal CNN (checker for the GPU forward / backward kernels)
+# --------------------------------------------------------------------------
+
+
+def _im2col(x: np.ndarray) -> np.ndarray:
+    """(B, H, W, C) -> (B*Ho*Wo, 9*C) for 3x3 / stride 2 / pad 1, columns
+    ordered (ky, kx, c)."""
+    B, H, W, C = x.shape
+    Ho, Wo = (H + 1) // 2, (W + 1) // 2
+    xp = np.zeros((B, H + 2, W + 2, C), dtype=x.dtype)
+    xp[:, 1:H + 1, 1:W + 1] = x
+    cols = np.empty((B, Ho, Wo, 3, 3, C), dtype=x.dtype)
+    for ky in range(3):
+        for kx in range(3):
+            cols[:, :, :, ky, kx] = xp[:, ky:ky + 2 * Ho:2, kx:kx + 2 * Wo:2]
+    return cols.reshape(B * Ho * Wo, 9 * C)
+
+
+def _col2im(dcols: np.ndarray, shape) -> np.ndarray:
+    B, H, W, C = shape
+    Ho, Wo = (H + 1) // 2, (W + 1) // 2
+    d = dcols.reshape(B, Ho, Wo, 3, 3, C)
+    dxp = np.zeros((B, H + 2, W + 2, C))
+    for ky in range(3):
+        for kx in range(3):
+            dxp[:, ky:ky + 2 * Ho:2, kx:kx + 2 * Wo:2] += d[:, :, :, ky, kx]
+    return dxp[:, 1:H + 1, 1:W + 1]
+
+
+def cnn_forward_backward(params: dict, x: np.ndarray, q_true: np.ndarray, laue_id: int):
+    """FP64 forward + backward of the proposal CNN (ebsdtorch_b200/learned.py
+    layout: conv{i}.w (Cout, 9*Cin) over (ky, kx, cin), conv{i}.b, fc1, fc2).
+    Returns (outputs (B, 6), mean loss, gradients dict)."""
+    B = x.shape[0]
+    a = x.reshape(B, x.shape[1], x.shape[2], 1).astype(np.float64)
+    cache = []
+    i = 0
+    while f"conv{i}.w" in params:
+        w, b = params[f"conv{i}.w"], params[f"conv{i}.b"]
+        cols = _im2col(a)
+        y = cols @ w.T + b
+        out = np.maximum(y, 0.0)
+        Ho, Wo = (a.shape[1] + 1) // 2, (a.shape[2] + 1) // 2
+        cache.append((a.shape, cols, out))
+        a = out.reshape(B, Ho, Wo, w.shape[0])
+        i += 1
+    feat = a.reshape(B, -1)
+    h_pre = feat @ params["fc1.w"].T + params["fc1.b"]
+    h = np.maximum(h_pre, 0.0)
+    z = h @ params["fc2.w"].T + params["fc2.b"]
+    loss, gz = rot6d_sym_loss(z, q_true, laue_id)
+    gz = gz / B
+    grads = {"fc2.w": gz.T @ h, "fc2.b": gz.sum(0)}
+    gh = (gz @ params["fc2.w"]) * (h > 0)
+    grads["fc1.w"], grads["fc1.b"] = gh.T @ feat, gh.sum(0)
+    g = (gh @ params["fc1.w"]).reshape(-1, params[f"conv{i - 1}.w"].shape[0])
+    for j in range(i - 1, -1, -1):
+        shape, cols, out = cache[j]
+        g = g * (out > 0)
+        grads[f"conv{j}.w"] = g.T @ cols
+        grads[f"conv{j}.b"] = g.sum(0)
+        if j > 0:
+            dx = _col2im(g @ params[f"conv{j}.w"], shape)
+            g = dx.reshape(-1, shape[3])
+    return z, float(loss.mean()), grads
+
+
+# --------------------------------------------------------------------------
 # Synthetic data (stands in for the reference's kikuchipy demo data)
 # --------------------------------------------------------------------------
 

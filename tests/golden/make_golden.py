@@ -249,6 +249,16 @@ def main(root: str = "/root/reference"):
         cov(chunk)
     np.savez_compressed(os.path.join(HERE, "covariance.npz"), x=x.numpy(), cov=cov.get_covmat().numpy())
 
+    # ---- A15: 6-D (Zhou) rotation representation ----
+    from ebsdtorch.s2_and_so3.orientations import zh2om, zh2qu, qu2zh, om2qu, qu2om
+    g = torch.Generator().manual_seed(61)
+    zh = torch.randn((3000, 6), generator=g, dtype=torch.float64)
+    qr = so3_uniform_quat(3000, cpu, dtype=torch.float64)
+    qr = torch.where(qr[:, :1] >= 0, qr, -qr)
+    np.savez_compressed(os.path.join(HERE, "rot6d.npz"), zh=zh.numpy(), om=zh2om(zh).numpy(), qu=zh2qu(zh).numpy(),
+                        qu_in=qr.numpy(), zh_out=qu2zh(qr).numpy(), om_out=qu2om(qr).numpy(),
+                        qu_back=om2qu(qu2om(qr)).numpy())
+
     # ---- A14: disorientation ----
     dis = {}
     torch.manual_seed(51)

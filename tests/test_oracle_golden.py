@@ -144,3 +144,60 @@ def test_pca_dictionary_index_matches_reference(golden, tag):
     assert top1.mean() == 1.0
     ref = d[f"metrics_{tag}"]
     assert np.abs(ov - ref).max() <= 1e-4 * np.abs(ref).max()
+
+
+def test_rot6d_conversions_match_reference(golden):
+    g = golden("rot6d")
+    assert np.abs(O.zh2om(g["zh"]) - g["om"]).max() < 1e-12
+    assert _sign_invariant_maxdiff(O.zh2qu(g["zh"]), g["qu"]) < 1e-12
+    assert np.abs(O.qu2zh(g["qu_in"]) - g["zh_out"]).max() < 1e-12
+    assert np.abs(O.qu2om(g["qu_in"]) - g["om_out"]).max() < 1e-12
+    assert _sign_invariant_maxdiff(O.om2qu(O.qu2om(g["qu_in"])), g["qu_back"]) < 1e-12
+
+
+def test_rot6d_sym_loss_gradient_finite_difference():
+    rng = np.random.default_rng(3)
+    zh = rng.standard_normal((40, 6))
+    q = rng.standard_normal((40, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    loss, grad = O.rot6d_sym_loss(zh, q, 11)
+    eps = 1e-6
+    for j in range(6):
+        dz = np.zeros_like(zh)
+        dz[:, j] = eps
+        lp, _ = O.rot6d_sym_loss(zh + dz, q, 11)
+        lm, _ = O.rot6d_sym_loss(zh - dz, q, 11)
+        assert np.allclose((lp - lm) / (2 * eps), grad[:, j], atol=1e-5, rtol=1e-4)
+    # the loss vanishes at any symmetry-equivalent target
+    g = O.laue_elements(11)
+    qt = O._qmul(q, np.broadcast_to(g[5], q.shape))
+    l0, g0 = O.rot6d_sym_loss(O.qu2zh(qt), q, 11)
+    assert np.abs(l0).max() < 1e-20 and np.abs(g0).max() < 1e-9
+
+
+def test_cnn_oracle_gradient_finite_difference():
+    """The FP64 CNN oracle (checker of the GPU CNN kernels) is itself exact."""
+    rng = np.random.default_rng(0)
+    ch = (1, 4, 6)
+    params = {}
+    for i, (a, b) in enumerate(zip(ch[:-1], ch[1:])):
+        params[f"conv{i}.w"] = rng.standard_normal((b, 9 * a)) * np.sqrt(2 / (9 * a))
+        params[f"conv{i}.b"] = rng.standard_normal(b) * 0.1
+    params["fc1.w"] = rng.standard_normal((5, 24)) * 0.3
+    params["fc1.b"] = rng.standard_normal(5) * 0.1
+    params["fc2.w"] = rng.standard_normal((6, 5)) * 0.3
+    params["fc2.b"] = rng.standard_normal(6) * 0.1
+    x = rng.standard_normal((3, 8, 8))
+    q = rng.standard_normal((3, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    _, _, g = O.cnn_forward_backward(params, x, q, 11)
+    eps = 1e-6
+    for k, v in params.items():
+        for _ in range(3):
+            idx = tuple(rng.integers(0, s) for s in v.shape)
+            p2 = {kk: vv.copy() for kk, vv in params.items()}
+            p3 = {kk: vv.copy() for kk, vv in params.items()}
+            p2[k][idx] += eps
+            p3[k][idx] -= eps
+            num = (O.cnn_forward_backward(p2, x, q, 11)[1] - O.cnn_forward_backward(p3, x, q, 11)[1]) / (2 * eps)
+            assert abs(num - g[k][idx]) <= 1e-6 * max(1.0, abs(num))
