@@ -789,10 +789,11 @@ def _col2im(dcols: np.ndarray, shape) -> np.ndarray:
     return dxp[:, 1:H + 1, 1:W + 1]
 
 
-def cnn_forward_backward(params: dict, x: np.ndarray, q_true: np.ndarray, laue_id: int):
+def cnn_forward_backward(params: dict, x: np.ndarray, q_true: np.ndarray, laue_id: int, grad_out=None):
     """FP64 forward + backward of the proposal CNN (ebsdtorch_b200/learned.py
     layout: conv{i}.w (Cout, 9*Cin) over (ky, kx, cin), conv{i}.b, fc1, fc2).
-    Returns (outputs (B, 6), mean loss, gradients dict)."""
+    grad_out, if given, replaces the loss gradient dL/dz (already divided by
+    the batch size). Returns (outputs (B, 6), mean loss, gradients dict)."""
     B = x.shape[0]
     a = x.reshape(B, x.shape[1], x.shape[2], 1).astype(np.float64)
     cache = []
@@ -811,7 +812,7 @@ def cnn_forward_backward(params: dict, x: np.ndarray, q_true: np.ndarray, laue_i
     h = np.maximum(h_pre, 0.0)
     z = h @ params["fc2.w"].T + params["fc2.b"]
     loss, gz = rot6d_sym_loss(z, q_true, laue_id)
-    gz = gz / B
+    gz = gz / B if grad_out is None else grad_out
     grads = {"fc2.w": gz.T @ h, "fc2.b": gz.sum(0)}
     gh = (gz @ params["fc2.w"]) * (h > 0)
     grads["fc1.w"], grads["fc1.b"] = gh.T @ feat, gh.sum(0)
