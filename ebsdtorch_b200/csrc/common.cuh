@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 
@@ -48,6 +49,81 @@ static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStre
 static inline int ceil_div(int64_t a, int64_t b) { return (int)((a + b - 1) / b); }
 
 int device_sm_count();
+
+// ---------------------------------------------------------------------------
+// Laue groups (host): rotation operators as unit quaternions, w >= 0
+// ---------------------------------------------------------------------------
+
+struct LaueTable {
+  float q[24 * 4];
+  int n;
+};
+
+// Rotation operators of each Laue group as closed sets of unit quaternions
+// (the groups of laue_generators.py:54-249), generated on the host.
+static inline void laue_qmul_d(const double* a, const double* b, double* o) {
+  o[0] = a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3];
+  o[1] = a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2];
+  o[2] = a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1];
+  o[3] = a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0];
+}
+
+static inline int build_laue_table(int laue, LaueTable* t) {
+  auto rot = [](double x, double y, double z, double deg, double* q) {
+    const double n = std::sqrt(x * x + y * y + z * z), h = deg * M_PI / 360.0;
+    q[0] = std::cos(h);
+    q[1] = std::sin(h) * x / n;
+    q[2] = std::sin(h) * y / n;
+    q[3] = std::sin(h) * z / n;
+  };
+  double g[3][4];
+  int ng = 0;
+  const int ax[11][3] = {{0, 0, 0}, {1, 0, 0}, {1, 4, 0}, {2, 0, 0}, {2, 4, 0}, {3, 0, 0},
+                         {3, 4, 0}, {5, 0, 0}, {5, 4, 0}, {1, 4, 6}, {2, 4, 6}};
+  // generator codes: 1 z2, 2 z4, 3 z3, 5 z6, 4 x2, 6 <111> 3-fold
+  for (int j = 0; j < 3; ++j) {
+    const int c = ax[laue - 1][j];
+    if (c == 0) continue;
+    switch (c) {
+      case 1: rot(0, 0, 1, 180, g[ng]); break;
+      case 2: rot(0, 0, 1, 90, g[ng]); break;
+      case 3: rot(0, 0, 1, 120, g[ng]); break;
+      case 5: rot(0, 0, 1, 60, g[ng]); break;
+      case 4: rot(1, 0, 0, 180, g[ng]); break;
+      case 6: rot(1, 1, 1, 120, g[ng]); break;
+    }
+    ++ng;
+  }
+  double el[24][4] = {{1, 0, 0, 0}};
+  int n = 1;
+  bool grew = true;
+  while (grew) {
+    grew = false;
+    const int cur = n;
+    for (int i = 0; i < cur; ++i)
+      for (int k = 0; k < ng; ++k) {
+        double c[4];
+        laue_qmul_d(el[i], g[k], c);
+        if (c[0] < 0)
+          for (double& v : c) v = -v;
+        bool known = false;
+        for (int e = 0; e < n && !known; ++e)
+          known = std::fabs(std::fabs(c[0] * el[e][0] + c[1] * el[e][1] + c[2] * el[e][2] + c[3] * el[e][3]) -
+                            1.0) < 1e-9;
+        if (!known && n < 24) {
+          for (int d = 0; d < 4; ++d) el[n][d] = c[d];
+          ++n;
+          grew = true;
+        }
+      }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 4; ++d) t->q[4 * i + d] = (float)el[i][d];
+  t->n = n;
+  return n;
+}
+
+
 
 // ---------------------------------------------------------------------------
 // Device helpers

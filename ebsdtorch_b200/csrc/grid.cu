@@ -188,7 +188,8 @@ __global__ void __launch_bounds__(1024) k_grid_scan(const int32_t* __restrict__ 
 __global__ void __launch_bounds__(kGridBlock) k_grid_write(int laue, int edge, int64_t n_total,
                                                            const int64_t* __restrict__ offsets,
                                                            float* __restrict__ out_f32,
-                                                           double* __restrict__ out_f64) {
+                                                           double* __restrict__ out_f64,
+                                                           int32_t* __restrict__ out_cells) {
   __shared__ int warp_cnt[kGridBlock / 32];
   const int64_t i = blockIdx.x * (int64_t)kGridBlock + threadIdx.x;
   double q[4] = {0, 0, 0, 0};
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(kGridBlock) k_grid_write(int laue, int edge, i
     const int64_t r = offsets[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u));
     reinterpret_cast<float4*>(out_f32)[r] =
         make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+    if (out_cells) out_cells[r] = (int32_t)i;
     if (out_f64) {
       out_f64[4 * r + 0] = q[0];
       out_f64[4 * r + 1] = q[1];
@@ -258,7 +260,7 @@ extern "C" int ebsd_grid_fz_count(int laue_id, int edge_length, void* workspace,
 
 extern "C" int ebsd_grid_fz_write(int laue_id, int edge_length, const void* workspace,
                                   size_t workspace_bytes, float* out_f32, double* out_f64,
-                                  void* stream) {
+                                  int32_t* out_cells, void* stream) {
   if (int rc = grid_check(laue_id, edge_length, workspace, workspace_bytes)) return rc;
   EBSD_ARG_CHECK(out_f32 != nullptr, "out_f32 is null");
   EBSD_ARG_CHECK((reinterpret_cast<uintptr_t>(out_f32) & 15) == 0, "out_f32 must be 16-byte aligned");
@@ -266,7 +268,7 @@ extern "C" int ebsd_grid_fz_write(int laue_id, int edge_length, const void* work
   const int64_t* offsets = reinterpret_cast<const int64_t*>(workspace);
   k_grid_write<<<nb, kGridBlock, 0, as_stream(stream)>>>(laue_id, edge_length,
                                                          grid_points(edge_length), offsets, out_f32,
-                                                         out_f64);
+                                                         out_f64, out_cells);
   EBSD_LAUNCH_CHECK();
   return 0;
 }

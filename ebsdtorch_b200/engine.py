@@ -157,14 +157,22 @@ class Searcher:
             raise MemoryError(
                 f"dictionary indexing needs more device memory than the budget of {budget / 2**30:.1f} GiB")
 
-    def run(self, fill_dict: DictFill, fill_queries: QueryFill, queries_reusable: bool = True):
+    def run(self, fill_dict: Optional[DictFill], fill_queries: QueryFill, resident: Optional[RowSet] = None):
         """Search all queries against all dictionary rows.
-        Returns (indices (Q, k) int64, scores (Q, k) float32) on the device."""
+        `resident`: an already filled RowSet holding the whole dictionary (then
+        fill_dict is not called). Returns (indices (Q, k) int64, scores (Q, k)
+        float32) on the device."""
         dev, Q, D, k = self.device, self.n_queries, self.n_dict, self.k
         out_val = torch.empty((Q, k), dtype=torch.float32, device=dev)
         out_idx = torch.empty((Q, k), dtype=torch.int64, device=dev)
         status = torch.zeros(1, dtype=torch.int32, device=dev)
-        dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
+        if resident is not None:
+            if resident.n_rows != D or resident.lp_dtype != self.lp_dtype or (self.rescore and resident.f32 is None):
+                raise ValueError("resident dictionary rows do not match the search")
+            self.dict_chunk = D
+            dict_rows = resident
+        else:
+            dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
         qc = self.query_chunk
         q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.rescore, dev)
         # match launches cover one wave of (query tile, dictionary range) units
@@ -177,10 +185,11 @@ class Searcher:
         for ci, d0 in enumerate(range(0, D, self.dict_chunk)):
             d1 = min(D, d0 + self.dict_chunk)
             nd = d1 - d0
-            if nd < dict_rows.n_rows:
-                dict_rows.lp[nd:].zero_()
-                dict_rows.norm[nd:].zero_()
-            fill_dict(d0, d1, dict_rows.buffers(0, nd))
+            if resident is None:
+                if nd < dict_rows.n_rows:
+                    dict_rows.lp[nd:].zero_()
+                    dict_rows.norm[nd:].zero_()
+                fill_dict(d0, d1, dict_rows.buffers(0, nd))
             col_scale = _col_scale(dict_rows, self.cfg.similarity)
             nd_pad = round_up(nd, TILE_D)
             d_lp = dict_rows.lp[:nd_pad]

@@ -43,9 +43,10 @@ def _cuda(t: torch.Tensor, name: str, dtype=None, contiguous=True) -> torch.Tens
 # ---------------------------------------------------------------- A1/A2 grid
 
 
-def grid_fz(laue_id: int, edge_length: int, device, want_f64: bool = False):
+def grid_fz(laue_id: int, edge_length: int, device, want_f64: bool = False, want_cells: bool = False):
     """FZ quaternions of the edge^3 cubochoric grid in reference order.
-    Returns (q_f32 (n, 4), q_f64 (n, 4) or None)."""
+    Returns (q_f32 (n, 4), q_f64 (n, 4) or None), plus the int32 grid cell of
+    each point when want_cells."""
     device = torch.device(device)
     lib = _capi.load()
     nbytes = int(lib.ebsd_grid_workspace_bytes(int(edge_length)))
@@ -58,8 +59,11 @@ def grid_fz(laue_id: int, edge_length: int, device, want_f64: bool = False):
     n = int(cnt.item())
     q32 = torch.empty((n, 4), dtype=torch.float32, device=device)
     q64 = torch.empty((n, 4), dtype=torch.float64, device=device) if want_f64 else None
+    cells = torch.empty(n, dtype=torch.int32, device=device) if want_cells else None
     if n:
-        call("ebsd_grid_fz_write", int(laue_id), int(edge_length), ptr(ws), nbytes, ptr(q32), ptr(q64), s)
+        call("ebsd_grid_fz_write", int(laue_id), int(edge_length), ptr(ws), nbytes, ptr(q32), ptr(q64), ptr(cells), s)
+    if want_cells:
+        return q32, q64, cells
     return q32, q64
 
 

@@ -72,9 +72,10 @@ int ebsd_grid_fz_count(int laue_id, int edge_length, void* workspace, size_t wor
 
 /* Pass 2 (after pass 1 on the same workspace): the FZ quaternions (w,x,y,z),
  * w >= 0, in the reference's grid order, to out_f32 (n x 4) and, if not NULL,
- * out_f64 (n x 4). */
+ * out_f64 (n x 4) and out_cells (n, the linear grid index (i*e + j)*e + k of
+ * each point). */
 int ebsd_grid_fz_write(int laue_id, int edge_length, const void* workspace, size_t workspace_bytes,
-                       float* out_f32, double* out_f64, void* stream);
+                       float* out_f32, double* out_f64, int32_t* out_cells, void* stream);
 
 /* out[i, :] = in[index[i], :] for rows of `width` floats.
  * Replaces the `so3_samples_fz[torch.randperm(n)]` gather
@@ -233,6 +234,23 @@ int ebsd_split3_bf16(const float* X, int64_t n_rows, int n_cols, int64_t ld, con
  * (radians). */
 int ebsd_disori_angle(const float* q1, const float* q2, int64_t n, int laue_id, float* out,
                       void* stream);
+
+/* ---- local dictionary search around orientation proposals --------------------
+ * No counterpart in the reference (search step of the learned-proposal path).
+ * cell_to_row (edge^3 int32): dictionary row of each cubochoric grid cell or
+ * -1, built by ebsd_cell_to_row from the cells of ebsd_grid_fz_write and the
+ * dictionary permutation (row j holds FZ point perm[j]; perm NULL = identity).
+ * ebsd_local_search: per query, the dictionary orientations within
+ * max_angle_rad of a symmetric copy of proposals[q] that lie in the grid cells
+ * within radius_cells of that copy are scored by the exact FP32 dot of
+ * q_f32[q] with d_f32[row]; the best row and score are written (ties: lower
+ * row; -1 / -inf when no candidate), and the candidate count if out_ncand. */
+int ebsd_cell_to_row(const int32_t* cells, const int64_t* perm, int64_t n, int64_t n_cells, int32_t* cell_to_row,
+                     void* stream);
+int ebsd_local_search(const float* q_f32, int64_t ld_q, int64_t n_queries, const float* proposals, int laue_id,
+                      int edge_length, const int32_t* cell_to_row, const float* dict_quats, const float* d_f32,
+                      int64_t ld_d, int64_t n_dict, int n_pix, int radius_cells, float max_angle_rad,
+                      int max_candidates, int64_t* out_idx, float* out_score, int32_t* out_ncand, void* stream);
 
 /* ---- A15: 6-D rotation representation and the learned proposal ------------
  * 6-D (Zhou et al.) -> quaternion (orientations.py:986-1005 zh2qu: Gram-Schmidt

@@ -260,6 +260,50 @@ def cu2qu(cu: np.ndarray, mode: str = "exact") -> np.ndarray:
     return ho2qu(cu2ho(cu), mode=mode)
 
 
+def qu2ho(qu: np.ndarray) -> np.ndarray:
+    """Quaternion -> homochoric vector h = axis * (3/4 (w - sin w))^(1/3)
+    (orientations.py:28-48), float64, series form near w = 0."""
+    qu = np.asarray(qu, dtype=np.float64)
+    w = 2.0 * np.arccos(np.clip(qu[..., 0], -1.0, 1.0))
+    n = np.linalg.norm(qu[..., 1:], axis=-1, keepdims=True)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        axis = np.where(n > 0, qu[..., 1:] / n, 0.0)
+    w2 = w * w
+    wms = np.where(w < 0.25, w * w2 / 6.0 * (1 - w2 / 20.0 * (1 - w2 / 42.0 * (1 - w2 / 72.0))), w - np.sin(w))
+    return axis * np.cbrt(0.75 * wms)[..., None]
+
+
+def ho2cu(ho: np.ndarray) -> np.ndarray:
+    """Homochoric -> cubochoric, the inverse of cu2ho (orientations.py:352-416,
+    Rosca et al. 2014): magnitudes ordered ascending, inverse square-to-sphere
+    and squircle steps, signs copied back."""
+    ho = np.asarray(ho, dtype=np.float64)
+    a = np.abs(ho)
+    order = np.argsort(a, axis=-1, kind="stable")
+    srt = np.take_along_axis(a, order, axis=-1)
+    x3, y3, z3 = srt[..., 0], srt[..., 1], srt[..., 2]
+    r = np.linalg.norm(ho, axis=-1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        pf = np.sqrt(2 * r / (r + z3))
+        x2, y2 = x3 * pf, y3 * pf
+        z2 = math.sqrt(math.pi / 6) * r
+        q = np.sqrt(x2 * x2 + 2 * y2 * y2)
+        pf2 = math.sqrt(math.pi / 6) * np.sqrt(x2 * x2 + y2 * (q + 2 * y2)) / math.sqrt(2.0)
+        x1 = pf2 * 12.0 / math.pi * np.arccos(np.clip((x2 * x2 + y2 * q) / (math.sqrt(2.0) * (x2 * x2 + y2 * y2)),
+                                                        -1.0, 1.0))
+        y1 = pf2
+    cs = np.stack((x1, y1, z2), axis=-1) / (math.pi / 6) ** (1.0 / 6.0)
+    cs = np.where(np.isnan(cs), 0.0, cs)
+    cu = np.empty_like(cs)
+    np.put_along_axis(cu, order, cs, axis=-1)
+    return np.copysign(cu, ho)
+
+
+def qu2cu(qu: np.ndarray) -> np.ndarray:
+    """Quaternion -> cubochoric (orientations.py:1024-1035)."""
+    return ho2cu(qu2ho(qu))
+
+
 def grid_edge_length(laue_id: int, angular_resolution_deg: float) -> int:
     """Cubochoric edge length for a target resolution (laue_fz_ori.py:540-547).
 
@@ -826,6 +870,26 @@ def cnn_forward_backward(params: dict, x: np.ndarray, q_true: np.ndarray, laue_i
             dx = _col2im(g @ params[f"conv{j}.w"], shape)
             g = dx.reshape(-1, shape[3])
     return z, float(loss.mean()), grads
+
+
+def local_search_bruteforce(q_rows: np.ndarray, proposals: np.ndarray, dictionary: np.ndarray,
+                            d_rows: np.ndarray, laue_id: int, max_angle_rad: float):
+    """Checker of ebsd_local_search: for each query, every dictionary
+    orientation whose disorientation from the proposal is at most
+    max_angle_rad, scored by the exact dot; best index (ties: lower index) and
+    score, -1 / -inf when none."""
+    Q = q_rows.shape[0]
+    best_i = np.full(Q, -1, dtype=np.int64)
+    best_v = np.full(Q, -np.inf)
+    for i in range(Q):
+        ang = disori_angle(np.broadcast_to(proposals[i], dictionary.shape), dictionary, laue_id)
+        cand = np.nonzero(ang <= max_angle_rad)[0]
+        if cand.size == 0:
+            continue
+        sc = d_rows[cand] @ q_rows[i]
+        j = np.lexsort((cand, -sc))[0]
+        best_i[i], best_v[i] = cand[j], sc[j]
+    return best_i, best_v
 
 
 # --------------------------------------------------------------------------
