@@ -1,6 +1,6 @@
 // Local dictionary search around per-pattern orientation proposals.
 //
-// For each pattern: every symmetry-equivalent copy q g of its proposal q
+// For each pattern: every symmetry-equivalent copy g q of its proposal q
 // (Laue operators g) is mapped to cubochoric coordinates (quaternion ->
 // homochoric -> cubochoric; the inverse of the map in grid.cu, Rosca et al.
 // 2014, as qu2cu orientations.py:1024-1035 and ho2cu :352-416), the grid cells
@@ -107,10 +107,11 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
   if (tid < ops.n) {
     const float4 pr = proposals[q];
     const float* o = ops.q + 4 * tid;
-    double g[4] = {(double)pr.x * o[0] - (double)pr.y * o[1] - (double)pr.z * o[2] - (double)pr.w * o[3],
-                   (double)pr.x * o[1] + (double)pr.y * o[0] + (double)pr.z * o[3] - (double)pr.w * o[2],
-                   (double)pr.x * o[2] - (double)pr.y * o[3] + (double)pr.z * o[0] + (double)pr.w * o[1],
-                   (double)pr.x * o[3] + (double)pr.y * o[2] - (double)pr.z * o[1] + (double)pr.w * o[0]};
+    // copy g q: crystal symmetry acts on the left (pattern(g q) == pattern(q))
+    double g[4] = {o[0] * (double)pr.x - o[1] * (double)pr.y - o[2] * (double)pr.z - o[3] * (double)pr.w,
+                   o[0] * (double)pr.y + o[1] * (double)pr.x + o[2] * (double)pr.w - o[3] * (double)pr.z,
+                   o[0] * (double)pr.z - o[1] * (double)pr.w + o[2] * (double)pr.x + o[3] * (double)pr.y,
+                   o[0] * (double)pr.w + o[1] * (double)pr.z - o[2] * (double)pr.y + o[3] * (double)pr.x};
     const double nrm = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2] + g[3] * g[3]);
     for (double& v : g) v /= nrm;
     if (g[0] < 0.0)

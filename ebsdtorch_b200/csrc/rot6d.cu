@@ -6,7 +6,7 @@
 // diagonal branch, then w >= 0 and the axis signs from the antisymmetric
 // part), qu2om :913-937, qu2zh :1008-1020 (first two rows).
 // The loss has no counterpart in the reference (it has no learned indexer):
-//   L_i = min over Laue operators g of || zh2om(z_i) - om(q_i g) ||_F^2,
+//   L_i = min over Laue operators g of || zh2om(z_i) - om(g q_i) ||_F^2,
 // with the exact gradient through the Gram-Schmidt map.
 #include <algorithm>
 #include <cmath>
@@ -108,10 +108,12 @@ __global__ void k_rot6d_loss(const float* __restrict__ zh, const float* __restri
     float best = INFINITY, tgt[3][3] = {};
     for (int g = 0; g < ops.n; ++g) {
       const float* o = ops.q + 4 * g;
-      const float qg[4] = {qt[0] * o[0] - qt[1] * o[1] - qt[2] * o[2] - qt[3] * o[3],
-                           qt[0] * o[1] + qt[1] * o[0] + qt[2] * o[3] - qt[3] * o[2],
-                           qt[0] * o[2] - qt[1] * o[3] + qt[2] * o[0] + qt[3] * o[1],
-                           qt[0] * o[3] + qt[1] * o[2] - qt[2] * o[1] + qt[3] * o[0]};
+      // g q: crystal symmetry acts on the left (pattern(g q) == pattern(q)
+      // for the projector's q v q* ray rotation)
+      const float qg[4] = {o[0] * qt[0] - o[1] * qt[1] - o[2] * qt[2] - o[3] * qt[3],
+                           o[0] * qt[1] + o[1] * qt[0] + o[2] * qt[3] - o[3] * qt[2],
+                           o[0] * qt[2] - o[1] * qt[3] + o[2] * qt[0] + o[3] * qt[1],
+                           o[0] * qt[3] + o[1] * qt[2] - o[2] * qt[1] + o[3] * qt[0]};
       float m[3][3];
       qu_to_om(qg, m);
       float d = 0.f;

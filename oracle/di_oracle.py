@@ -767,7 +767,7 @@ def qu2zh(qu: np.ndarray) -> np.ndarray:
 
 
 def rot6d_sym_loss(zh: np.ndarray, q_true: np.ndarray, laue_id: int):
-    """Per-sample loss min over Laue operators g of ||zh2om(zh) - om(q_true g)||_F^2
+    """Per-sample loss min over Laue operators g of ||zh2om(zh) - om(g q_true)||_F^2
     and its gradient with respect to zh (Gram-Schmidt backward), float64.
     The CNN head's training objective (a new part: the reference has no
     learned indexer)."""
@@ -776,7 +776,7 @@ def rot6d_sym_loss(zh: np.ndarray, q_true: np.ndarray, laue_id: int):
     best = np.full(zh.shape[0], np.inf)
     target = np.zeros_like(R)
     for op in g:
-        Rt = qu2om(_qmul(q_true, np.broadcast_to(op, q_true.shape)))
+        Rt = qu2om(_qmul(np.broadcast_to(op, q_true.shape), q_true))
         d = np.sum((R - Rt) ** 2, axis=(-2, -1))
         sel = d < best
         best = np.where(sel, d, best)

@@ -168,9 +168,9 @@ def test_rot6d_sym_loss_gradient_finite_difference():
         lp, _ = O.rot6d_sym_loss(zh + dz, q, 11)
         lm, _ = O.rot6d_sym_loss(zh - dz, q, 11)
         assert np.allclose((lp - lm) / (2 * eps), grad[:, j], atol=1e-5, rtol=1e-4)
-    # the loss vanishes at any symmetry-equivalent target
+    # the loss vanishes at any symmetry-equivalent target g q
     g = O.laue_elements(11)
-    qt = O._qmul(q, np.broadcast_to(g[5], q.shape))
+    qt = O._qmul(np.broadcast_to(g[5], q.shape), q)
     l0, g0 = O.rot6d_sym_loss(O.qu2zh(qt), q, 11)
     assert np.abs(l0).max() < 1e-20 and np.abs(g0).max() < 1e-9
 
@@ -201,3 +201,18 @@ def test_cnn_oracle_gradient_finite_difference():
             p3[k][idx] -= eps
             num = (O.cnn_forward_backward(p2, x, q, 11)[1] - O.cnn_forward_backward(p3, x, q, 11)[1]) / (2 * eps)
             assert abs(num - g[k][idx]) <= 1e-6 * max(1.0, abs(num))
+
+
+def test_symmetry_acts_on_the_left():
+    """pattern(g q) == pattern(q) for crystal symmetry g with the projector's
+    q v q* ray rotation; the learned-path loss and local search rely on it."""
+    from ebsdtorch_b200.synthetic import synthetic_master_pattern
+
+    mp = synthetic_master_pattern(129, seed=1, noise=0.0).numpy().astype(np.float64)
+    rays = O.unit_rays(O.detector_coords_sample_frame((24, 24), (0.5, 0.5, 0.6), (0, 70, 0)))
+    q = np.array([0.7, 0.1, -0.5, 0.2])
+    q /= np.linalg.norm(q)
+    base = O.project_patterns(mp, rays, q[None])[0]
+    g = O.laue_elements(11)[1]  # 180 deg about z: maps lattice points onto lattice points exactly
+    assert np.abs(O.project_patterns(mp, rays, O._qmul(g, q)[None])[0] - base).max() < 1e-3
+    assert np.abs(O.project_patterns(mp, rays, O._qmul(q, g)[None])[0] - base).max() > 0.1
