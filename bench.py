@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -415,6 +416,77 @@ def run_ours(args, wl):
         dist.destroy_process_group()
 
 
+def run_learned(args, wl):
+    """Learned proposal + local search + plain-DI fallback on the full
+    workload (the CNN is trained first on freshly projected patterns)."""
+    import torch
+
+    from ebsdtorch_b200 import _capi, synthetic
+    from ebsdtorch_b200.ebsd import EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations
+    from ebsdtorch_b200.learned import train_proposal_cnn
+    from ebsdtorch_b200.local_search import learned_dictionary_index
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    _capi.load()
+    mp_t = synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev)
+    mp = MasterPattern(mp_t, laue_group=11)
+    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+    t0 = time.perf_counter()
+    model, losses = train_proposal_cnn(mp_t, geom, 11, steps=args.train_steps, batch=256, lr=1e-3,
+                                       mean_counts=wl["counts"], seed=0)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    truth = synthetic.random_quaternions(wl["Q"], 5000).to(dev)
+    pats = synthetic.synthetic_patterns(mp_t, geom, truth, mean_counts=wl["counts"], seed=5001)
+    exp = ExperimentPatterns(pats)
+    for _ in range(args.warmup):
+        torch.manual_seed(0)
+        learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
+                                 max_angle_deg=args.max_angle, coarse_resolution_deg=args.coarse_res)
+    torch.cuda.synchronize()
+    with ClockSampler(int(dev.index or 0)) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            torch.manual_seed(0)
+            st = learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
+                                          max_angle_deg=args.max_angle, coarse_resolution_deg=args.coarse_res)
+        e1.record()
+        torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3 / args.steps
+    learned_idx = exp.raw_indexing_indices[0][:, 0].clone()
+    # plain DI on the same patterns (bf16 + FP32 re-score == FP32 DI top-1)
+    exp_f = ExperimentPatterns(pats)
+    torch.manual_seed(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    dictionary_index_orientations(mp, geom, exp_f, dictionary_resolution_degrees=wl["res"], top_k_matches=1,
+                                  match_dtype=torch.float32)
+    torch.cuda.synchronize()
+    t_full = time.perf_counter() - t0
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+
+    ang = disori_angle_laue(exp.orientations.float().contiguous(), exp_f.orientations.float().contiguous(), 11, 11)
+    line = {
+        "metric": METRIC, "value": wl["Q"] / secs, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": "learned proposal + local DI (<= %.1f deg on a %.1f deg dictionary, then the full "
+                               "dictionary) + plain-DI fallback; " % (args.max_angle, args.coarse_res) + wl["name"], "train_steps": args.train_steps, "train_batch": 256,
+                   "train_patterns": 256 * args.train_steps},
+        "learned": {"within_0.5deg_of_plain_di": float((ang < math.radians(0.5)).float().mean()),
+                    "same_top1_index_as_plain_di": float((learned_idx == exp_f.raw_indexing_indices[0][:, 0])
+                                                         .float().mean()),
+                    "fallback_fraction": st.n_fallback / st.n_patterns, "mean_candidates": st.mean_candidates,
+                    "stage_seconds": st.seconds, "train_seconds": t_train,
+                    "final_train_loss": float(losses[-100:].mean()),
+                    "plain_di_seconds_same_gpu": t_full, "speedup_vs_plain_di_bf16": t_full / secs},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -427,10 +499,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--fp32-subset", type=int, default=4096)
+    ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
+    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--max-angle", type=float, default=8.0)
+    ap.add_argument("--coarse-res", type=float, default=2.0)
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
+    elif args.learned:
+        run_learned(args, wl)
     else:
         run_ours(args, wl)
 

@@ -82,12 +82,17 @@ class LearnedStats:
 
 
 def learned_dictionary_index(master_pattern, geometry, experiment_patterns, model, dictionary_resolution_degrees=0.5,
-                             max_angle_deg: float = 3.0, fallback_ratio: float = 0.9, batch: int = 1024,
-                             precision: str = "bf16", rescore_k: int = 32, device=None,
+                             max_angle_deg: float = 8.0, coarse_resolution_deg: Optional[float] = 2.0,
+                             fallback_ratio: float = 0.9, batch: int = 1024, precision: str = "bf16",
+                             rescore_k: int = 32, device=None,
                              phase_dictionary: Optional[PhaseDictionary] = None) -> LearnedStats:
     """Top-1 indexing of one phase by learned proposal + local search with
-    plain-DI fallback. Writes raw_indexing_results / orientations like
-    dictionary_index_orientations and returns timing and fallback counts."""
+    plain-DI fallback. With coarse_resolution_deg the search runs in two
+    stages: within max_angle_deg of the proposal on a coarse dictionary, then
+    within 1.5 coarse spacings of the coarse winner on the full-resolution
+    dictionary (without it: one stage within max_angle_deg). Writes
+    raw_indexing_results / orientations like dictionary_index_orientations and
+    returns timing and fallback counts."""
     from .ebsd.indexing import _device, _master_pattern_tensor, _unit_rays_soa
 
     sec = {}
@@ -97,6 +102,10 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     mp_t = _master_pattern_tensor(master_pattern, 1, dev)
     pd = phase_dictionary or PhaseDictionary(mp_t, rays, master_pattern.laue_group, dictionary_resolution_degrees,
                                              precision)
+    coarse = None
+    if coarse_resolution_deg is not None and coarse_resolution_deg > dictionary_resolution_degrees:
+        coarse = PhaseDictionary(mp_t, rays, master_pattern.laue_group, coarse_resolution_deg, precision,
+                                 permute=False)
     torch.cuda.synchronize(dev)
     sec["dictionary"] = time.perf_counter() - t0
     pats = experiment_patterns.patterns
@@ -121,7 +130,14 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     torch.cuda.synchronize(dev)
     sec["proposals"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    idx, score, ncand = local_search(pd, q_f32, proposals, max_angle_deg)
+    if coarse is not None:
+        cidx, _, _ = local_search(coarse, q_f32, proposals, max_angle_deg)
+        found = cidx >= 0
+        refined = torch.where(found[:, None], kernels.gather_rows(coarse.quats, cidx.clamp_min(0)), proposals)
+        idx, score, ncand = local_search(pd, q_f32, refined.contiguous(), 1.5 * coarse_resolution_deg)
+        idx = torch.where(found, idx, torch.full_like(idx, -1))
+    else:
+        idx, score, ncand = local_search(pd, q_f32, proposals, max_angle_deg)
     valid = idx >= 0
     med = torch.median(score[valid]) if bool(valid.any()) else torch.tensor(0.0, device=dev)
     fb = (~valid) | (score < fallback_ratio * med)

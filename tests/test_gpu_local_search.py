@@ -108,14 +108,15 @@ def test_trained_network_gain():
     pats = synthetic.synthetic_patterns(mp_t, geom, truth, mean_counts=200.0, seed=778)
     exp_l = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
-    st = learned_dictionary_index(mp, geom, exp_l, model, dictionary_resolution_degrees=2.0, max_angle_deg=8.0)
+    st = learned_dictionary_index(mp, geom, exp_l, model, dictionary_resolution_degrees=1.0, max_angle_deg=8.0,
+                                  coarse_resolution_deg=3.0)
     exp_u = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
     st_u = learned_dictionary_index(mp, geom, exp_u, OrientationCNN((64, 64), 11, seed=9, device=DEV),
-                                    dictionary_resolution_degrees=2.0, max_angle_deg=8.0)
+                                    dictionary_resolution_degrees=1.0, max_angle_deg=8.0, coarse_resolution_deg=3.0)
     exp_f = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
-    dictionary_index_orientations(mp, geom, exp_f, dictionary_resolution_degrees=2.0, match_dtype=torch.float32)
+    dictionary_index_orientations(mp, geom, exp_f, dictionary_resolution_degrees=1.0, match_dtype=torch.float32)
     full = exp_f.raw_indexing_indices[0][:, 0]
     agree = (exp_l.raw_indexing_indices[0][:, 0] == full).float().mean().item()
     agree_u = (exp_u.raw_indexing_indices[0][:, 0] == full).float().mean().item()
