@@ -440,10 +440,12 @@ def run_learned(args, wl):
     truth = synthetic.random_quaternions(wl["Q"], 5000).to(dev)
     pats = synthetic.synthetic_patterns(mp_t, geom, truth, mean_counts=wl["counts"], seed=5001)
     exp = ExperimentPatterns(pats)
+    pyramid = tuple(float(v) for v in args.pyramid.split(",") if v)
     for _ in range(args.warmup):
         torch.manual_seed(0)
         learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
-                                 max_angle_deg=args.max_angle, coarse_resolution_deg=args.coarse_res)
+                                 max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
+                                 fallback_ratio=args.fallback_ratio)
     torch.cuda.synchronize()
     with ClockSampler(int(dev.index or 0)) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -451,11 +453,17 @@ def run_learned(args, wl):
         for _ in range(args.steps):
             torch.manual_seed(0)
             st = learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
-                                          max_angle_deg=args.max_angle, coarse_resolution_deg=args.coarse_res)
+                                          max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
+                                          fallback_ratio=args.fallback_ratio)
         e1.record()
         torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) / 1e3 / args.steps
     learned_idx = exp.raw_indexing_indices[0][:, 0].clone()
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+
+    perr = torch.rad2deg(disori_angle_laue(exp.proposals.contiguous(), truth.float().contiguous(), 11, 11))
+    prop_err = {f"p{q}": float(torch.quantile(perr, q / 100.0)) for q in (50, 90, 99)}
+    prop_err["frac_within_max_angle"] = float((perr <= args.max_angle).float().mean())
     # plain DI on the same patterns (bf16 + FP32 re-score == FP32 DI top-1)
     exp_f = ExperimentPatterns(pats)
     torch.manual_seed(0)
@@ -465,20 +473,29 @@ def run_learned(args, wl):
                                   match_dtype=torch.float32)
     torch.cuda.synchronize()
     t_full = time.perf_counter() - t0
-    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
-
     ang = disori_angle_laue(exp.orientations.float().contiguous(), exp_f.orientations.float().contiguous(), 11, 11)
+    # local cosine / map median before the fallback, for patterns that agree
+    # with plain DI and for those that do not (how the threshold separates them)
+    ratio = exp.local_cosine_ratio
+    miss = ang >= math.radians(0.5)
+    qs = torch.tensor([0.01, 0.05, 0.5, 0.95, 0.99], device=ratio.device)
+    ratio_q = {"agree": [round(float(v), 4) for v in torch.quantile(ratio[~miss], qs)] if bool((~miss).any()) else [],
+               "miss": [round(float(v), 4) for v in torch.quantile(ratio[miss], qs)] if bool(miss.any()) else []}
     line = {
         "metric": METRIC, "value": wl["Q"] / secs, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
-        "config": {"workload": "learned proposal + local DI (<= %.1f deg on a %.1f deg dictionary, then the full "
-                               "dictionary) + plain-DI fallback; " % (args.max_angle, args.coarse_res) + wl["name"], "train_steps": args.train_steps, "train_batch": 256,
+        "config": {"workload": "learned proposal + coarse-to-fine local DI (<= %.1f deg of the proposal on the %s deg "
+                               "dictionaries, then the full one) + plain-DI fallback; " % (args.max_angle, args.pyramid)
+                               + wl["name"], "train_steps": args.train_steps, "train_batch": 256,
                    "train_patterns": 256 * args.train_steps},
         "learned": {"within_0.5deg_of_plain_di": float((ang < math.radians(0.5)).float().mean()),
                     "same_top1_index_as_plain_di": float((learned_idx == exp_f.raw_indexing_indices[0][:, 0])
                                                          .float().mean()),
                     "fallback_fraction": st.n_fallback / st.n_patterns, "mean_candidates": st.mean_candidates,
+                    "stage_radii_deg": st.stage_radii_deg, "stage_mean_candidates": st.stage_mean_candidates,
+                    "proposal_error_deg": prop_err, "fallback_ratio": args.fallback_ratio,
+                    "cosine_over_median_q01_05_50_95_99": ratio_q,
                     "stage_seconds": st.seconds, "train_seconds": t_train,
                     "final_train_loss": float(losses[-100:].mean()),
                     "plain_di_seconds_same_gpu": t_full, "speedup_vs_plain_di_bf16": t_full / secs},
@@ -501,8 +518,9 @@ def main():
     ap.add_argument("--fp32-subset", type=int, default=4096)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--train-steps", type=int, default=3000)
-    ap.add_argument("--max-angle", type=float, default=8.0)
-    ap.add_argument("--coarse-res", type=float, default=2.0)
+    ap.add_argument("--max-angle", type=float, default=12.0)
+    ap.add_argument("--fallback-ratio", type=float, default=0.9)
+    ap.add_argument("--pyramid", default="2.0,1.0", help="intermediate dictionary resolutions (deg), coarse first")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

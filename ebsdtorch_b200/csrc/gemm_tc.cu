@@ -57,6 +57,11 @@ struct GemmParams {
   int64_t m_valid;
   float alpha;
   int accumulate;
+  const float* bias;     // MODE 2: per-row (output channel) bias
+  __nv_bfloat16* out16;  // MODE 2: bf16 activations, (n_valid x ld_out)
+  float* out32;          // MODE 2: optional FP32 copy, same layout
+  int64_t ld_out;
+  int relu;
   int* status;
 };
 
@@ -89,7 +94,9 @@ __device__ __forceinline__ void report_timeout(const GemmParams& p, volatile int
   atomicExch(p.status, EBSD_DEVICE_TIMEOUT);
 }
 
-// MODE 0: top-k epilogue. MODE 1: store epilogue.
+// MODE 0: top-k epilogue. MODE 1: store epilogue. MODE 2: convolution
+// epilogue, out[col, row] = act(acc[row, col] + bias[row]) stored transposed
+// in bf16 (and FP32 when asked).
 template <int KIND, int MODE, int KC>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
@@ -300,6 +307,23 @@ __global__ void __launch_bounds__(THREADS, 1)
               if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
             }
           }
+        } else if constexpr (MODE == 2) {
+          const int64_t grow = (int64_t)m_tile * BM + row;
+          if (grow < p.m_valid) {
+            const float b = p.bias ? __ldg(p.bias + grow) : 0.f;
+            // the warp's 32 threads own 32 consecutive channels: each store
+            // instruction writes 32 consecutive values of one pixel
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int64_t col = col0 + j;
+              if (col < p.n_valid) {
+                float r = v[j] + b;
+                if (p.relu) r = fmaxf(r, 0.f);
+                p.out16[col * p.ld_out + grow] = __float2bfloat16_rn(r);
+                if (p.out32) p.out32[col * p.ld_out + grow] = r;
+              }
+            }
+          }
         } else {
           const int64_t grow = (int64_t)m_tile * BM + row;
           if (grow < p.m_valid) {
@@ -494,10 +518,9 @@ extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, co
                                   : launch_topk<1>(n_cand, ta, tb, p, grid, s);
 }
 
-extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad,
-                            int64_t k_pad, int lp_dtype, float alpha, int accumulate, float* C,
-                            int64_t ldc, int64_t m_valid, int64_t n_valid, int* d_status,
-                            void* stream) {
+extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
+                            int lp_dtype, float alpha, int accumulate, float* C, int64_t ldc, int64_t m_valid,
+                            int64_t n_valid, int splits, int* d_status, void* stream) {
   if (int rc = check_operands(A, m_pad, B, n_pad, k_pad, lp_dtype, d_status)) return rc;
   EBSD_ARG_CHECK(C != nullptr, "null output");
   EBSD_ARG_CHECK(m_valid > 0 && m_valid <= m_pad && n_valid > 0 && n_valid <= n_pad,
@@ -508,8 +531,9 @@ extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t
   if (int rc = make_tmap(&tb, B, lp_dtype, n_pad, k_pad, BN)) return rc;
   GemmParams p{};
   p.n_tiles = (int)(n_pad / BN);
-  // one dictionary tile per unit keeps all SMs busy for small outputs
-  p.splits = p.n_tiles;
+  // splits <= 0: one B tile per unit; otherwise each unit streams a range of
+  // n_tiles / splits B tiles (amortises CTA set-up when K is short)
+  p.splits = splits <= 0 ? p.n_tiles : std::min(splits, p.n_tiles);
   p.k_iters = (int)(k_pad * (lp_dtype == EBSD_DT_BF16 ? 2 : 1) / BKB);
   p.n_valid = n_valid;
   p.C = C;
@@ -524,4 +548,31 @@ extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t
   cudaStream_t s = as_stream(stream);
   return lp_dtype == EBSD_DT_BF16 ? launch<0, 1, 1>(ta, tb, p, grid, s)
                                   : launch<1, 1, 1>(ta, tb, p, grid, s);
+}
+
+extern "C" int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* cols, int64_t rows_pad,
+                                 int64_t k_pad, const float* bias, int cout, int64_t n_rows, int relu, void* out16,
+                                 int64_t ld_out, float* out32, int splits, int* d_status, void* stream) {
+  if (int rc = check_operands(w16, cout_pad, cols, rows_pad, k_pad, EBSD_DT_BF16, d_status)) return rc;
+  EBSD_ARG_CHECK(out16 != nullptr, "null output");
+  EBSD_ARG_CHECK(cout > 0 && cout <= cout_pad && n_rows > 0 && n_rows <= rows_pad, "valid extents out of range");
+  EBSD_ARG_CHECK(ld_out >= cout, "ld_out < cout");
+  CUtensorMap ta, tb;
+  if (int rc = make_tmap(&ta, w16, EBSD_DT_BF16, cout_pad, k_pad, BM)) return rc;
+  if (int rc = make_tmap(&tb, cols, EBSD_DT_BF16, rows_pad, k_pad, BN)) return rc;
+  GemmParams p{};
+  p.n_tiles = (int)(rows_pad / BN);
+  p.splits = splits <= 0 ? p.n_tiles : std::min(splits, p.n_tiles);
+  p.k_iters = (int)(k_pad * 2 / BKB);
+  p.n_valid = n_rows;
+  p.m_valid = cout;
+  p.bias = bias;
+  p.out16 = reinterpret_cast<__nv_bfloat16*>(out16);
+  p.out32 = out32;
+  p.ld_out = ld_out;
+  p.relu = relu;
+  p.status = d_status;
+  const int64_t m_tiles = cout_pad / BM;
+  EBSD_ARG_CHECK(m_tiles * p.splits < INT32_MAX, "too many work units");
+  return launch<0, 2, 1>(ta, tb, p, (int)(m_tiles * p.splits), as_stream(stream));
 }

@@ -177,8 +177,9 @@ def merge_rescore(part_val, part_idx, n_queries: int, part_slots: int, n_cand: i
 
 
 def gemm_nt(A, B, out, alpha: float = 1.0, accumulate: bool = False, m_valid=None, n_valid=None, status=None,
-            lp_dtype: int = DT_BF16) -> torch.Tensor:
-    """out[:m_valid, :n_valid] = alpha * A @ B.T (+ out)."""
+            lp_dtype: int = DT_BF16, splits: int = 0) -> torch.Tensor:
+    """out[:m_valid, :n_valid] = alpha * A @ B.T (+ out). splits <= 0: one
+    256-row tile of B per work unit; else each unit streams 1/splits of B."""
     _cuda(A, "A")
     _cuda(B, "B")
     if status is None:
@@ -186,8 +187,8 @@ def gemm_nt(A, B, out, alpha: float = 1.0, accumulate: bool = False, m_valid=Non
     m_valid = A.shape[0] if m_valid is None else m_valid
     n_valid = B.shape[0] if n_valid is None else n_valid
     call("ebsd_gemm_nt", ptr(A), A.shape[0], ptr(B), B.shape[0], A.shape[1], lp_dtype, float(alpha),
-         int(bool(accumulate)), ptr(out), out.stride(0), int(m_valid), int(n_valid), ptr(status),
-         _stream(A.device))
+         int(bool(accumulate)), ptr(out), out.stride(0), int(m_valid), int(n_valid), int(splits),
+         ptr(status), _stream(A.device))
     return status
 
 

@@ -42,14 +42,18 @@ class _Conv:
         self.b = torch.zeros(cout, device=device)
         self.state = [torch.zeros_like(self.w), torch.zeros_like(self.w), torch.zeros_like(self.b),
                       torch.zeros_like(self.b)]
-        # bf16 copies read by the GEMMs: W (256 x K_pad) and W^T (K_pad256 x cout_pad64)
-        self.w16 = torch.zeros((256, self.K_pad), dtype=torch.bfloat16, device=device)
+        # bf16 copies read by the GEMMs: W (cout_pad128 x K_pad) and W^T (K_pad256 x cout_pad64)
+        self.w16 = torch.zeros((round_up(cout, 128), self.K_pad), dtype=torch.bfloat16, device=device)
         self.w16[:cout, :self.K] = self.w.bfloat16()
         self.ld_t = round_up(cout, 64)
         self.w16t = torch.zeros((round_up(self.K_pad, 256), self.ld_t), dtype=torch.bfloat16, device=device)
         self.w16t[:self.K, :cout] = self.w.t().bfloat16()
         self.gw = torch.zeros_like(self.w)
         self.gb = torch.zeros_like(self.b)
+        # device status word of the forward GEMM (non-zero after a timeout)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)
+        sms = torch.cuda.get_device_properties(device).multi_processor_count if self.w.is_cuda else 148
+        self.fwd_splits = max(1, 2 * sms // (self.w16.shape[0] // 128))
 
     def params(self):
         return [self.w, self.b]
@@ -57,13 +61,15 @@ class _Conv:
     def forward(self, x: torch.Tensor, B: int, H: int, W: int, keep: dict, want32: bool = False):
         Ho, Wo = (H + 1) // 2, (W + 1) // 2
         M = B * Ho * Wo
-        cols = torch.empty((M, self.K_pad), dtype=torch.bfloat16, device=x.device)
-        call("ebsd_cnn_im2col", ptr(x), B, H, W, self.cin, M, self.K_pad, ptr(cols), _stream(x))
-        y = torch.empty((M, self.cout), dtype=torch.float32, device=x.device)
-        kernels.gemm_nt(cols, self.w16, y, m_valid=M, n_valid=self.cout)
+        cols = torch.empty((round_up(M, 256), self.K_pad), dtype=torch.bfloat16, device=x.device)
+        call("ebsd_cnn_im2col", ptr(x), B, H, W, self.cin, cols.shape[0], self.K_pad, ptr(cols), _stream(x))
+        # one tcgen05 GEMM with the output channels on the 128-row side and
+        # the long pixel axis streamed in a few hundred units; bias, ReLU and
+        # the bf16 (and FP32) activation stores are fused into its epilogue
         out = torch.empty((M, self.cout), dtype=torch.bfloat16, device=x.device)
         out32 = torch.empty((M, self.cout), dtype=torch.float32, device=x.device) if want32 else None
-        call("ebsd_cnn_bias_act", ptr(y), self.cout, ptr(self.b), M, self.cout, 1, ptr(out), self.cout, ptr(out32),
+        call("ebsd_cnn_conv_fwd", ptr(self.w16), self.w16.shape[0], ptr(cols), cols.shape[0], self.K_pad,
+             ptr(self.b), self.cout, M, 1, ptr(out), self.cout, ptr(out32), self.fwd_splits, ptr(self.status),
              _stream(x))
         keep.update(cols=cols, out=out, M=M, H=H, W=W, B=B)
         return out, out32, Ho, Wo
@@ -153,8 +159,9 @@ class OrientationCNN:
         return sum(t.numel() for c in self.convs for t in c.params()) + sum(
             t.numel() for d in (self.fc1, self.fc2) for t in (d.w, d.b))
 
-    def forward(self, x: torch.Tensor) -> torch.Tensor:
-        """x: (B, H, W) float32 -> (B, 6) float32 6-D rotation outputs."""
+    def forward(self, x: torch.Tensor, keep: bool = True) -> torch.Tensor:
+        """x: (B, H, W) float32 -> (B, 6) float32 6-D rotation outputs. With
+        keep=False the activations needed by backward() are not retained."""
         B = x.shape[0]
         if B % 128:
             raise ValueError("batch size must be a multiple of 128")
@@ -164,14 +171,25 @@ class OrientationCNN:
         a, h, w = x16, self.H, self.W
         a32 = None
         for i, conv in enumerate(self.convs):
-            keep = {}
-            a, a32, h, w = conv.forward(a, B, h, w, keep, want32=(i == len(self.convs) - 1))
-            self._keep.append(keep)
+            saved = {}
+            a, a32, h, w = conv.forward(a, B, h, w, saved, want32=(i == len(self.convs) - 1))
+            if keep:
+                self._keep.append(saved)
         k1, k2 = {}, {}
         hid = self.fc1.forward(a32.view(B, -1), k1)
         out = self.fc2.forward(hid, k2)
-        self._keep += [k1, k2]
+        if keep:
+            self._keep += [k1, k2]
         return out
+
+    def check_status(self) -> None:
+        """Raise if a forward GEMM reported a device timeout (reads the
+        status words, so it synchronises)."""
+        for i, c in enumerate(self.convs):
+            st = int(c.status.item())
+            if st:
+                c.status.zero_()
+                raise RuntimeError(f"convolution {i} GEMM reported device status {st:#x}")
 
     def backward(self, dout: torch.Tensor) -> None:
         k1, k2 = self._keep[-2], self._keep[-1]
@@ -208,8 +226,8 @@ class OrientationCNN:
              _stream(out))
         return loss, grad
 
-    def predict_quaternions(self, x: torch.Tensor) -> torch.Tensor:
-        out = self.forward(x)
+    def predict_quaternions(self, x: torch.Tensor, keep: bool = False) -> torch.Tensor:
+        out = self.forward(x, keep=keep)
         qu = torch.empty((x.shape[0], 4), dtype=torch.float32, device=x.device)
         call("ebsd_zh_to_qu", ptr(out), out.shape[0], ptr(qu), None, _stream(out))
         return qu

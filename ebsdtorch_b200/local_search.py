@@ -72,6 +72,13 @@ def local_search(pd: PhaseDictionary, q_f32: torch.Tensor, proposals: torch.Tens
     return idx, score, ncand
 
 
+def cell_angle_deg(edge: int) -> float:
+    """Side of one cubochoric grid cell as a rotation angle near the identity:
+    the homochoric vector of a small rotation w is ~w/2 and the cube side is
+    pi^(2/3), so a cell spans ~2 pi^(2/3) / edge radians."""
+    return math.degrees(2.0 * math.pi ** (2.0 / 3.0) / edge)
+
+
 @dataclass
 class LearnedStats:
     n_patterns: int
@@ -79,33 +86,48 @@ class LearnedStats:
     median_local_score: float
     mean_candidates: float
     seconds: dict
+    stage_radii_deg: tuple = ()
+    stage_mean_candidates: tuple = ()
 
 
 def learned_dictionary_index(master_pattern, geometry, experiment_patterns, model, dictionary_resolution_degrees=0.5,
-                             max_angle_deg: float = 8.0, coarse_resolution_deg: Optional[float] = 2.0,
-                             fallback_ratio: float = 0.9, batch: int = 1024, precision: str = "bf16",
-                             rescore_k: int = 32, device=None,
+                             max_angle_deg: float = 12.0, pyramid_resolutions_deg=(2.0, 1.0),
+                             stage_margin: float = 1.25, fallback_ratio: float = 0.9, batch: int = 4096,
+                             precision: str = "bf16", rescore_k: int = 32, device=None,
                              phase_dictionary: Optional[PhaseDictionary] = None) -> LearnedStats:
-    """Top-1 indexing of one phase by learned proposal + local search with
-    plain-DI fallback. With coarse_resolution_deg the search runs in two
-    stages: within max_angle_deg of the proposal on a coarse dictionary, then
-    within 1.5 coarse spacings of the coarse winner on the full-resolution
-    dictionary (without it: one stage within max_angle_deg). Writes
-    raw_indexing_results / orientations like dictionary_index_orientations and
-    returns timing and fallback counts."""
+    """Top-1 indexing of one phase by learned proposal + coarse-to-fine local
+    search + plain-DI fallback.
+
+    Stage 0 searches the coarsest dictionary of `pyramid_resolutions_deg`
+    within `max_angle_deg` of each network proposal; stage k searches the
+    next finer dictionary within `stage_margin` cells of the previous stage's
+    cell size (cell_angle_deg) around the previous winner; the last stage is
+    the full-resolution dictionary, built exactly as for plain DI. Resolutions
+    not coarser than the full one are ignored; consecutive grid edges may
+    differ by at most 3x so that every stage radius fits the kernel's 8-cell
+    neighbourhood. Patterns whose final cosine falls below fallback_ratio x
+    the map's median (or that found no candidate) are re-indexed by full
+    plain DI against the resident rows. Writes raw_indexing_results /
+    orientations like dictionary_index_orientations; returns timings and
+    counts."""
     from .ebsd.indexing import _device, _master_pattern_tensor, _unit_rays_soa
 
     sec = {}
     dev = _device(master_pattern, device)
+    laue = master_pattern.laue_group
     t0 = time.perf_counter()
     rays = _unit_rays_soa(geometry, 1, None, dev)
     mp_t = _master_pattern_tensor(master_pattern, 1, dev)
-    pd = phase_dictionary or PhaseDictionary(mp_t, rays, master_pattern.laue_group, dictionary_resolution_degrees,
-                                             precision)
-    coarse = None
-    if coarse_resolution_deg is not None and coarse_resolution_deg > dictionary_resolution_degrees:
-        coarse = PhaseDictionary(mp_t, rays, master_pattern.laue_group, coarse_resolution_deg, precision,
-                                 permute=False)
+    pd = phase_dictionary or PhaseDictionary(mp_t, rays, laue, dictionary_resolution_degrees, precision)
+    levels = sorted({float(r) for r in (pyramid_resolutions_deg or ()) if r > dictionary_resolution_degrees},
+                    reverse=True)
+    stages = [PhaseDictionary(mp_t, rays, laue, r, precision, permute=False) for r in levels] + [pd]
+    radii = [float(max_angle_deg)] + [stage_margin * cell_angle_deg(d.edge) for d in stages[:-1]]
+    for d, r in zip(stages, radii):
+        need = int(math.ceil(r * (4.0 / 3.0) * d.edge / 199.0)) + 1
+        if need > 8:
+            raise ValueError(f"a {r:.2f} deg search on the edge-{d.edge} grid needs {need} > 8 cells; "
+                             "add a pyramid level or lower max_angle_deg")
     torch.cuda.synchronize(dev)
     sec["dictionary"] = time.perf_counter() - t0
     pats = experiment_patterns.patterns
@@ -126,21 +148,27 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
         nb_pad = -(-nb // 128) * 128
         x = torch.zeros((nb_pad, H, W), dtype=torch.float32, device=dev)
         x[:nb] = (q_f32[b0:b1] * (math.sqrt(P) / q_norm[b0:b1].clamp_min(1e-12))[:, None]).view(nb, H, W)
-        proposals[b0:b1] = model.predict_quaternions(x)[:nb]
+        proposals[b0:b1] = model.predict_quaternions(x, keep=False)[:nb]
     torch.cuda.synchronize(dev)
+    model.check_status()
     sec["proposals"] = time.perf_counter() - t0
     t0 = time.perf_counter()
-    if coarse is not None:
-        cidx, _, _ = local_search(coarse, q_f32, proposals, max_angle_deg)
-        found = cidx >= 0
-        refined = torch.where(found[:, None], kernels.gather_rows(coarse.quats, cidx.clamp_min(0)), proposals)
-        idx, score, ncand = local_search(pd, q_f32, refined.contiguous(), 1.5 * coarse_resolution_deg)
-        idx = torch.where(found, idx, torch.full_like(idx, -1))
-    else:
-        idx, score, ncand = local_search(pd, q_f32, proposals, max_angle_deg)
+    centers = proposals
+    found = torch.ones(Q, dtype=torch.bool, device=dev)
+    stage_cand = []
+    for k, (d, r) in enumerate(zip(stages, radii)):
+        idx, score, ncand = local_search(d, q_f32, centers, r)
+        stage_cand.append(ncand)
+        found &= idx >= 0
+        if k + 1 < len(stages):
+            centers = torch.where(found[:, None], kernels.gather_rows(d.quats, idx.clamp_min(0)), centers)
+    idx = torch.where(found, idx, torch.full_like(idx, -1))
     valid = idx >= 0
-    med = torch.median(score[valid]) if bool(valid.any()) else torch.tensor(0.0, device=dev)
-    fb = (~valid) | (score < fallback_ratio * med)
+    # fallback on the cosine (the raw dot also scales with the row norms)
+    cos = score / (q_norm * pd.rows.norm[idx.clamp_min(0)]).clamp_min(1e-30)
+    med = torch.median(cos[valid]) if bool(valid.any()) else torch.tensor(0.0, device=dev)
+    fb = (~valid) | (cos < fallback_ratio * med)
+    experiment_patterns.local_cosine_ratio = torch.where(valid, cos / med.clamp_min(1e-30), torch.zeros_like(cos))
     fb_rows = torch.nonzero(fb).reshape(-1)
     torch.cuda.synchronize(dev)
     sec["local_search"] = time.perf_counter() - t0
@@ -165,4 +193,6 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     experiment_patterns.dictionaries = {0: pd.quats}
     experiment_patterns.proposals = proposals
     experiment_patterns.combine_indexing_results(higher_is_better=True)
-    return LearnedStats(Q, n_fb, float(med), float(ncand.float().mean()), sec)
+    total = torch.stack(stage_cand).float()
+    return LearnedStats(Q, n_fb, float(med), float(total.sum(0).mean()), sec, tuple(radii),
+                        tuple(float(v) for v in total.mean(1).cpu()))

@@ -207,12 +207,14 @@ int ebsd_match_topk_noalloc(const void* queries_lp, int64_t n_queries, int64_t n
 /* ---- A11/A12: PCA -------------------------------------------------------------
  * C (m_valid x n_valid, row stride ldc) = alpha * A B^T (+ C if accumulate),
  * A (m_pad x k_pad), B (n_pad x k_pad) lp rows, m_pad % 128 == 0,
- * n_pad % 256 == 0. tcgen05 kernel with a store epilogue. Used for the
- * covariance (pca_covmat.py:53-91 einsum) and the PCA projections
- * (indexing.py:401, 421, 452 torch.matmul). */
+ * n_pad % 256 == 0. tcgen05 kernel with a store epilogue.
+ * splits <= 0 gives one 256-row B tile per work unit; splits > 0 makes each
+ * (A tile, B range) unit stream n_pad / 256 / splits B tiles. Used for the
+ * covariance (pca_covmat.py:53-91 einsum), the PCA projections
+ * (indexing.py:401, 421, 452 torch.matmul) and the CNN gradient GEMMs. */
 int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
                  int lp_dtype, float alpha, int accumulate, float* C, int64_t ldc, int64_t m_valid,
-                 int64_t n_valid, int* d_status, void* stream);
+                 int64_t n_valid, int splits, int* d_status, void* stream);
 
 /* Column means of an (n_rows x n_cols) fp32 matrix (row stride ld). */
 int ebsd_col_mean(const float* X, int64_t n_rows, int n_cols, int64_t ld, float* mean, void* stream);
@@ -268,6 +270,15 @@ int ebsd_rot6d_sym_loss(const float* zh, const float* q_true, int64_t n, int lau
  * activations as im2col + ebsd_gemm_nt; FP32 dense head; Adam). */
 int ebsd_cnn_im2col(const void* x, int B, int H, int W, int C, int64_t m_pad, int ld, void* cols, void* stream);
 int ebsd_cnn_col2im(const float* dcols, int64_t ld, int B, int H, int W, int C, float* dx, void* stream);
+/* Convolution forward as one tcgen05 GEMM with a fused epilogue:
+ * out[r, c] = act(sum_k cols[r, k] w16[c, k] + bias[c]) for rows r < n_rows
+ * and channels c < cout, stored bf16 (row stride ld_out) and, when out32 is
+ * not null, FP32 with the same layout. w16 (cout_pad x k_pad, cout_pad % 128
+ * == 0) and cols (rows_pad x k_pad, rows_pad % 256 == 0) are bf16, k_pad %
+ * 64 == 0; act is ReLU when relu != 0. splits as for ebsd_gemm_nt. */
+int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* cols, int64_t rows_pad, int64_t k_pad,
+                      const float* bias, int cout, int64_t n_rows, int relu, void* out16, int64_t ld_out,
+                      float* out32, int splits, int* d_status, void* stream);
 int ebsd_cnn_bias_act(const float* y, int64_t ldy, const float* bias, int64_t M, int C, int relu, void* out,
                       int64_t ld_out, float* out32, void* stream);
 int ebsd_cnn_relu_grad(const float* dy, int64_t ldy, const void* act, int64_t lda, int64_t M, int C, float* g32,

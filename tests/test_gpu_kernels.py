@@ -265,6 +265,14 @@ def test_gemm_nt_store_and_split3():
     assert int(st.item()) == 0
     ref = X.double().cpu() @ Vt.double().cpu().T
     assert (out.double().cpu() - ref).abs().max() <= 2e-5 * ref.abs().max()
+    # several B tiles streamed by one work unit give the same result
+    Wt = torch.from_numpy(rng.standard_normal((1000, 200))).float().to(DEV)
+    B4 = kernels.split3(Wt, 1, False, seg, round_up(1000, 256), 3 * seg)
+    o1 = torch.empty((300, 1000), device=DEV)
+    o2 = torch.empty((300, 1000), device=DEV)
+    kernels.gemm_nt(A3, B4, o1, m_valid=300, n_valid=1000)
+    assert int(kernels.gemm_nt(A3, B4, o2, m_valid=300, n_valid=1000, splits=2).item()) == 0
+    assert torch.equal(o1, o2)
     # transposed split: X^T X with centring
     mu = kernels.col_mean(X)
     segn = round_up(300, 64)

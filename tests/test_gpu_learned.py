@@ -90,6 +90,33 @@ def test_cnn_gradients_match_oracle():
     assert report["fc2.b"][1] < 1e-5  # FP32 head: exact
 
 
+@pytest.mark.parametrize("cin,cout,hw,batch", [(1, 32, 64, 1024), (64, 128, 16, 256), (256, 256, 8, 128)])
+def test_conv_forward_matches_fp32_convolution(cin, cout, hw, batch):
+    """Fused im2col GEMM + bias + ReLU (ebsd_cnn_conv_fwd) against an FP32
+    convolution of the same bf16-rounded input and weights; the first case
+    streams ~14 pixel tiles per work unit, the last uses two channel tiles."""
+    from ebsdtorch_b200.learned import _Conv
+
+    gen = torch.Generator().manual_seed(cin + cout)
+    conv = _Conv(cin, cout, gen, torch.device(DEV))
+    conv.b.copy_(torch.randn(cout, generator=gen).to(DEV) * 0.1)
+    x = torch.randn((batch, hw, hw, cin), generator=gen).to(DEV).bfloat16()
+    out, out32, ho, wo = conv.forward(x, batch, hw, hw, {}, want32=True)
+    torch.cuda.synchronize()
+    assert int(conv.status.item()) == 0
+    w = conv.w.bfloat16().float().view(cout, 3, 3, cin).permute(0, 3, 1, 2)
+    prev = torch.backends.cudnn.allow_tf32
+    torch.backends.cudnn.allow_tf32 = False
+    try:
+        ref = torch.nn.functional.conv2d(x.float().permute(0, 3, 1, 2), w, conv.b, stride=2, padding=1)
+    finally:
+        torch.backends.cudnn.allow_tf32 = prev
+    ref = torch.relu(ref).permute(0, 2, 3, 1).reshape(batch * ho * wo, cout)
+    scale = float(ref.abs().max())
+    assert float((out32 - ref).abs().max()) <= 1e-4 * scale
+    assert float((out.float() - ref).abs().max()) <= 8e-3 * scale
+
+
 def test_cnn_training_learns_orientations():
     """A short training run on projector-generated patterns lowers the
     symmetric rotation loss (400 steps of 128 fresh 64 x 64 patterns)."""

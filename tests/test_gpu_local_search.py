@@ -108,12 +108,11 @@ def test_trained_network_gain():
     pats = synthetic.synthetic_patterns(mp_t, geom, truth, mean_counts=200.0, seed=778)
     exp_l = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
-    st = learned_dictionary_index(mp, geom, exp_l, model, dictionary_resolution_degrees=1.0, max_angle_deg=8.0,
-                                  coarse_resolution_deg=3.0)
+    st = learned_dictionary_index(mp, geom, exp_l, model, dictionary_resolution_degrees=1.0)
     exp_u = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
     st_u = learned_dictionary_index(mp, geom, exp_u, OrientationCNN((64, 64), 11, seed=9, device=DEV),
-                                    dictionary_resolution_degrees=1.0, max_angle_deg=8.0, coarse_resolution_deg=3.0)
+                                    dictionary_resolution_degrees=1.0)
     exp_f = ExperimentPatterns(pats.clone())
     torch.manual_seed(5)
     dictionary_index_orientations(mp, geom, exp_f, dictionary_resolution_degrees=1.0, match_dtype=torch.float32)
@@ -121,6 +120,7 @@ def test_trained_network_gain():
     agree = (exp_l.raw_indexing_indices[0][:, 0] == full).float().mean().item()
     agree_u = (exp_u.raw_indexing_indices[0][:, 0] == full).float().mean().item()
     print({"trained_fallback": st.n_fallback, "untrained_fallback": st_u.n_fallback, "agree": agree,
-           "agree_untrained": agree_u, "final_loss": float(losses[-50:].mean())})
+           "agree_untrained": agree_u, "final_loss": float(losses[-50:].mean()), "radii": st.stage_radii_deg,
+           "stage_candidates": st.stage_mean_candidates})
     assert agree >= 0.97
     assert agree - agree_u >= 0.2
