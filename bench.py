@@ -445,7 +445,7 @@ def run_learned(args, wl):
         torch.manual_seed(0)
         learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
                                  max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
-                                 fallback_ratio=args.fallback_ratio)
+                                 fallback_ratio=args.fallback_ratio, stage_margin=args.stage_margin)
     torch.cuda.synchronize()
     with ClockSampler(int(dev.index or 0)) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -454,7 +454,7 @@ def run_learned(args, wl):
             torch.manual_seed(0)
             st = learned_dictionary_index(mp, geom, exp, model, dictionary_resolution_degrees=wl["res"],
                                           max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
-                                          fallback_ratio=args.fallback_ratio)
+                                          fallback_ratio=args.fallback_ratio, stage_margin=args.stage_margin)
         e1.record()
         torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) / 1e3 / args.steps
@@ -495,6 +495,7 @@ def run_learned(args, wl):
                     "fallback_fraction": st.n_fallback / st.n_patterns, "mean_candidates": st.mean_candidates,
                     "stage_radii_deg": st.stage_radii_deg, "stage_mean_candidates": st.stage_mean_candidates,
                     "proposal_error_deg": prop_err, "fallback_ratio": args.fallback_ratio,
+                    "stage_margin_cells": args.stage_margin,
                     "cosine_over_median_q01_05_50_95_99": ratio_q,
                     "stage_seconds": st.seconds, "train_seconds": t_train,
                     "final_train_loss": float(losses[-100:].mean()),
@@ -518,9 +519,10 @@ def main():
     ap.add_argument("--fp32-subset", type=int, default=4096)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--train-steps", type=int, default=3000)
-    ap.add_argument("--max-angle", type=float, default=12.0)
-    ap.add_argument("--fallback-ratio", type=float, default=0.9)
-    ap.add_argument("--pyramid", default="2.0,1.0", help="intermediate dictionary resolutions (deg), coarse first")
+    ap.add_argument("--max-angle", type=float, default=16.0)
+    ap.add_argument("--fallback-ratio", type=float, default=0.95)
+    ap.add_argument("--stage-margin", type=float, default=1.6)
+    ap.add_argument("--pyramid", default="3.0,1.5,0.75", help="intermediate dictionary resolutions (deg), coarse first")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -16,25 +16,93 @@ static int nblocks(int64_t n, int per = 256) {
 }
 
 // cols[(b, oy, ox), (ky, kx, c)] = x[b, 2 oy - 1 + ky, 2 ox - 1 + kx, c] (0 outside);
-// rows >= M and columns >= K of the padded (m_pad x ld) output are zero.
-__global__ void k_im2col(const __nv_bfloat16* __restrict__ x, int B, int H, int W, int C, int Ho, int Wo,
-                         int64_t m_pad, int ld, __nv_bfloat16* __restrict__ cols) {
-  const int64_t M = (int64_t)B * Ho * Wo;
-  const int K = 9 * C;
-  const int64_t total = m_pad * ld;
-  for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = t / ld;
-    const int k = (int)(t - r * ld);
-    __nv_bfloat16 v = __float2bfloat16_rn(0.f);
-    if (r < M && k < K) {
-      const int b = (int)(r / (Ho * Wo));
-      const int rem = (int)(r - (int64_t)b * Ho * Wo);
+// rows >= M and columns >= K of the padded output (row stride ld, ld % 8 == 0)
+// are zero. One thread per 8-column chunk of a row, consecutive threads on
+// consecutive chunks, so each warp's 16-byte stores are contiguous; with
+// C % 8 == 0 (vec) a chunk lies in one tap and is one 16-byte load. Rows
+// [r0, r0 + n_rows) per launch, with 32-bit chunk indices.
+__global__ void k_im2col(const __nv_bfloat16* __restrict__ x, int H, int W, int C, int Ho, int Wo, int M, int r0,
+                         int n_rows, int ld, int vec, __nv_bfloat16* __restrict__ cols) {
+  const int nj = ld >> 3;
+  const unsigned total = (unsigned)n_rows * (unsigned)nj;
+  const int K = 9 * C, hw = Ho * Wo;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int rl = (int)(t / (unsigned)nj);
+    const int j = (int)(t - (unsigned)rl * (unsigned)nj);
+    const int r = r0 + rl, k0 = 8 * j;
+    uint4 chunk = make_uint4(0u, 0u, 0u, 0u);
+    if (r < M && k0 < K) {
+      const int b = r / hw, rem = r - b * hw;
       const int oy = rem / Wo, ox = rem - oy * Wo;
-      const int tap = k / C, c = k - tap * C;
-      const int iy = 2 * oy - 1 + tap / 3, ix = 2 * ox - 1 + tap % 3;
-      if (iy >= 0 && iy < H && ix >= 0 && ix < W) v = x[(((int64_t)b * H + iy) * W + ix) * C + c];
+      if (vec) {
+        const int tap = k0 / C, c0 = k0 - tap * C;
+        const int iy = 2 * oy - 1 + tap / 3, ix = 2 * ox - 1 + tap % 3;
+        if (iy >= 0 && iy < H && ix >= 0 && ix < W)
+          chunk = __ldg(reinterpret_cast<const uint4*>(x + (((int64_t)b * H + iy) * W + ix) * C + c0));
+      } else {
+        __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          const int k = k0 + e;
+          __nv_bfloat16 val = __float2bfloat16_rn(0.f);
+          if (k < K) {
+            const int tap = k / C, c = k - tap * C;
+            const int iy = 2 * oy - 1 + tap / 3, ix = 2 * ox - 1 + tap % 3;
+            if (iy >= 0 && iy < H && ix >= 0 && ix < W) val = x[(((int64_t)b * H + iy) * W + ix) * C + c];
+          }
+          v[e] = val;
+        }
+        chunk = *reinterpret_cast<const uint4*>(v);
+      }
     }
-    cols[t] = v;
+    *reinterpret_cast<uint4*>(cols + (int64_t)r * ld + k0) = chunk;
+  }
+}
+
+// Direct convolution of a single-channel input (the first layer):
+// out[(b, oy, ox), c] = act(sum_{ky,kx} x[b, 2 oy - 1 + ky, 2 ox - 1 + kx] w[c, 3 ky + kx] + bias[c]),
+// one thread per output pixel and all COUT channels, weights (bf16, as the
+// GEMM path reads them) broadcast from shared memory, 16-byte stores.
+template <int COUT>
+__global__ void k_conv_c1(const __nv_bfloat16* __restrict__ x, int H, int W, int Ho, int Wo, int M,
+                          const __nv_bfloat16* __restrict__ w16, int ldw, const float* __restrict__ bias, int relu,
+                          __nv_bfloat16* __restrict__ out, float* __restrict__ out32) {
+  __shared__ float ws[COUT][9];
+  __shared__ float bs[COUT];
+  for (int i = threadIdx.x; i < COUT * 9; i += blockDim.x) ws[i / 9][i % 9] = __bfloat162float(w16[(i / 9) * ldw + i % 9]);
+  for (int i = threadIdx.x; i < COUT; i += blockDim.x) bs[i] = bias ? bias[i] : 0.f;
+  __syncthreads();
+  const int hw = Ho * Wo;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < M; r += gridDim.x * blockDim.x) {
+    const int b = r / hw, rem = r - b * hw;
+    const int oy = rem / Wo, ox = rem - oy * Wo;
+    float xv[9];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const int iy = 2 * oy - 1 + t / 3, ix = 2 * ox - 1 + t % 3;
+      xv[t] = (iy >= 0 && iy < H && ix >= 0 && ix < W) ? __bfloat162float(x[((int64_t)b * H + iy) * W + ix]) : 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < COUT; c += 8) {
+      float o[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        float acc = 0.f;
+#pragma unroll
+        for (int t = 0; t < 9; ++t) acc = fmaf(xv[t], ws[c + e][t], acc);
+        acc += bs[c + e];
+        o[e] = relu ? fmaxf(acc, 0.f) : acc;
+      }
+      __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = __float2bfloat16_rn(o[e]);
+      *reinterpret_cast<uint4*>(out + (int64_t)r * COUT + c) = *reinterpret_cast<const uint4*>(v);
+      if (out32) {
+        float4* d = reinterpret_cast<float4*>(out32 + (int64_t)r * COUT + c);
+        d[0] = make_float4(o[0], o[1], o[2], o[3]);
+        d[1] = make_float4(o[4], o[5], o[6], o[7]);
+      }
+    }
   }
 }
 
@@ -226,9 +294,43 @@ extern "C" int ebsd_cnn_im2col(const void* x, int B, int H, int W, int C, int64_
                                void* stream) {
   EBSD_ARG_CHECK(x && cols && B > 0 && H > 0 && W > 0 && C > 0, "ebsd_cnn_im2col: bad arguments");
   const int Ho = (H + 1) / 2, Wo = (W + 1) / 2;
-  EBSD_ARG_CHECK(ld >= 9 * C && m_pad >= (int64_t)B * Ho * Wo, "ebsd_cnn_im2col: output too small");
-  k_im2col<<<nblocks(m_pad * ld), 256, 0, CNN_STREAM>>>(reinterpret_cast<const __nv_bfloat16*>(x), B, H, W, C, Ho,
-                                                       Wo, m_pad, ld, reinterpret_cast<__nv_bfloat16*>(cols));
+  const int64_t M = (int64_t)B * Ho * Wo;
+  EBSD_ARG_CHECK(ld >= 9 * C && ld % 8 == 0 && m_pad >= M, "ebsd_cnn_im2col: output too small or ld % 8 != 0");
+  EBSD_ARG_CHECK(m_pad < INT32_MAX && (int64_t)B * H * W * C < ((int64_t)1 << 40), "ebsd_cnn_im2col: too large");
+  EBSD_ARG_CHECK(((uintptr_t)cols & 15) == 0, "ebsd_cnn_im2col: cols must be 16-byte aligned");
+  const int vec = (C % 8 == 0) && (((uintptr_t)x & 15) == 0);
+  const int64_t nj = ld / 8;
+  const int64_t rows_per = std::max<int64_t>(1, (INT32_MAX / 2) / nj);
+  for (int64_t r0 = 0; r0 < m_pad; r0 += rows_per) {
+    const int n_rows = (int)std::min(rows_per, m_pad - r0);
+    k_im2col<<<nblocks((int64_t)n_rows * nj), 256, 0, CNN_STREAM>>>(
+        reinterpret_cast<const __nv_bfloat16*>(x), H, W, C, Ho, Wo, (int)M, (int)r0, n_rows, ld, vec,
+        reinterpret_cast<__nv_bfloat16*>(cols));
+    EBSD_LAUNCH_CHECK();
+  }
+  return 0;
+}
+
+extern "C" int ebsd_cnn_conv_c1(const void* x, int B, int H, int W, const void* w16, int ldw, const float* bias,
+                                int cout, int relu, void* out16, float* out32, void* stream) {
+  EBSD_ARG_CHECK(x && w16 && out16 && B > 0 && H > 0 && W > 0 && ldw >= 9, "ebsd_cnn_conv_c1: bad arguments");
+  const int Ho = (H + 1) / 2, Wo = (W + 1) / 2;
+  const int64_t M = (int64_t)B * Ho * Wo;
+  EBSD_ARG_CHECK(M < INT32_MAX, "ebsd_cnn_conv_c1: too many output pixels");
+  EBSD_ARG_CHECK(((uintptr_t)out16 & 15) == 0 && ((uintptr_t)out32 & 15) == 0,
+                 "ebsd_cnn_conv_c1: outputs must be 16-byte aligned");
+  const int blocks = nblocks(M);
+  auto args = [&](auto kern) {
+    kern<<<blocks, 256, 0, CNN_STREAM>>>(reinterpret_cast<const __nv_bfloat16*>(x), H, W, Ho, Wo, (int)M,
+                                         reinterpret_cast<const __nv_bfloat16*>(w16), ldw, bias, relu,
+                                         reinterpret_cast<__nv_bfloat16*>(out16), out32);
+  };
+  switch (cout) {
+    case 16: args(k_conv_c1<16>); break;
+    case 32: args(k_conv_c1<32>); break;
+    case 64: args(k_conv_c1<64>); break;
+    default: EBSD_ARG_CHECK(false, "ebsd_cnn_conv_c1: cout %d not in {16, 32, 64}", cout);
+  }
   EBSD_LAUNCH_CHECK();
   return 0;
 }

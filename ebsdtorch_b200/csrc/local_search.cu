@@ -85,23 +85,108 @@ __device__ void qu_to_cu(const double q[4], double cu[3]) {
   for (int i = 0; i < 3; ++i) cu[i] = copysign(isnan(c[i]) ? 0.0 : c[i], h[i]);
 }
 
+struct LocalRows {
+  const float* f32;    // zero-mean FP32 rows (the reference metric)
+  int64_t ld_f32;
+  const void* lp;      // unit-norm low-precision rows (null: score in FP32)
+  int64_t ld_lp;
+  const float* norm;   // |row| (lp scoring: raw dot = norm * lp_scale * q . lp)
+  const float* lp_scale;
+  int n_rescore;       // lp scoring: FP32 re-score of the best n (0: none)
+};
+
+constexpr int kLocalWarps = kLocalThreads / 32;
+constexpr int kRescoreMax = kLocalWarps;
+
+// Keeps (v, i) lists sorted best-first (higher v, then lower i); identical in
+// all lanes of a warp.
+template <int R>
+__device__ __forceinline__ void keep_best(float (&bv)[R], int64_t (&bi)[R], float v, int64_t i) {
+  if (!(v > bv[R - 1] || (v == bv[R - 1] && i >= 0 && (bi[R - 1] < 0 || i < bi[R - 1])))) return;
+  bv[R - 1] = v;
+  bi[R - 1] = i;
+#pragma unroll
+  for (int j = R - 1; j > 0; --j) {
+    const bool sw = bv[j] > bv[j - 1] || (bv[j] == bv[j - 1] && bi[j] >= 0 && (bi[j - 1] < 0 || bi[j] < bi[j - 1]));
+    if (sw) {
+      const float tv = bv[j];
+      bv[j] = bv[j - 1];
+      bv[j - 1] = tv;
+      const int64_t ti = bi[j];
+      bi[j] = bi[j - 1];
+      bi[j - 1] = ti;
+    }
+  }
+}
+
+__device__ __forceinline__ bool better(float v, int64_t i, float bv, int64_t bi) {
+  return i >= 0 && (bi < 0 || v > bv || (v == bv && i < bi));
+}
+
+// Dot of the shared-memory FP32 query row with one low-precision row, whose
+// zero-padded length covers n_vec 16-byte chunks (query padded with zeros).
+template <int LP>
+__device__ __forceinline__ float lp_dot(const float* qrow, const uint4* __restrict__ d, int n_vec, int lane) {
+  float acc = 0.f;
+  for (int v = lane; v < n_vec; v += 32) {
+    const uint4 u = __ldg(d + v);
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+    if constexpr (LP == EBSD_DT_BF16) {
+      const float4 qa = reinterpret_cast<const float4*>(qrow)[2 * v];
+      const float4 qb = reinterpret_cast<const float4*>(qrow)[2 * v + 1];
+      const float qv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[e]));
+        acc = fmaf(f.x, qv[2 * e], acc);
+        acc = fmaf(f.y, qv[2 * e + 1], acc);
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float4 q4 = reinterpret_cast<const float4*>(qrow)[4 * v + e];
+        const __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[e] & 0xffffu), __NV_E4M3);
+        const __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[e] >> 16), __NV_E4M3);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&lo));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&hi));
+        acc = fmaf(a.x, q4.x, acc);
+        acc = fmaf(a.y, q4.y, acc);
+        acc = fmaf(b.x, q4.z, acc);
+        acc = fmaf(b.y, q4.w, acc);
+      }
+    }
+  }
+  return warp_sum(acc);
+}
+
+__device__ __forceinline__ float f32_dot(const float* qrow, const float* __restrict__ drow, int n_pix, int lane) {
+  float acc = 0.f;
+  for (int p = lane; p < n_pix; p += 32) acc = fmaf(__ldg(drow + p), qrow[p], acc);
+  return warp_sum(acc);
+}
+
+// LP 0: every candidate scored in FP32. LP = EBSD_DT_BF16 / EBSD_DT_E4M3:
+// candidates ranked by their low-precision rows (half or a quarter of the
+// bytes), then the best n_rescore re-scored in FP32 (or, with n_rescore 0,
+// the low-precision estimate of the best one returned).
+template <int LP>
 __global__ void __launch_bounds__(kLocalThreads) k_local_search(
     const float* __restrict__ q_f32, int64_t ld_q, const float4* __restrict__ proposals, const LaueTable ops,
-    int edge, const int32_t* __restrict__ cell_to_row, const float4* __restrict__ dict_quats,
-    const float* __restrict__ d_f32, int64_t ld_d, int64_t n_dict, int n_pix, int laue, int radius,
-    float cos_half_max, float fz_slack, int max_cand, int64_t* __restrict__ out_idx, float* __restrict__ out_score,
-    int32_t* __restrict__ out_ncand) {
+    int edge, const int32_t* __restrict__ cell_to_row, const float4* __restrict__ dict_quats, const LocalRows rows,
+    int64_t n_dict, int n_pix, int n_pix_pad, int laue, int radius, float cos_half_max, float fz_slack, int max_cand,
+    int64_t* __restrict__ out_idx, float* __restrict__ out_score, int32_t* __restrict__ out_ncand) {
   extern __shared__ float qrow[];
   __shared__ int cand[kMaxLocalCand];
   __shared__ int base_cell[24][3];
   __shared__ float4 copy_q[24];
   __shared__ int n_cand;
   __shared__ int copy_ok[24];
-  __shared__ float best_v[kLocalThreads / 32];
-  __shared__ int64_t best_i[kLocalThreads / 32];
+  __shared__ float best_v[kLocalWarps][kRescoreMax];
+  __shared__ int64_t best_i[kLocalWarps][kRescoreMax];
+  __shared__ int64_t sel[kRescoreMax];
   const int64_t q = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int p = tid; p < n_pix; p += blockDim.x) qrow[p] = q_f32[q * ld_q + p];
+  for (int p = tid; p < n_pix_pad; p += blockDim.x) qrow[p] = p < n_pix ? q_f32[q * ld_q + p] : 0.f;
   if (tid == 0) n_cand = 0;
   const double kHalf = 1.0725146985555127, step = 2.0 * kHalf / edge;
   if (tid < ops.n) {
@@ -141,34 +226,121 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
   }
   __syncthreads();
   const int nc = min(n_cand, max_cand);
-  float bv = -INFINITY;
-  int64_t bi = -1;
-  for (int c = wid; c < nc; c += blockDim.x / 32) {
-    const int64_t row = cand[c];
-    const float* drow = d_f32 + row * ld_d;
-    float acc = 0.f;
-    for (int p = lane; p < n_pix; p += 32) acc = fmaf(__ldg(drow + p), qrow[p], acc);
-    acc = warp_sum(acc);
-    if (acc > bv || (acc == bv && row < bi)) {
-      bv = acc;
-      bi = row;
+  float v_out = -INFINITY;
+  int64_t i_out = -1;
+  if constexpr (LP == 0) {
+    float bv = -INFINITY;
+    int64_t bi = -1;
+    for (int c = wid; c < nc; c += kLocalWarps) {
+      const int64_t row = cand[c];
+      const float acc = f32_dot(qrow, rows.f32 + row * rows.ld_f32, n_pix, lane);
+      if (better(acc, row, bv, bi)) {
+        bv = acc;
+        bi = row;
+      }
+    }
+    if (lane == 0) {
+      best_v[wid][0] = bv;
+      best_i[wid][0] = bi;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int w = 0; w < kLocalWarps; ++w)
+        if (better(best_v[w][0], best_i[w][0], v_out, i_out)) {
+          v_out = best_v[w][0];
+          i_out = best_i[w][0];
+        }
+    }
+  } else {
+    constexpr int kChunk = 16;  // bytes per vector load
+    const int n_vec = n_pix_pad / (LP == EBSD_DT_BF16 ? kChunk / 2 : kChunk);
+    float bv[kRescoreMax];
+    int64_t bi[kRescoreMax];
+#pragma unroll
+    for (int j = 0; j < kRescoreMax; ++j) {
+      bv[j] = -INFINITY;
+      bi[j] = -1;
+    }
+    const int esz = LP == EBSD_DT_BF16 ? 2 : 1;
+    for (int c = wid; c < nc; c += kLocalWarps) {
+      const int64_t row = cand[c];
+      const uint4* d = reinterpret_cast<const uint4*>(static_cast<const uint8_t*>(rows.lp) + row * rows.ld_lp * esz);
+      float acc = lp_dot<LP>(qrow, d, n_vec, lane);
+      acc *= __ldg(rows.norm + row) * (rows.lp_scale ? __ldg(rows.lp_scale + row) : 1.f);
+      keep_best<kRescoreMax>(bv, bi, acc, row);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int j = 0; j < kRescoreMax; ++j) {
+        best_v[wid][j] = bv[j];
+        best_i[wid][j] = bi[j];
+      }
+    }
+    __syncthreads();
+    const int n_sel = max(1, min(rows.n_rescore, kRescoreMax));
+    if (wid == 0) {
+      // merge the warps' lists: n_sel rounds of a warp-wide arg-max over the
+      // kLocalWarps x kRescoreMax entries (two per lane)
+      float* fv = &best_v[0][0];
+      int64_t* fi = &best_i[0][0];
+      for (int r = 0; r < n_sel; ++r) {
+        float v = -INFINITY;
+        int64_t i = -1;
+        int at = -1;
+        for (int e = lane; e < kLocalWarps * kRescoreMax; e += 32)
+          if (better(fv[e], fi[e], v, i)) {
+            v = fv[e];
+            i = fi[e];
+            at = e;
+          }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+          const int64_t oi = __shfl_xor_sync(0xffffffffu, i, o);
+          const int oat = __shfl_xor_sync(0xffffffffu, at, o);
+          if (better(ov, oi, v, i)) {
+            v = ov;
+            i = oi;
+            at = oat;
+          }
+        }
+        if (lane == 0) {
+          sel[r] = i;
+          if (r == 0) {
+            v_out = v;
+            i_out = i;
+          }
+          if (at >= 0) fi[at] = -1;
+        }
+        __syncwarp();
+      }
+    }
+    if (rows.n_rescore > 0) {
+      __syncthreads();
+      // FP32 re-score: warp w takes the w-th selected row
+      if (wid < n_sel) {
+        const int64_t row = sel[wid];
+        const float acc = row >= 0 ? f32_dot(qrow, rows.f32 + row * rows.ld_f32, n_pix, lane) : -INFINITY;
+        if (lane == 0) {
+          best_v[wid][0] = acc;
+          best_i[wid][0] = row;
+        }
+      }
+      __syncthreads();
+      if (tid == 0) {
+        v_out = -INFINITY;
+        i_out = -1;
+        for (int w = 0; w < n_sel; ++w)
+          if (better(best_v[w][0], best_i[w][0], v_out, i_out)) {
+            v_out = best_v[w][0];
+            i_out = best_i[w][0];
+          }
+      }
     }
   }
-  if (lane == 0) {
-    best_v[wid] = bv;
-    best_i[wid] = bi;
-  }
-  __syncthreads();
   if (tid == 0) {
-    float v = -INFINITY;
-    int64_t i = -1;
-    for (int w = 0; w < (int)(blockDim.x / 32); ++w)
-      if (best_i[w] >= 0 && (best_v[w] > v || (best_v[w] == v && best_i[w] < i))) {
-        v = best_v[w];
-        i = best_i[w];
-      }
-    out_idx[q] = i;
-    out_score[q] = v;
+    out_idx[q] = i_out;
+    out_score[q] = v_out;
     if (out_ncand) out_ncand[q] = n_cand;
   }
 }
@@ -209,9 +381,10 @@ extern "C" int ebsd_cell_to_row(const int32_t* cells, const int64_t* perm, int64
 
 extern "C" int ebsd_local_search(const float* q_f32, int64_t ld_q, int64_t n_queries, const float* proposals,
                                  int laue_id, int edge_length, const int32_t* cell_to_row, const float* dict_quats,
-                                 const float* d_f32, int64_t ld_d, int64_t n_dict, int n_pix, int radius_cells,
-                                 float max_angle_rad, int max_candidates, int64_t* out_idx, float* out_score,
-                                 int32_t* out_ncand, void* stream) {
+                                 const float* d_f32, int64_t ld_d, const void* d_lp, int lp_dtype, int64_t ld_lp,
+                                 const float* d_norm, const float* d_lp_scale, int n_rescore, int64_t n_dict,
+                                 int n_pix, int radius_cells, float max_angle_rad, int max_candidates,
+                                 int64_t* out_idx, float* out_score, int32_t* out_ncand, void* stream) {
   EBSD_ARG_CHECK(q_f32 && proposals && cell_to_row && dict_quats && d_f32 && out_idx && out_score,
                  "ebsd_local_search: null pointer");
   EBSD_ARG_CHECK(laue_id >= 1 && laue_id <= 11, "Laue group %d is not supported", laue_id);
@@ -223,16 +396,35 @@ extern "C" int ebsd_local_search(const float* q_f32, int64_t ld_q, int64_t n_que
   EBSD_ARG_CHECK(n_pix >= 1 && n_pix <= 40960 && ld_q >= n_pix && ld_d >= n_pix, "bad row length");
   EBSD_ARG_CHECK(((uintptr_t)proposals & 15) == 0 && ((uintptr_t)dict_quats & 15) == 0,
                  "quaternion arrays must be 16-byte aligned");
+  int n_pix_pad = n_pix;
+  if (d_lp) {
+    EBSD_ARG_CHECK(lp_dtype == EBSD_DT_BF16 || lp_dtype == EBSD_DT_E4M3, "bad lp_dtype");
+    EBSD_ARG_CHECK(d_norm != nullptr && (lp_dtype == EBSD_DT_BF16 || d_lp_scale != nullptr),
+                   "low-precision scoring needs the row norms (and e4m3 scales)");
+    EBSD_ARG_CHECK(n_rescore >= 0 && n_rescore <= kRescoreMax, "n_rescore must be in [0, %d]", kRescoreMax);
+    const int per = lp_dtype == EBSD_DT_BF16 ? 8 : 16;
+    n_pix_pad = (n_pix + per - 1) / per * per;
+    const int esz = lp_dtype == EBSD_DT_BF16 ? 2 : 1;
+    // the vector loads read n_pix_pad elements: the row padding must cover
+    // them (and be zero, as the projector writes it)
+    EBSD_ARG_CHECK(ld_lp >= n_pix_pad && (ld_lp * esz) % 16 == 0 && ((uintptr_t)d_lp & 15) == 0,
+                   "low-precision rows must be 16-byte aligned with ld_lp >= %d", n_pix_pad);
+  }
   if (n_queries == 0) return 0;
   EBSD_ARG_CHECK(n_queries < INT32_MAX, "too many queries");
   LaueTable t{};
   build_laue_table(laue_id, &t);
-  const size_t smem = (size_t)n_pix * sizeof(float);
-  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_local_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_local_search<<<(int)n_queries, kLocalThreads, smem, as_stream(stream)>>>(
-      q_f32, ld_q, reinterpret_cast<const float4*>(proposals), t, edge_length, cell_to_row,
-      reinterpret_cast<const float4*>(dict_quats), d_f32, ld_d, n_dict, n_pix, laue_id, radius_cells,
-      cosf(0.5f * max_angle_rad), 2.25f * max_angle_rad + 1e-3f, max_candidates, out_idx, out_score, out_ncand);
-  EBSD_LAUNCH_CHECK();
-  return 0;
+  LocalRows rows{d_f32, ld_d, d_lp, ld_lp, d_norm, d_lp_scale, n_rescore};
+  const size_t smem = (size_t)n_pix_pad * sizeof(float);
+  auto run = [&](auto kern) -> int {
+    EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kern<<<(int)n_queries, kLocalThreads, smem, as_stream(stream)>>>(
+        q_f32, ld_q, reinterpret_cast<const float4*>(proposals), t, edge_length, cell_to_row,
+        reinterpret_cast<const float4*>(dict_quats), rows, n_dict, n_pix, n_pix_pad, laue_id, radius_cells,
+        cosf(0.5f * max_angle_rad), 2.25f * max_angle_rad + 1e-3f, max_candidates, out_idx, out_score, out_ncand);
+    EBSD_LAUNCH_CHECK();
+    return 0;
+  };
+  if (!d_lp) return run(k_local_search<0>);
+  return lp_dtype == EBSD_DT_BF16 ? run(k_local_search<EBSD_DT_BF16>) : run(k_local_search<EBSD_DT_E4M3>);
 }

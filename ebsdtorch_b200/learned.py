@@ -6,8 +6,10 @@ Architecture: five 3x3 / stride-2 / pad-1 convolutions with ReLU
 4 x 4 x 256), then a two-layer head (4096 -> 64 with ReLU, 64 -> 6) that
 predicts the 6-D rotation representation of Zhou et al. (orientations.py:940);
 1.24 M parameters. Convolutions run in bf16 on the tcgen05 GEMM (im2col
-forward; weight- and column-gradient GEMMs + col2im backward), the head in
-FP32. The loss is the symmetry-aware rotation loss min_g ||R(z) - R(q g)||_F^2
+forward with bias, ReLU and the activation stores fused into the GEMM
+epilogue; weight- and column-gradient GEMMs + col2im backward), except the
+single-channel first layer, computed directly on the CUDA cores; the head in
+FP32. The loss is the symmetry-aware rotation loss min_g ||R(z) - R(g q)||_F^2
 (ebsd_rot6d_sym_loss), optimiser Adam on FP32 master weights.
 
 This part has no counterpart in the reference (ebsdtorch has no learned
@@ -58,20 +60,32 @@ class _Conv:
     def params(self):
         return [self.w, self.b]
 
+    def _im2col(self, x: torch.Tensor, B: int, H: int, W: int) -> torch.Tensor:
+        M = B * ((H + 1) // 2) * ((W + 1) // 2)
+        cols = torch.empty((round_up(M, 256), self.K_pad), dtype=torch.bfloat16, device=x.device)
+        call("ebsd_cnn_im2col", ptr(x), B, H, W, self.cin, cols.shape[0], self.K_pad, ptr(cols), _stream(x))
+        return cols
+
     def forward(self, x: torch.Tensor, B: int, H: int, W: int, keep: dict, want32: bool = False):
         Ho, Wo = (H + 1) // 2, (W + 1) // 2
         M = B * Ho * Wo
-        cols = torch.empty((round_up(M, 256), self.K_pad), dtype=torch.bfloat16, device=x.device)
-        call("ebsd_cnn_im2col", ptr(x), B, H, W, self.cin, cols.shape[0], self.K_pad, ptr(cols), _stream(x))
-        # one tcgen05 GEMM with the output channels on the 128-row side and
-        # the long pixel axis streamed in a few hundred units; bias, ReLU and
-        # the bf16 (and FP32) activation stores are fused into its epilogue
         out = torch.empty((M, self.cout), dtype=torch.bfloat16, device=x.device)
         out32 = torch.empty((M, self.cout), dtype=torch.float32, device=x.device) if want32 else None
-        call("ebsd_cnn_conv_fwd", ptr(self.w16), self.w16.shape[0], ptr(cols), cols.shape[0], self.K_pad,
-             ptr(self.b), self.cout, M, 1, ptr(out), self.cout, ptr(out32), self.fwd_splits, ptr(self.status),
-             _stream(x))
-        keep.update(cols=cols, out=out, M=M, H=H, W=W, B=B)
+        if self.cin == 1:
+            # 9 taps: a direct SIMT convolution beats a GEMM padded to K = 64
+            call("ebsd_cnn_conv_c1", ptr(x), B, H, W, ptr(self.w16), self.K_pad, ptr(self.b), self.cout, 1, ptr(out),
+                 ptr(out32), _stream(x))
+            keep.update(x=x)
+        else:
+            # one tcgen05 GEMM with the output channels on the 128-row side and
+            # the long pixel axis streamed in a few hundred units; bias, ReLU
+            # and the bf16 (and FP32) activation stores are fused into its epilogue
+            cols = self._im2col(x, B, H, W)
+            call("ebsd_cnn_conv_fwd", ptr(self.w16), self.w16.shape[0], ptr(cols), cols.shape[0], self.K_pad,
+                 ptr(self.b), self.cout, M, 1, ptr(out), self.cout, ptr(out32), self.fwd_splits, ptr(self.status),
+                 _stream(x))
+            keep.update(cols=cols)
+        keep.update(out=out, M=M, H=H, W=W, B=B)
         return out, out32, Ho, Wo
 
     def backward(self, dout: torch.Tensor, keep: dict, need_dx: bool) -> Optional[torch.Tensor]:
@@ -88,7 +102,8 @@ class _Conv:
         gT = torch.empty((round_up(self.cout, 128), M), dtype=torch.bfloat16, device=dev)
         call("ebsd_cnn_transpose", ptr(g16), 0, M, self.cout, ld16, ptr(gT), gT.shape[0], M, s)
         colsT = torch.empty((round_up(self.K_pad, 256), M), dtype=torch.bfloat16, device=dev)
-        call("ebsd_cnn_transpose", ptr(keep["cols"]), 0, M, self.K_pad, self.K_pad, ptr(colsT), colsT.shape[0], M, s)
+        cols = keep["cols"] if "cols" in keep else self._im2col(keep["x"], B, H, W)
+        call("ebsd_cnn_transpose", ptr(cols), 0, M, self.K_pad, self.K_pad, ptr(colsT), colsT.shape[0], M, s)
         kernels.gemm_nt(gT, colsT, self.gw, m_valid=self.cout, n_valid=self.K)
         if not need_dx:
             return None

@@ -57,17 +57,25 @@ class PhaseDictionary:
 
 
 def local_search(pd: PhaseDictionary, q_f32: torch.Tensor, proposals: torch.Tensor, max_angle_deg: float = 3.0,
-                 radius_cells: Optional[int] = None, max_candidates: int = 1024):
-    """Best dictionary row near each proposal: (index int64, exact FP32 score,
-    candidate count int32), -1 / -inf when no candidate lies in the radius."""
+                 radius_cells: Optional[int] = None, max_candidates: int = 1024, n_rescore: Optional[int] = None):
+    """Best dictionary row near each proposal: (index int64, score, candidate
+    count int32), -1 / -inf when no candidate lies in the radius.
+
+    n_rescore None: every candidate scored by the exact FP32 dot. Otherwise
+    candidates are ranked by the dictionary's low-precision rows and the best
+    n_rescore (<= 8) re-scored in FP32; n_rescore 0 returns the low-precision
+    estimate (enough to seed a finer stage)."""
     Q = q_f32.shape[0]
     dev = q_f32.device
     idx = torch.empty(Q, dtype=torch.int64, device=dev)
     score = torch.empty(Q, dtype=torch.float32, device=dev)
     ncand = torch.empty(Q, dtype=torch.int32, device=dev)
     r = pd.default_radius(max_angle_deg) if radius_cells is None else radius_cells
+    rows = pd.rows
+    lp = rows.lp if n_rescore is not None else None
     call("ebsd_local_search", ptr(q_f32), q_f32.stride(0), Q, ptr(proposals.contiguous()), pd.laue, pd.edge,
-         ptr(pd.cell_to_row), ptr(pd.quats), ptr(pd.rows.f32), pd.rows.f32.stride(0), pd.n, pd.n_pix, r,
+         ptr(pd.cell_to_row), ptr(pd.quats), ptr(rows.f32), rows.f32.stride(0), ptr(lp), rows.lp_dtype,
+         rows.lp.stride(0), ptr(rows.norm), ptr(rows.lp_scale), int(n_rescore or 0), pd.n, pd.n_pix, r,
          math.radians(max_angle_deg), max_candidates, ptr(idx), ptr(score), ptr(ncand), _stream(dev))
     return idx, score, ncand
 
@@ -91,8 +99,9 @@ class LearnedStats:
 
 
 def learned_dictionary_index(master_pattern, geometry, experiment_patterns, model, dictionary_resolution_degrees=0.5,
-                             max_angle_deg: float = 12.0, pyramid_resolutions_deg=(2.0, 1.0),
-                             stage_margin: float = 1.25, fallback_ratio: float = 0.9, batch: int = 4096,
+                             max_angle_deg: float = 16.0, pyramid_resolutions_deg=(3.0, 1.5, 0.75),
+                             stage_margin: float = 1.6, fallback_ratio: float = 0.95, n_rescore: int = 8,
+                             batch: int = 4096,
                              precision: str = "bf16", rescore_k: int = 32, device=None,
                              phase_dictionary: Optional[PhaseDictionary] = None) -> LearnedStats:
     """Top-1 indexing of one phase by learned proposal + coarse-to-fine local
@@ -107,7 +116,9 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     differ by at most 3x so that every stage radius fits the kernel's 8-cell
     neighbourhood. Patterns whose final cosine falls below fallback_ratio x
     the map's median (or that found no candidate) are re-indexed by full
-    plain DI against the resident rows. Writes raw_indexing_results /
+    plain DI against the resident rows. Every stage ranks its candidates
+    by the dictionaries' low-precision rows; the last re-scores its best
+    n_rescore in FP32. Writes raw_indexing_results /
     orientations like dictionary_index_orientations; returns timings and
     counts."""
     from .ebsd.indexing import _device, _master_pattern_tensor, _unit_rays_soa
@@ -157,7 +168,10 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     found = torch.ones(Q, dtype=torch.bool, device=dev)
     stage_cand = []
     for k, (d, r) in enumerate(zip(stages, radii)):
-        idx, score, ncand = local_search(d, q_f32, centers, r)
+        last = k + 1 == len(stages)
+        # candidates ranked by the low-precision rows; only the last stage
+        # re-scores its best n_rescore in FP32 (the reference metric)
+        idx, score, ncand = local_search(d, q_f32, centers, r, n_rescore=n_rescore if last else 0)
         stage_cand.append(ncand)
         found &= idx >= 0
         if k + 1 < len(stages):

@@ -246,13 +246,20 @@ int ebsd_disori_angle(const float* q1, const float* q2, int64_t n, int laue_id, 
  * max_angle_rad of a symmetric copy of proposals[q] that lie in the grid cells
  * within radius_cells of that copy are scored by the exact FP32 dot of
  * q_f32[q] with d_f32[row]; the best row and score are written (ties: lower
- * row; -1 / -inf when no candidate), and the candidate count if out_ncand. */
+ * row; -1 / -inf when no candidate), and the candidate count if out_ncand.
+ * With d_lp (unit-norm bf16 / e4m3 rows as the projector writes them, row
+ * stride ld_lp, zero padding) candidates are first ranked by
+ * d_norm * d_lp_scale * (q . lp) and only the best n_rescore (<= 8) are
+ * re-scored in FP32; n_rescore 0 returns the low-precision estimate of the
+ * best candidate (for intermediate coarse-to-fine stages). */
 int ebsd_cell_to_row(const int32_t* cells, const int64_t* perm, int64_t n, int64_t n_cells, int32_t* cell_to_row,
                      void* stream);
 int ebsd_local_search(const float* q_f32, int64_t ld_q, int64_t n_queries, const float* proposals, int laue_id,
                       int edge_length, const int32_t* cell_to_row, const float* dict_quats, const float* d_f32,
-                      int64_t ld_d, int64_t n_dict, int n_pix, int radius_cells, float max_angle_rad,
-                      int max_candidates, int64_t* out_idx, float* out_score, int32_t* out_ncand, void* stream);
+                      int64_t ld_d, const void* d_lp, int lp_dtype, int64_t ld_lp, const float* d_norm,
+                      const float* d_lp_scale, int n_rescore, int64_t n_dict, int n_pix, int radius_cells,
+                      float max_angle_rad, int max_candidates, int64_t* out_idx, float* out_score,
+                      int32_t* out_ncand, void* stream);
 
 /* ---- A15: 6-D rotation representation and the learned proposal ------------
  * 6-D (Zhou et al.) -> quaternion (orientations.py:986-1005 zh2qu: Gram-Schmidt
@@ -262,13 +269,21 @@ int ebsd_zh_to_qu(const float* zh, int64_t n, float* out_qu, float* out_om, void
 int ebsd_qu_to_zh(const float* qu, int64_t n, float* out_zh, void* stream);
 /* Training objective of the orientation-proposal network (no counterpart in
  * the reference): loss[i] = min over the Laue operators g of
- * ||zh2om(zh[i]) - om(q_true[i] g)||_F^2 and grad = grad_scale * dloss/dzh. */
+ * ||zh2om(zh[i]) - om(g q_true[i])||_F^2 (crystal symmetry acts on the left)
+ * and grad = grad_scale * dloss/dzh. */
 int ebsd_rot6d_sym_loss(const float* zh, const float* q_true, int64_t n, int laue_id, float grad_scale,
                         float* out_loss, float* out_grad, void* stream);
 
 /* CNN building blocks (3x3 / stride 2 / pad 1 convolutions on NHWC bf16
- * activations as im2col + ebsd_gemm_nt; FP32 dense head; Adam). */
+ * activations as im2col + tcgen05 GEMM; FP32 dense head; Adam).
+ * im2col: cols (m_pad x ld bf16, ld % 8 == 0, 16-byte aligned) gets the
+ * patches of x (B x H x W x C), zero rows/columns as padding. */
 int ebsd_cnn_im2col(const void* x, int B, int H, int W, int C, int64_t m_pad, int ld, void* cols, void* stream);
+/* First-layer (single input channel) convolution computed directly:
+ * out16 / out32 ((B Ho Wo) x cout, 16-byte aligned; out32 may be null) =
+ * act(conv(x, w16[:, :9]) + bias), cout in {16, 32, 64}, w16 row stride ldw. */
+int ebsd_cnn_conv_c1(const void* x, int B, int H, int W, const void* w16, int ldw, const float* bias, int cout,
+                     int relu, void* out16, float* out32, void* stream);
 int ebsd_cnn_col2im(const float* dcols, int64_t ld, int B, int H, int W, int C, float* dx, void* stream);
 /* Convolution forward as one tcgen05 GEMM with a fused epilogue:
  * out[r, c] = act(sum_k cols[r, k] w16[c, k] + bias[c]) for rows r < n_rows

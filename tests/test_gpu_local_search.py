@@ -57,6 +57,17 @@ def test_local_search_matches_bruteforce_oracle():
         ok = ri >= 0
         assert np.abs(score.cpu().numpy()[ok] - rv[ok]).max() <= 1e-5 * np.abs(rv[ok]).max()
         assert int(ncand.min()) >= 0
+        # candidates ranked by the bf16 rows, best 8 re-scored in FP32
+        li, ls, lc = local_search(pd, q_f32, prop_t, max_angle_deg=max_deg, n_rescore=8)
+        assert torch.equal(lc, ncand)
+        li_n = li.cpu().numpy()
+        assert (li_n == ri).mean() >= 0.99, (max_deg, (li_n == ri).mean())
+        same = (li_n == ri) & ok
+        assert np.abs(ls.cpu().numpy()[same] - rv[same]).max() <= 1e-5 * np.abs(rv[ok]).max()
+        # no re-score: the bf16 estimate of the bf16-best candidate
+        ei, es, _ = local_search(pd, q_f32, prop_t, max_angle_deg=max_deg, n_rescore=0)
+        assert (ei.cpu().numpy() == ri).mean() >= 0.9
+        assert np.abs(es.cpu().numpy()[ok] - rv[ok]).max() <= 1e-2 * np.abs(rv[ok]).max()
 
 
 def test_local_search_near_plain_di_answer_reproduces_it():
