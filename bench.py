@@ -233,11 +233,12 @@ def _reference_rows_torch(mp, rays, quats):
     return out - out.mean(dim=-1, keepdim=True)
 
 
-def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192):
+def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, return_values=False):
     """The reference's plain FP32 DI loop on the GPU (torch eager, TF32 off):
     per dictionary chunk, project it, then query @ chunk.T in FP32, chunk
     top-k and a running top-k merge (knn.py:80-103, 219-266). Returns
-    (indices (Q, k), seconds spent projecting, seconds spent matching)."""
+    (indices (Q, k), seconds spent projecting, seconds spent matching), and
+    the sorted FP32 values as a fourth item with return_values."""
     import torch
 
     torch.backends.cuda.matmul.allow_tf32 = False
@@ -260,6 +261,8 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192):
         t_proj += t1 - t0
         t_match += time.perf_counter() - t1
     order = torch.topk(best_v, k, dim=1, largest=True, sorted=True)[1]
+    if return_values:
+        return torch.gather(best_i, 1, order), t_proj, t_match, torch.gather(best_v, 1, order)
     return torch.gather(best_i, 1, order), t_proj, t_match
 
 

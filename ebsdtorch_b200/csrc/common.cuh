@@ -156,6 +156,32 @@ __device__ __forceinline__ float warp_max(float v) {
   return v;
 }
 
+// Dots of a shared-memory FP32 row with R FP32 rows of n4 float4 chunks
+// (16-byte aligned); every lane keeps R independent 16-byte loads in flight.
+// All lanes get the sums.
+template <int R>
+__device__ __forceinline__ void f32_dot_rows(const float* qrow, const float* const (&d)[R], int n4, int lane,
+                                             float (&acc)[R]) {
+#pragma unroll
+  for (int j = 0; j < R; ++j) acc[j] = 0.f;
+  const float4* q4 = reinterpret_cast<const float4*>(qrow);
+  for (int v = lane; v < n4; v += 32) {
+    float4 x[R];
+#pragma unroll
+    for (int j = 0; j < R; ++j) x[j] = __ldg(reinterpret_cast<const float4*>(d[j]) + v);
+    const float4 y = q4[v];
+#pragma unroll
+    for (int j = 0; j < R; ++j) {
+      acc[j] = fmaf(x[j].x, y.x, acc[j]);
+      acc[j] = fmaf(x[j].y, y.y, acc[j]);
+      acc[j] = fmaf(x[j].z, y.z, acc[j]);
+      acc[j] = fmaf(x[j].w, y.w, acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < R; ++j) acc[j] = warp_sum(acc[j]);
+}
+
 // Block-wide sum; `red` must hold one slot per warp. All threads get the sum.
 template <typename T>
 __device__ __forceinline__ T block_sum(T v, T* red) {

@@ -18,7 +18,7 @@
 
 namespace ebsd {
 
-constexpr int kRowThreads = 256;
+constexpr int kRowThreads = 512;
 constexpr int kMaxRowPix = 57344;  // 224 KiB of fp32 in shared memory
 
 __device__ __forceinline__ float2 lambert_side_by_side(float x, float y, float z) {
@@ -75,21 +75,20 @@ struct RowOut {
   float* lp_scale;
 };
 
-// Row values are in row[0..n). Finalise and write outputs for `r`.
-__device__ void finalize_row(float* row, int n, int subtract_mean, int64_t r, const RowOut& o,
-                             float* fred, double* dred) {
+// Row values are in row[0..n); part_sum is this thread's sum of the values it
+// wrote. Finalise and write the outputs of row `r` (the shared row itself is
+// left as it was): mean (FP64 block sum), then the norm and absmax of the
+// zero-mean row, then the FP32 and low-precision rows in one pass (16-byte
+// stores when the row length and strides allow).
+__device__ void finalize_row(const float* row, int n, int subtract_mean, float part_sum, int64_t r,
+                             const RowOut& o, float* fred, double* dred) {
   const int tid = threadIdx.x;
   double mean = 0.0;
-  if (subtract_mean) {
-    float s = 0.0f;
-    for (int p = tid; p < n; p += blockDim.x) s += row[p];
-    mean = block_sum<double>((double)s, dred) / (double)n;
-  }
+  if (subtract_mean) mean = block_sum<double>((double)part_sum, dred) / (double)n;
   const float meanf = (float)mean;
   float ss = 0.0f, amax = 0.0f;
   for (int p = tid; p < n; p += blockDim.x) {
     const float v = row[p] - meanf;
-    row[p] = v;
     ss += v * v;
     amax = fmaxf(amax, fabsf(v));
   }
@@ -105,21 +104,42 @@ __device__ void finalize_row(float* row, int n, int subtract_mean, int64_t r, co
     if (o.norm) o.norm[r] = nrm;
     if (o.lp_scale) o.lp_scale[r] = qscale;
   }
-  if (o.f32) {
-    float* dst = o.f32 + r * o.ld_f32;
-    for (int p = tid; p < n; p += blockDim.x) dst[p] = row[p];
-  }
-  if (o.lp) {
-    if (o.lp_dtype == EBSD_DT_BF16) {
-      __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(o.lp) + r * o.ld_lp;
-      for (int p = tid; p < o.ld_lp; p += blockDim.x)
-        dst[p] = __float2bfloat16_rn(p < n ? row[p] * inv : 0.0f);
-    } else {
-      __nv_fp8_e4m3* dst = reinterpret_cast<__nv_fp8_e4m3*>(o.lp) + r * o.ld_lp;
-      const float s = inv / qscale;
-      for (int p = tid; p < o.ld_lp; p += blockDim.x)
-        dst[p] = __nv_fp8_e4m3(p < n ? row[p] * s : 0.0f);
+  float* f32 = o.f32 ? o.f32 + r * o.ld_f32 : nullptr;
+  const bool bf16 = o.lp && o.lp_dtype == EBSD_DT_BF16;
+  __nv_bfloat16* lp16 = bf16 ? reinterpret_cast<__nv_bfloat16*>(o.lp) + r * o.ld_lp : nullptr;
+  const bool vec = (n & 7) == 0 && (!f32 || ((reinterpret_cast<uintptr_t>(f32) & 15) == 0)) &&
+                   (!lp16 || ((reinterpret_cast<uintptr_t>(lp16) & 15) == 0)) && (o.lp == nullptr || bf16);
+  if (vec) {
+    // eight values per thread and step: two float4 loads and stores, one
+    // 16-byte bf16 store
+    for (int c = tid; c < n / 8; c += blockDim.x) {
+      const float4 a = reinterpret_cast<const float4*>(row)[2 * c];
+      const float4 b = reinterpret_cast<const float4*>(row)[2 * c + 1];
+      const float v[8] = {a.x - meanf, a.y - meanf, a.z - meanf, a.w - meanf,
+                          b.x - meanf, b.y - meanf, b.z - meanf, b.w - meanf};
+      if (f32) {
+        reinterpret_cast<float4*>(f32)[2 * c] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4*>(f32)[2 * c + 1] = make_float4(v[4], v[5], v[6], v[7]);
+      }
+      if (lp16) {
+        __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) h[e] = __float2bfloat16_rn(v[e] * inv);
+        reinterpret_cast<uint4*>(lp16)[c] = *reinterpret_cast<const uint4*>(h);
+      }
     }
+    if (lp16)
+      for (int p = n + tid; p < o.ld_lp; p += blockDim.x) lp16[p] = __float2bfloat16_rn(0.0f);
+    return;
+  }
+  if (f32)
+    for (int p = tid; p < n; p += blockDim.x) f32[p] = row[p] - meanf;
+  if (lp16) {
+    for (int p = tid; p < o.ld_lp; p += blockDim.x) lp16[p] = __float2bfloat16_rn(p < n ? (row[p] - meanf) * inv : 0.0f);
+  } else if (o.lp) {
+    __nv_fp8_e4m3* dst = reinterpret_cast<__nv_fp8_e4m3*>(o.lp) + r * o.ld_lp;
+    const float sc = inv / qscale;
+    for (int p = tid; p < o.ld_lp; p += blockDim.x) dst[p] = __nv_fp8_e4m3(p < n ? (row[p] - meanf) * sc : 0.0f);
   }
 }
 
@@ -134,13 +154,16 @@ __global__ void __launch_bounds__(kRowThreads) k_project(
   const float* rz = rays + 2 * (int64_t)n_pix;
   for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
     const float4 q = quats[r];
+    float part = 0.0f;
     for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
       const float3 v = rotate(q, __ldg(rx + p), __ldg(ry + p), __ldg(rz + p));
       const float2 uv = lambert_side_by_side(v.x, v.y, v.z);
-      row[p] = sample_border(mp, mp_h, mp_w2, uv.x, uv.y);
+      const float val = sample_border(mp, mp_h, mp_w2, uv.x, uv.y);
+      row[p] = val;
+      part += val;
     }
     __syncthreads();
-    finalize_row(row, n_pix, subtract_mean, r, o, fred, dred);
+    finalize_row(row, n_pix, subtract_mean, part, r, o, fred, dred);
     __syncthreads();
   }
 }
@@ -156,6 +179,7 @@ __global__ void __launch_bounds__(kRowThreads) k_prep(const float* __restrict__ 
   const float cnt = (float)(b * b);
   for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
     const float* img = pats + r * stride;
+    float part = 0.0f;
     for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
       const int idx = pix ? __ldg(pix + p) : p;
       float v;
@@ -170,9 +194,10 @@ __global__ void __launch_bounds__(kRowThreads) k_prep(const float* __restrict__ 
         v = s / cnt;
       }
       row[p] = v;
+      part += v;
     }
     __syncthreads();
-    finalize_row(row, n_pix, subtract_mean, r, o, fred, dred);
+    finalize_row(row, n_pix, subtract_mean, part, r, o, fred, dred);
     __syncthreads();
   }
 }

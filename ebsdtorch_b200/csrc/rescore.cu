@@ -86,33 +86,42 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   // 2. exact FP32 scores of the best n_rescore (or approximate * |q|)
   const int nr = n_rescore;
   if (d_f32) {
-    for (int c = wid; c < nr; c += nw) {
-      const int64_t di = (ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
-      float acc = 0.0f;
-      if (di >= 0) {
-        const float* drow = d_f32 + (di - d_base) * ld_d;
-        if ((n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0) {
-          const float4* d4 = reinterpret_cast<const float4*>(drow);
-          const float4* q4 = reinterpret_cast<const float4*>(qrow);
-          for (int p = lane; p < (n_pix >> 2); p += 32) {
-            const float4 a = __ldg(d4 + p), b = q4[p];
-            acc = fmaf(a.x, b.x, acc);
-            acc = fmaf(a.y, b.y, acc);
-            acc = fmaf(a.z, b.z, acc);
-            acc = fmaf(a.w, b.w, acc);
-          }
-        } else {
-          for (int p = lane; p < n_pix; p += 32) acc = fmaf(__ldg(drow + p), qrow[p], acc);
+    // four rows per warp at once (four 16-byte loads in flight per lane)
+    constexpr int R = 4;
+    const bool vec = (n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0;
+    for (int c0 = wid * R; c0 < nr; c0 += nw * R) {
+      int64_t di[R];
+      const float* d[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const int c = c0 + j;
+        di[j] = (c < nr && ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
+        d[j] = d_f32 + (di[j] >= 0 ? di[j] - d_base : 0) * ld_d;  // a missing row re-reads row 0
+      }
+      float acc[R];
+      if (vec) {
+        f32_dot_rows<R>(qrow, d, n_pix >> 2, lane, acc);
+      } else {
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          float a = 0.0f;
+          for (int p = lane; p < n_pix; p += 32) a = fmaf(__ldg(d[j] + p), qrow[p], a);
+          acc[j] = warp_sum(a);
         }
       }
-      acc = warp_sum(acc);
       if (lane == 0) {
-        if (similarity == EBSD_SIM_COSINE && di >= 0) {
-          const float den = q_norm[q] * d_norm[di - d_base];
-          acc = den > 0.0f ? acc / den : 0.0f;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+          const int c = c0 + j;
+          if (c >= nr) break;
+          float v = acc[j];
+          if (similarity == EBSD_SIM_COSINE && di[j] >= 0) {
+            const float den = q_norm[q] * d_norm[di[j] - d_base];
+            v = den > 0.0f ? v / den : 0.0f;
+          }
+          fin_v[c] = di[j] >= 0 ? v : -INFINITY;
+          fin_i[c] = di[j];
         }
-        fin_v[c] = di >= 0 ? acc : -INFINITY;
-        fin_i[c] = di;
       }
     }
   } else {

@@ -101,7 +101,7 @@ class LearnedStats:
 def learned_dictionary_index(master_pattern, geometry, experiment_patterns, model, dictionary_resolution_degrees=0.5,
                              max_angle_deg: float = 16.0, pyramid_resolutions_deg=(3.0, 1.5, 0.75),
                              stage_margin: float = 1.6, fallback_ratio: float = 0.95, n_rescore: int = 8,
-                             batch: int = 4096,
+                             pyramid_precision: str = "bf16", batch: int = 4096,
                              precision: str = "bf16", rescore_k: int = 32, device=None,
                              phase_dictionary: Optional[PhaseDictionary] = None) -> LearnedStats:
     """Top-1 indexing of one phase by learned proposal + coarse-to-fine local
@@ -117,8 +117,10 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     neighbourhood. Patterns whose final cosine falls below fallback_ratio x
     the map's median (or that found no candidate) are re-indexed by full
     plain DI against the resident rows. Every stage ranks its candidates
-    by the dictionaries' low-precision rows; the last re-scores its best
-    n_rescore in FP32. Writes raw_indexing_results /
+    by the dictionaries' low-precision rows (`pyramid_precision` for the
+    intermediate ones, which only place the next stage's centre; `precision`
+    for the full one, which also serves the fallback); the last re-scores its
+    best n_rescore in FP32. Writes raw_indexing_results /
     orientations like dictionary_index_orientations; returns timings and
     counts."""
     from .ebsd.indexing import _device, _master_pattern_tensor, _unit_rays_soa
@@ -132,7 +134,7 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     pd = phase_dictionary or PhaseDictionary(mp_t, rays, laue, dictionary_resolution_degrees, precision)
     levels = sorted({float(r) for r in (pyramid_resolutions_deg or ()) if r > dictionary_resolution_degrees},
                     reverse=True)
-    stages = [PhaseDictionary(mp_t, rays, laue, r, precision, permute=False) for r in levels] + [pd]
+    stages = [PhaseDictionary(mp_t, rays, laue, r, pyramid_precision, permute=False) for r in levels] + [pd]
     radii = [float(max_angle_deg)] + [stage_margin * cell_angle_deg(d.edge) for d in stages[:-1]]
     for d, r in zip(stages, radii):
         need = int(math.ceil(r * (4.0 / 3.0) * d.edge / 199.0)) + 1
