@@ -26,24 +26,29 @@
 namespace ebsd {
 
 constexpr int BM = 128;
-constexpr int BN = 256;
 constexpr int BKB = 128;  // bytes of K per stage and row (one 128-byte swizzle atom)
-constexpr int STAGES = 4;
 constexpr int A_BYTES = BM * BKB;
-constexpr int B_BYTES = BN * BKB;
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
 constexpr int EPI_THREADS = 128;
 constexpr int THREADS = 64 + EPI_THREADS;
 constexpr int SCRATCH_BYTES = 32 * EPI_THREADS * 4;
-constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 1) + 16;
-constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + BAR_BYTES;
-constexpr uint32_t TMEM_COLS = 2 * BN;
 
-static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+// Shape of one CTA tile: 128 query rows x BN dictionary rows (N of the MMA).
+template <int BN_>
+struct Tile {
+  static constexpr int BN = BN_;
+  static constexpr int STAGES = BN_ == 256 ? 4 : 6;
+  static constexpr int B_BYTES = BN_ * BKB;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 1) + 16;
+  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + BAR_BYTES;
+  static constexpr uint32_t TMEM_COLS = 2 * BN_;  // two accumulators
+  static_assert(SMEM_BYTES <= 232448, "shared memory budget");
+};
 
 struct GemmParams {
   int n_tiles;
   int splits;
+  int units;  // m_tiles * splits; a CTA takes units blockIdx.x, + gridDim.x, ...
   int k_iters;
   int64_t n_valid;
   const float* col_scale;
@@ -65,7 +70,7 @@ struct GemmParams {
   int* status;
 };
 
-template <int KIND>
+template <int KIND, int BN>
 __host__ __device__ constexpr uint32_t make_idesc() {
   // c_format F32 (bit 4); a/b format bits 7-9 / 10-12 (kind::f16: 1 = BF16;
   // kind::f8f6f4: 0 = E4M3); K-major A and B; N >> 3 at bit 17; M >> 4 at bit 24.
@@ -97,10 +102,13 @@ __device__ __forceinline__ void report_timeout(const GemmParams& p, volatile int
 // MODE 0: top-k epilogue. MODE 1: store epilogue. MODE 2: convolution
 // epilogue, out[col, row] = act(acc[row, col] + bias[row]) stored transposed
 // in bf16 (and FP32 when asked).
-template <int KIND, int MODE, int KC>
+template <int KIND, int MODE, int KC, int BN>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const GemmParams p) {
+  using T = Tile<BN>;
+  constexpr int STAGES = T::STAGES;
+  constexpr int STAGE_BYTES = T::STAGE_BYTES;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_s = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
@@ -117,10 +125,13 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m_tile = blockIdx.x / p.splits;
-  const int split = blockIdx.x - m_tile * p.splits;
-  const int n_begin = (int)((int64_t)split * p.n_tiles / p.splits);
-  const int n_end = (int)((int64_t)(split + 1) * p.n_tiles / p.splits);
+  // work unit -> (query tile, dictionary tile range)
+  auto unit_tile = [&](int u) { return u / p.splits; };
+  auto unit_range = [&](int u, int& n_begin, int& n_end) {
+    const int split = u - (u / p.splits) * p.splits;
+    n_begin = (int)((int64_t)split * p.n_tiles / p.splits);
+    n_end = (int)((int64_t)(split + 1) * p.n_tiles / p.splits);
+  };
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -139,7 +150,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     prefetch_tmap(&tmA);
     prefetch_tmap(&tmB);
   }
-  if (warp == 1) tmem_alloc(smem_u32(tmem_slot), TMEM_COLS);
+  if (warp == 1) tmem_alloc(smem_u32(tmem_slot), T::TMEM_COLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -151,22 +162,26 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t stage = 0, phase = 0;
       int64_t issued = 0;
       bool ok = true;
-      const int a_row = m_tile * BM;
-      for (int n = n_begin; n < n_end && ok; ++n) {
-        for (int k = 0; k < p.k_iters; ++k) {
-          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
-            ok = false;
-            break;
-          }
-          const uint32_t a_dst = sbase + stage * STAGE_BYTES;
-          mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
-          const int kx = k * (KIND == 0 ? BKB / 2 : BKB);  // element coordinate
-          tma_load_2d(a_dst, &tmA, kx, a_row, full_bar(stage));
-          tma_load_2d(a_dst + A_BYTES, &tmB, kx, n * BN, full_bar(stage));
-          ++issued;
-          if (++stage == STAGES) {
-            stage = 0;
-            phase ^= 1u;
+      for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+        const int a_row = unit_tile(u) * BM;
+        int n_begin, n_end;
+        unit_range(u, n_begin, n_end);
+        for (int n = n_begin; n < n_end && ok; ++n) {
+          for (int k = 0; k < p.k_iters; ++k) {
+            if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+              ok = false;
+              break;
+            }
+            const uint32_t a_dst = sbase + stage * STAGE_BYTES;
+            mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
+            const int kx = k * (KIND == 0 ? BKB / 2 : BKB);  // element coordinate
+            tma_load_2d(a_dst, &tmA, kx, a_row, full_bar(stage));
+            tma_load_2d(a_dst + A_BYTES, &tmB, kx, n * BN, full_bar(stage));
+            ++issued;
+            if (++stage == STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
           }
         }
       }
@@ -195,39 +210,43 @@ __global__ void __launch_bounds__(THREADS, 1)
       int acc = 0;
       uint32_t acc_phase = 0;
       bool ok = true, any = false;
-      constexpr uint32_t idesc = make_idesc<KIND>();
-      for (int n = n_begin; n < n_end && ok; ++n) {
-        if (!mbar_wait(acce_bar(acc), acc_phase ^ 1u, abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-        for (int k = 0; k < p.k_iters; ++k) {
-          if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+      constexpr uint32_t idesc = make_idesc<KIND, BN>();
+      for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+        int n_begin, n_end;
+        unit_range(u, n_begin, n_end);
+        for (int n = n_begin; n < n_end && ok; ++n) {
+          if (!mbar_wait(acce_bar(acc), acc_phase ^ 1u, abort_flag)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a_addr = sbase + stage * STAGE_BYTES;
-          const uint32_t b_addr = a_addr + A_BYTES;
-#pragma unroll
-          for (int kk = 0; kk < BKB / 32; ++kk) {
-            tc_mma<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32),
-                         idesc, (k | kk) != 0 ? 1u : 0u);
+          const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
+          for (int k = 0; k < p.k_iters; ++k) {
+            if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_addr = sbase + stage * STAGE_BYTES;
+            const uint32_t b_addr = a_addr + A_BYTES;
+  #pragma unroll
+            for (int kk = 0; kk < BKB / 32; ++kk) {
+              tc_mma<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32),
+                           idesc, (k | kk) != 0 ? 1u : 0u);
+            }
+            any = true;
+            tc_commit(empty_bar(stage));
+            if (++stage == STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
           }
-          any = true;
-          tc_commit(empty_bar(stage));
-          if (++stage == STAGES) {
-            stage = 0;
-            phase ^= 1u;
+          if (!ok) break;
+          tc_commit(accf_bar(acc));
+          if (++acc == 2) {
+            acc = 0;
+            acc_phase ^= 1u;
           }
-        }
-        if (!ok) break;
-        tc_commit(accf_bar(acc));
-        if (++acc == 2) {
-          acc = 0;
-          acc_phase ^= 1u;
         }
       }
       if (!ok) {
@@ -249,121 +268,128 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t lane_addr = (uint32_t)(wq * 32) << 16;
     float bv[KC];
     int bi[KC];
-#pragma unroll
-    for (int j = 0; j < KC; ++j) {
-      bv[j] = -INFINITY;
-      bi[j] = -1;
-    }
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
-    for (int n = n_begin; n < n_end; ++n) {
-      bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag);
-      got = __all_sync(0xffffffffu, got);
-      if (!got) {
-        ok = false;
-        break;
+    for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+      const int m_tile = unit_tile(u);
+      const int split = u - m_tile * p.splits;
+      int n_begin, n_end;
+      unit_range(u, n_begin, n_end);
+  #pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        bv[j] = -INFINITY;
+        bi[j] = -1;
       }
-      tc_fence_after();
-      const int64_t tile_col = (int64_t)n * BN;
-#pragma unroll 1
-      for (int c = 0; c < BN / 32; ++c) {
-        __syncwarp();
-        float v[32];
-        tmem_ld32(tmem_base + lane_addr + (uint32_t)(acc * BN + c * 32), v);
-        const int64_t col0 = tile_col + c * 32;
-        if constexpr (MODE == 0) {
-          uint32_t mask = 0;
-          const float thr = bv[KC - 1];
-          if (col0 + 32 <= p.n_valid) {
-            if (p.col_scale) {
-              const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
-#pragma unroll
-              for (int j4 = 0; j4 < 8; ++j4) {
-                const float4 s4 = __ldg(cs + j4);
-                v[4 * j4 + 0] *= s4.x;
-                v[4 * j4 + 1] *= s4.y;
-                v[4 * j4 + 2] *= s4.z;
-                v[4 * j4 + 3] *= s4.w;
+      for (int n = n_begin; n < n_end; ++n) {
+        bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag);
+        got = __all_sync(0xffffffffu, got);
+        if (!got) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const int64_t tile_col = (int64_t)n * BN;
+  #pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+          __syncwarp();
+          float v[32];
+          tmem_ld32(tmem_base + lane_addr + (uint32_t)(acc * BN + c * 32), v);
+          const int64_t col0 = tile_col + c * 32;
+          if constexpr (MODE == 0) {
+            uint32_t mask = 0;
+            const float thr = bv[KC - 1];
+            if (col0 + 32 <= p.n_valid) {
+              if (p.col_scale) {
+                const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
+  #pragma unroll
+                for (int j4 = 0; j4 < 8; ++j4) {
+                  const float4 s4 = __ldg(cs + j4);
+                  v[4 * j4 + 0] *= s4.x;
+                  v[4 * j4 + 1] *= s4.y;
+                  v[4 * j4 + 2] *= s4.z;
+                  v[4 * j4 + 3] *= s4.w;
+                }
+              }
+            } else {
+  #pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const bool valid = col0 + j < p.n_valid;
+                const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
+                v[j] = valid ? v[j] * sc : -INFINITY;
+              }
+            }
+  #pragma unroll
+            for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
+            if (mask) {
+  #pragma unroll
+              for (int j = 0; j < 32; ++j) scratch[j * EPI_THREADS + etid] = v[j];
+              while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const float sc = scratch[j * EPI_THREADS + etid];
+                if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
+              }
+            }
+          } else if constexpr (MODE == 2) {
+            const int64_t grow = (int64_t)m_tile * BM + row;
+            if (grow < p.m_valid) {
+              const float b = p.bias ? __ldg(p.bias + grow) : 0.f;
+              // the warp's 32 threads own 32 consecutive channels: each store
+              // instruction writes 32 consecutive values of one pixel
+  #pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const int64_t col = col0 + j;
+                if (col < p.n_valid) {
+                  float r = v[j] + b;
+                  if (p.relu) r = fmaxf(r, 0.f);
+                  p.out16[col * p.ld_out + grow] = __float2bfloat16_rn(r);
+                  if (p.out32) p.out32[col * p.ld_out + grow] = r;
+                }
               }
             }
           } else {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const bool valid = col0 + j < p.n_valid;
-              const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
-              v[j] = valid ? v[j] * sc : -INFINITY;
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
-          if (mask) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) scratch[j * EPI_THREADS + etid] = v[j];
-            while (mask) {
-              const int j = __ffs(mask) - 1;
-              mask &= mask - 1u;
-              const float sc = scratch[j * EPI_THREADS + etid];
-              if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
-            }
-          }
-        } else if constexpr (MODE == 2) {
-          const int64_t grow = (int64_t)m_tile * BM + row;
-          if (grow < p.m_valid) {
-            const float b = p.bias ? __ldg(p.bias + grow) : 0.f;
-            // the warp's 32 threads own 32 consecutive channels: each store
-            // instruction writes 32 consecutive values of one pixel
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int64_t col = col0 + j;
-              if (col < p.n_valid) {
-                float r = v[j] + b;
-                if (p.relu) r = fmaxf(r, 0.f);
-                p.out16[col * p.ld_out + grow] = __float2bfloat16_rn(r);
-                if (p.out32) p.out32[col * p.ld_out + grow] = r;
-              }
-            }
-          }
-        } else {
-          const int64_t grow = (int64_t)m_tile * BM + row;
-          if (grow < p.m_valid) {
-            float* dst = p.C + grow * p.ldc;
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int64_t col = col0 + j;
-              if (col < p.n_valid) {
-                const float r = p.alpha * v[j];
-                dst[col] = p.accumulate ? dst[col] + r : r;
+            const int64_t grow = (int64_t)m_tile * BM + row;
+            if (grow < p.m_valid) {
+              float* dst = p.C + grow * p.ldc;
+  #pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const int64_t col = col0 + j;
+                if (col < p.n_valid) {
+                  const float r = p.alpha * v[j];
+                  dst[col] = p.accumulate ? dst[col] + r : r;
+                }
               }
             }
           }
         }
+        tc_fence_before();
+        mbar_arrive(acce_bar(acc));
+        if (++acc == 2) {
+          acc = 0;
+          acc_phase ^= 1u;
+        }
       }
-      tc_fence_before();
-      mbar_arrive(acce_bar(acc));
-      if (++acc == 2) {
-        acc = 0;
-        acc_phase ^= 1u;
+      if constexpr (MODE == 0) {
+        if (ok) {
+          const int64_t q = (int64_t)m_tile * BM + row;
+          const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
+  #pragma unroll
+          for (int j = 0; j < KC; ++j) {
+            p.part_val[base + j] = bv[j];
+            p.part_idx[base + j] = bi[j];
+          }
+        }
       }
     }
-    if (!ok) {
-      if (lane == 0) report_timeout(p, abort_flag);
-    } else if constexpr (MODE == 0) {
-      const int64_t q = (int64_t)m_tile * BM + row;
-      const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
-#pragma unroll
-      for (int j = 0; j < KC; ++j) {
-        p.part_val[base + j] = bv[j];
-        p.part_idx[base + j] = bi[j];
-      }
-    }
+    if (!ok && lane == 0) report_timeout(p, abort_flag);
   }
 
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, TMEM_COLS);
+    tmem_dealloc(tmem_base, T::TMEM_COLS);
   }
 }
 
@@ -416,34 +442,35 @@ static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t ro
   return 0;
 }
 
-template <int KIND, int MODE, int KC>
+template <int KIND, int MODE, int KC, int BN>
 static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
                   cudaStream_t s) {
-  auto kern = k_tc_gemm<KIND, MODE, KC>;
-  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-  kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, b, p);
+  auto kern = k_tc_gemm<KIND, MODE, KC, BN>;
+  constexpr int smem = Tile<BN>::SMEM_BYTES;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  kern<<<grid, THREADS, smem, s>>>(a, b, p);
   EBSD_LAUNCH_CHECK();
   return 0;
 }
 
-template <int KIND>
+template <int KIND, int BN>
 static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
                        int grid, cudaStream_t s) {
   switch (kc) {
-    case 1: return launch<KIND, 0, 1>(a, b, p, grid, s);
-    case 2: return launch<KIND, 0, 2>(a, b, p, grid, s);
-    case 4: return launch<KIND, 0, 4>(a, b, p, grid, s);
-    case 8: return launch<KIND, 0, 8>(a, b, p, grid, s);
-    case 16: return launch<KIND, 0, 16>(a, b, p, grid, s);
-    case 32: return launch<KIND, 0, 32>(a, b, p, grid, s);
-    case 64: return launch<KIND, 0, 64>(a, b, p, grid, s);
+    case 1: return launch<KIND, 0, 1, BN>(a, b, p, grid, s);
+    case 2: return launch<KIND, 0, 2, BN>(a, b, p, grid, s);
+    case 4: return launch<KIND, 0, 4, BN>(a, b, p, grid, s);
+    case 8: return launch<KIND, 0, 8, BN>(a, b, p, grid, s);
+    case 16: return launch<KIND, 0, 16, BN>(a, b, p, grid, s);
+    case 32: return launch<KIND, 0, 32, BN>(a, b, p, grid, s);
+    case 64: return launch<KIND, 0, 64, BN>(a, b, p, grid, s);
   }
   set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
   return EBSD_ERR_ARG;
 }
 
 static int check_operands(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
-                          int lp_dtype, int* status) {
+                          int lp_dtype, int* status, int BN = 256) {
   EBSD_ARG_CHECK(A && B && status, "null operand or status pointer");
   EBSD_ARG_CHECK(lp_dtype == EBSD_DT_BF16 || lp_dtype == EBSD_DT_E4M3,
                  "lp_dtype must be EBSD_DT_BF16 or EBSD_DT_E4M3");
@@ -471,38 +498,40 @@ extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad)
   // and ~1.3 GHz under the power cap; multi-wave or 1-range shapes that keep
   // many more operand tiles in flight settle at 0.68-1.1 PFLOP/s.
   const int64_t m_tiles = std::max<int64_t>(1, n_queries_pad / BM);
-  const int64_t n_tiles = std::max<int64_t>(1, n_dict_pad / BN);
+  const int64_t n_tiles = std::max<int64_t>(1, n_dict_pad / 256);
   const int64_t sms = device_sm_count();
   int64_t splits = std::max<int64_t>(1, sms / m_tiles);
   splits = std::min(splits, n_tiles);
   return (int)splits;
 }
 
-extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
-                               int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad,
-                               int lp_dtype, const float* col_scale, int n_cand, int splits,
-                               float* part_val, int32_t* part_idx, int part_slots, int slot_base,
-                               int32_t index_base, int* d_status, void* stream) {
-  if (int rc = check_operands(queries_lp, n_queries_pad, dict_lp, n_dict_pad, k_pad, lp_dtype,
-                              d_status))
+extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
+                                     int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
+                                     const float* col_scale, int n_cand, int splits, float* part_val,
+                                     int32_t* part_idx, int part_slots, int slot_base, int32_t index_base,
+                                     int tile_n, int max_ctas, int* d_status, void* stream) {
+  if (tile_n == 0) tile_n = 256;
+  EBSD_ARG_CHECK(tile_n == 128 || tile_n == 256, "tile_n must be 128 or 256");
+  if (int rc = check_operands(queries_lp, n_queries_pad, dict_lp, n_dict_pad, k_pad, lp_dtype, d_status, tile_n))
     return rc;
   EBSD_ARG_CHECK(part_val && part_idx, "null partial-result buffers");
   EBSD_ARG_CHECK(n_dict_valid > 0 && n_dict_valid <= n_dict_pad, "n_dict_valid out of range");
   EBSD_ARG_CHECK((int64_t)index_base + n_dict_valid <= INT32_MAX, "dictionary index overflow");
   EBSD_ARG_CHECK(!col_scale || ((uintptr_t)col_scale & 15) == 0, "col_scale must be 16-byte aligned");
-  const int n_tiles = (int)(n_dict_pad / BN);
+  const int n_tiles = (int)(n_dict_pad / tile_n);
   if (splits <= 0) splits = ebsd_match_auto_splits(n_queries_pad, n_dict_pad);
-  EBSD_ARG_CHECK(splits <= n_tiles, "splits (%d) > dictionary tiles (%d)", splits, n_tiles);
+  splits = std::min(splits, n_tiles);
   EBSD_ARG_CHECK(slot_base >= 0 && slot_base + splits <= part_slots,
                  "part_slots (%d) < slot_base (%d) + splits (%d)", part_slots, slot_base, splits);
   const int64_t m_tiles = n_queries_pad / BM;
   EBSD_ARG_CHECK(m_tiles * splits < INT32_MAX, "too many work units");
   CUtensorMap ta, tb;
   if (int rc = make_tmap(&ta, queries_lp, lp_dtype, n_queries_pad, k_pad, BM)) return rc;
-  if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, BN)) return rc;
+  if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, tile_n)) return rc;
   GemmParams p{};
   p.n_tiles = n_tiles;
   p.splits = splits;
+  p.units = (int)(m_tiles * splits);
   p.k_iters = (int)(k_pad * (lp_dtype == EBSD_DT_BF16 ? 2 : 1) / BKB);
   p.n_valid = n_dict_valid;
   p.col_scale = col_scale;
@@ -512,10 +541,27 @@ extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, co
   p.slot_base = slot_base;
   p.index_base = index_base;
   p.status = d_status;
-  const int grid = (int)(m_tiles * splits);
+  // max_ctas > 0: persistent launch, each CTA loops over units
+  const int grid = max_ctas > 0 ? std::min(p.units, max_ctas) : p.units;
   cudaStream_t s = as_stream(stream);
-  return lp_dtype == EBSD_DT_BF16 ? launch_topk<0>(n_cand, ta, tb, p, grid, s)
-                                  : launch_topk<1>(n_cand, ta, tb, p, grid, s);
+  if (tile_n == 128)
+    return lp_dtype == EBSD_DT_BF16 ? launch_topk<0, 128>(n_cand, ta, tb, p, grid, s)
+                                    : launch_topk<1, 128>(n_cand, ta, tb, p, grid, s);
+  return lp_dtype == EBSD_DT_BF16 ? launch_topk<0, 256>(n_cand, ta, tb, p, grid, s)
+                                  : launch_topk<1, 256>(n_cand, ta, tb, p, grid, s);
+}
+
+extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
+                               int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad,
+                               int lp_dtype, const float* col_scale, int n_cand, int splits,
+                               float* part_val, int32_t* part_idx, int part_slots, int slot_base,
+                               int32_t index_base, int* d_status, void* stream) {
+  if (splits > 0 && n_dict_pad >= 256)
+    EBSD_ARG_CHECK(splits <= n_dict_pad / 256, "splits (%d) > dictionary tiles (%lld)", splits,
+                   (long long)(n_dict_pad / 256));
+  return ebsd_match_topk_tiled(queries_lp, n_queries_pad, dict_lp, n_dict_pad, n_dict_valid, k_pad, lp_dtype,
+                               col_scale, n_cand, splits, part_val, part_idx, part_slots, slot_base, index_base,
+                               256, 0, d_status, stream);
 }
 
 extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
@@ -528,9 +574,9 @@ extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t
   EBSD_ARG_CHECK(ldc >= n_valid, "ldc < n_valid");
   CUtensorMap ta, tb;
   if (int rc = make_tmap(&ta, A, lp_dtype, m_pad, k_pad, BM)) return rc;
-  if (int rc = make_tmap(&tb, B, lp_dtype, n_pad, k_pad, BN)) return rc;
+  if (int rc = make_tmap(&tb, B, lp_dtype, n_pad, k_pad, 256)) return rc;
   GemmParams p{};
-  p.n_tiles = (int)(n_pad / BN);
+  p.n_tiles = (int)(n_pad / 256);
   // splits <= 0: one B tile per unit; otherwise each unit streams a range of
   // n_tiles / splits B tiles (amortises CTA set-up when K is short)
   p.splits = splits <= 0 ? p.n_tiles : std::min(splits, p.n_tiles);
@@ -544,10 +590,10 @@ extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t
   p.status = d_status;
   const int64_t m_tiles = m_pad / BM;
   EBSD_ARG_CHECK(m_tiles * p.splits < INT32_MAX, "too many work units");
-  const int grid = (int)(m_tiles * p.splits);
+  p.units = (int)(m_tiles * p.splits);
   cudaStream_t s = as_stream(stream);
-  return lp_dtype == EBSD_DT_BF16 ? launch<0, 1, 1>(ta, tb, p, grid, s)
-                                  : launch<1, 1, 1>(ta, tb, p, grid, s);
+  return lp_dtype == EBSD_DT_BF16 ? launch<0, 1, 1, 256>(ta, tb, p, p.units, s)
+                                  : launch<1, 1, 1, 256>(ta, tb, p, p.units, s);
 }
 
 extern "C" int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* cols, int64_t rows_pad,
@@ -559,9 +605,9 @@ extern "C" int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* 
   EBSD_ARG_CHECK(ld_out >= cout, "ld_out < cout");
   CUtensorMap ta, tb;
   if (int rc = make_tmap(&ta, w16, EBSD_DT_BF16, cout_pad, k_pad, BM)) return rc;
-  if (int rc = make_tmap(&tb, cols, EBSD_DT_BF16, rows_pad, k_pad, BN)) return rc;
+  if (int rc = make_tmap(&tb, cols, EBSD_DT_BF16, rows_pad, k_pad, 256)) return rc;
   GemmParams p{};
-  p.n_tiles = (int)(rows_pad / BN);
+  p.n_tiles = (int)(rows_pad / 256);
   p.splits = splits <= 0 ? p.n_tiles : std::min(splits, p.n_tiles);
   p.k_iters = (int)(k_pad * 2 / BKB);
   p.n_valid = n_rows;
@@ -574,5 +620,6 @@ extern "C" int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* 
   p.status = d_status;
   const int64_t m_tiles = cout_pad / BM;
   EBSD_ARG_CHECK(m_tiles * p.splits < INT32_MAX, "too many work units");
-  return launch<0, 2, 1>(ta, tb, p, (int)(m_tiles * p.splits), as_stream(stream));
+  p.units = (int)(m_tiles * p.splits);
+  return launch<0, 2, 1, 256>(ta, tb, p, p.units, as_stream(stream));
 }

@@ -46,6 +46,14 @@ class SearchConfig:
     workspace_bytes: Optional[int] = None
     query_chunk: Optional[int] = None
     dict_chunk: Optional[int] = None
+    # match launch shape (the batch autotuner sets these): dictionary rows per
+    # CTA tile (0 = 256), dictionary ranges per query tile (0 = automatic),
+    # query tiles per launch (0 = one wave), or one persistent launch per
+    # query chunk with one CTA per SM
+    tile_n: int = 0
+    splits: int = 0
+    wave_tiles: int = 0
+    persistent: bool = False
 
     def validate(self):
         if self.precision not in LP_DTYPES:
@@ -54,6 +62,10 @@ class SearchConfig:
             raise ValueError(f"similarity must be 'dot' or 'cosine', got {self.similarity!r}")
         if not 0 <= self.rescore_k <= 128:
             raise ValueError("rescore_k must be in [0, 128]")
+        if self.tile_n not in (0, 128, 256):
+            raise ValueError("tile_n must be 0, 128 or 256")
+        if self.splits < 0 or self.wave_tiles < 0:
+            raise ValueError("splits and wave_tiles must be >= 0")
 
 
 def _pow2_at_least(n: int) -> int:
@@ -157,15 +169,20 @@ class Searcher:
             raise MemoryError(
                 f"dictionary indexing needs more device memory than the budget of {budget / 2**30:.1f} GiB")
 
-    def run(self, fill_dict: Optional[DictFill], fill_queries: QueryFill, resident: Optional[RowSet] = None):
+    def run(self, fill_dict: Optional[DictFill], fill_queries: QueryFill, resident: Optional[RowSet] = None,
+            check: bool = True, status: Optional[torch.Tensor] = None):
         """Search all queries against all dictionary rows.
         `resident`: an already filled RowSet holding the whole dictionary (then
         fill_dict is not called). Returns (indices (Q, k) int64, scores (Q, k)
-        float32) on the device."""
+        float32) on the device. With check=False nothing synchronises (for
+        CUDA-graph capture): the caller reads `status` (a device int32 word,
+        non-zero after a kernel timeout) later with check_status()."""
         dev, Q, D, k = self.device, self.n_queries, self.n_dict, self.k
         out_val = torch.empty((Q, k), dtype=torch.float32, device=dev)
         out_idx = torch.empty((Q, k), dtype=torch.int64, device=dev)
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        if status is None:
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.status = status
         if resident is not None:
             if resident.n_rows != D or resident.lp_dtype != self.lp_dtype or (self.rescore and resident.f32 is None):
                 raise ValueError("resident dictionary rows do not match the search")
@@ -175,9 +192,17 @@ class Searcher:
             dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
         qc = self.query_chunk
         q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.rescore, dev)
-        # match launches cover one wave of (query tile, dictionary range) units
-        qm = wave_query_tiles(dev) * TILE_Q
-        max_splits = max(1, torch.cuda.get_device_properties(dev).multi_processor_count)
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        cfg = self.cfg
+        split_cap = MAX_MERGE_CANDIDATES // self.n_cand
+        if cfg.persistent:
+            # one launch per query chunk; each of the SMs' CTAs loops over units
+            qm, max_ctas = round_up(qc, TILE_Q), sms
+            max_splits = min(cfg.splits or 4, split_cap)
+        else:
+            # launches of one wave of (query tile, dictionary range) units
+            qm, max_ctas = (cfg.wave_tiles or wave_query_tiles(dev)) * TILE_Q, 0
+            max_splits = min(cfg.splits or max(1, sms), split_cap)
         part_val = torch.empty((min(qm, round_up(qc, TILE_Q)) * max_splits * self.n_cand,), dtype=torch.float32,
                                device=dev)
         part_idx = torch.empty(part_val.shape, dtype=torch.int32, device=dev)
@@ -201,14 +226,17 @@ class Searcher:
                     s1 = min(nq, s0 + qm)
                     ns = s1 - s0
                     ns_pad = round_up(ns, TILE_Q)
-                    splits = min(kernels.auto_splits(ns_pad, nd_pad), MAX_MERGE_CANDIDATES // self.n_cand)
+                    tile = cfg.tile_n or 256
+                    auto = max_splits if cfg.persistent else kernels.auto_splits(ns_pad, nd_pad)
+                    splits = max(1, min(cfg.splits or auto, max_splits, split_cap, nd_pad // tile))
                     timers = MATCH_TIMERS
                     if timers is not None:
                         ev0 = torch.cuda.Event(enable_timing=True)
                         ev1 = torch.cuda.Event(enable_timing=True)
                         ev0.record()
                     kernels.match_topk(q_rows.lp[s0:s0 + ns_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand,
-                                       splits, part_val, part_idx, splits, 0, d0, status)
+                                       splits, part_val, part_idx, splits, 0, d0, status, tile_n=cfg.tile_n,
+                                       max_ctas=max_ctas)
                     if timers is not None:
                         ev1.record()
                         timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))
@@ -223,8 +251,14 @@ class Searcher:
                         min(self.n_rescore, splits * self.n_cand), k,
                         out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
                         out_val[g0:g1], out_idx[g0:g1])
-        st = int(status.item())
-        if st != 0:
-            code = "device wait timed out" if st == DEVICE_TIMEOUT else f"status {st:#x}"
-            raise RuntimeError(f"dictionary match kernel reported an error: {code}")
+        if check:
+            check_status(status)
         return out_idx, out_val
+
+
+def check_status(status: torch.Tensor) -> None:
+    """Raise if a match kernel reported an error in its device status word."""
+    st = int(status.item())
+    if st != 0:
+        code = "device wait timed out" if st == DEVICE_TIMEOUT else f"status {st:#x}"
+        raise RuntimeError(f"dictionary match kernel reported an error: {code}")

@@ -152,6 +152,17 @@ int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* d
                     const float* col_scale, int n_cand, int splits, float* part_val,
                     int32_t* part_idx, int part_slots, int slot_base, int32_t index_base,
                     int* d_status, void* stream);
+/* The same match with the launch shape chosen by the caller (the batch
+ * planner's autotuner): tile_n 128 or 256 dictionary rows per CTA tile (0 =
+ * 256; n_dict_pad must be a multiple of it), and max_ctas > 0 for a
+ * persistent launch of min(units, max_ctas) CTAs that each loop over work
+ * units u, u + grid, ... (0 = one CTA per unit). Splits larger than the
+ * number of dictionary tiles are reduced to it. */
+int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
+                          int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
+                          const float* col_scale, int n_cand, int splits, float* part_val, int32_t* part_idx,
+                          int part_slots, int slot_base, int32_t index_base, int tile_n, int max_ctas,
+                          int* d_status, void* stream);
 
 /* ---- A10 (final) + FP32 re-score ------------------------------------------
  * Replaces ChunkedKNN.retrieve_topk (knn.py:268-287). Per query: merge the
