@@ -29,6 +29,8 @@ SIGNATURES = {
     "ebsd_gather_rows": (i32, [vp, i64, i32, vp, i64, vp, vp]),
     "ebsd_project_dictionary": (i32, [vp, i32, i32, vp, i32, vp, i64, i32, vp, i64, vp, i32, i64, vp, vp, vp]),
     "ebsd_prep_patterns": (i32, [vp, i64, i32, i32, i64, i32, vp, i32, i32, vp, i64, vp, i32, i64, vp, vp, vp]),
+    "ebsd_prep_patterns_typed": (i32, [vp, i32, i64, i32, i32, i64, i32, vp, i32, i32, vp, i64, vp, i32, i64, vp,
+                                       vp, vp]),
     "ebsd_sample_master_pattern": (i32, [vp, i32, i32, vp, i64, i32, vp, vp]),
     "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
     "ebsd_match_auto_splits": (i32, [i64, i64]),
@@ -69,12 +71,14 @@ DEVICE_TIMEOUT = 0x7001
 # kernels launched by one successful call of each entry point
 LAUNCHES_PER_CALL = {
     "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
-    "ebsd_prep_patterns": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1, "ebsd_match_topk": 1, "ebsd_match_topk_tiled": 1,
+    "ebsd_prep_patterns": 1, "ebsd_prep_patterns_typed": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1,
+    "ebsd_match_topk": 1, "ebsd_match_topk_tiled": 1,
     "ebsd_merge_rescore": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
     "ebsd_disori_angle": 1, "ebsd_match_topk_noalloc": 2, "ebsd_zh_to_qu": 1, "ebsd_qu_to_zh": 1,
     "ebsd_cell_to_row": 2, "ebsd_local_search": 1,
     "ebsd_rot6d_sym_loss": 1, "ebsd_cnn_im2col": 1, "ebsd_cnn_col2im": 1, "ebsd_cnn_bias_act": 1,
-    "ebsd_cnn_conv_fwd": 1, "ebsd_cnn_conv_c1": 1,    "ebsd_cnn_relu_grad": 1, "ebsd_cnn_col_sum": 1, "ebsd_cnn_transpose": 1, "ebsd_cnn_scale_cast": 1,
+    "ebsd_cnn_conv_fwd": 1, "ebsd_cnn_conv_c1": 1, "ebsd_cnn_relu_grad": 1, "ebsd_cnn_col_sum": 1,
+    "ebsd_cnn_transpose": 1, "ebsd_cnn_scale_cast": 1,
     "ebsd_cnn_dense_fwd": 1, "ebsd_cnn_dense_bwd": 2, "ebsd_cnn_adam": 1,
 }
 launch_count = 0  # running total of kernels launched through call()

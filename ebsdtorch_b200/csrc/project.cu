@@ -168,7 +168,14 @@ __global__ void __launch_bounds__(kRowThreads) k_project(
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads) k_prep(const float* __restrict__ pats, int64_t n_rows,
+__device__ __forceinline__ float load_pixel(const float* p, int64_t i) { return __ldg(p + i); }
+__device__ __forceinline__ float load_pixel(const uint16_t* p, int64_t i) { return (float)__ldg(p + i); }
+__device__ __forceinline__ float load_pixel(const uint8_t* p, int64_t i) { return (float)__ldg(p + i); }
+__device__ __forceinline__ float load_pixel(const __half* p, int64_t i) { return __half2float(__ldg(p + i)); }
+
+// Patterns of type T (fp32, uint16 or uint8 detector counts, fp16) -> rows.
+template <typename T>
+__global__ void __launch_bounds__(kRowThreads) k_prep(const T* __restrict__ pats, int64_t n_rows,
                                                       int h, int w, int64_t stride, int b,
                                                       const int32_t* __restrict__ pix, int n_pix,
                                                       int subtract_mean, RowOut o) {
@@ -178,19 +185,19 @@ __global__ void __launch_bounds__(kRowThreads) k_prep(const float* __restrict__ 
   const int wb = w / b;
   const float cnt = (float)(b * b);
   for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
-    const float* img = pats + r * stride;
+    const T* img = pats + r * stride;
     float part = 0.0f;
     for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
       const int idx = pix ? __ldg(pix + p) : p;
       float v;
       if (b == 1) {
-        v = __ldg(img + idx);
+        v = load_pixel(img, idx);
       } else {
         const int i = idx / wb, j = idx - i * wb;
-        const float* src = img + (int64_t)(i * b) * w + j * b;
+        const int64_t src = (int64_t)(i * b) * w + j * b;
         float s = 0.0f;
         for (int a = 0; a < b; ++a)
-          for (int c = 0; c < b; ++c) s += __ldg(src + (int64_t)a * w + c);
+          for (int c = 0; c < b; ++c) s += load_pixel(img, src + (int64_t)a * w + c);
         v = s / cnt;
       }
       row[p] = v;
@@ -268,12 +275,27 @@ extern "C" int ebsd_project_dictionary(const float* master_pattern, int mp_h, in
   return 0;
 }
 
-extern "C" int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int height, int width,
-                                  int64_t pattern_stride, int binning, const int32_t* pix_index,
-                                  int n_pix, int subtract_mean, float* out_f32, int64_t ld_f32,
-                                  void* out_lp, int lp_dtype, int64_t ld_lp, float* out_norm,
-                                  float* out_lp_scale, void* stream) {
+template <typename T>
+static int launch_prep(const T* patterns, int64_t n_rows, int height, int width, int64_t pattern_stride,
+                       int binning, const int32_t* pix_index, int n_pix, int subtract_mean, const RowOut& o,
+                       void* stream) {
+  const size_t smem = (size_t)n_pix * sizeof(float);
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_prep<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const int grid = row_grid(n_rows, smem, (const void*)k_prep<T>);
+  k_prep<T><<<grid, kRowThreads, smem, as_stream(stream)>>>(patterns, n_rows, height, width, pattern_stride,
+                                                           binning, pix_index, n_pix, subtract_mean, o);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+extern "C" int ebsd_prep_patterns_typed(const void* patterns, int pattern_dtype, int64_t n_rows, int height,
+                                        int width, int64_t pattern_stride, int binning, const int32_t* pix_index,
+                                        int n_pix, int subtract_mean, float* out_f32, int64_t ld_f32, void* out_lp,
+                                        int lp_dtype, int64_t ld_lp, float* out_norm, float* out_lp_scale,
+                                        void* stream) {
   EBSD_ARG_CHECK(patterns != nullptr, "ebsd_prep_patterns: null patterns");
+  EBSD_ARG_CHECK(pattern_dtype >= EBSD_PAT_F32 && pattern_dtype <= EBSD_PAT_F16, "unknown pattern_dtype %d",
+                 pattern_dtype);
   EBSD_ARG_CHECK(binning >= 1 && height % binning == 0 && width % binning == 0,
                  "binning %d must divide the pattern shape (%d, %d)", binning, height, width);
   const int n_binned = (height / binning) * (width / binning);
@@ -285,15 +307,30 @@ extern "C" int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int hei
   RowOut o{out_f32, ld_f32, out_lp, lp_dtype, ld_lp, out_norm, out_lp_scale};
   if (int rc = check_row_out(o, n_pix)) return rc;
   if (n_rows == 0) return 0;
-  const size_t smem = (size_t)n_pix * sizeof(float);
-  EBSD_CUDA_CHECK(
-      cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int grid = row_grid(n_rows, smem, (const void*)k_prep);
-  k_prep<<<grid, kRowThreads, smem, as_stream(stream)>>>(patterns, n_rows, height, width,
-                                                        pattern_stride, binning, pix_index, n_pix,
-                                                        subtract_mean, o);
-  EBSD_LAUNCH_CHECK();
-  return 0;
+  switch (pattern_dtype) {
+    case EBSD_PAT_U16:
+      return launch_prep(static_cast<const uint16_t*>(patterns), n_rows, height, width, pattern_stride, binning,
+                         pix_index, n_pix, subtract_mean, o, stream);
+    case EBSD_PAT_U8:
+      return launch_prep(static_cast<const uint8_t*>(patterns), n_rows, height, width, pattern_stride, binning,
+                         pix_index, n_pix, subtract_mean, o, stream);
+    case EBSD_PAT_F16:
+      return launch_prep(static_cast<const __half*>(patterns), n_rows, height, width, pattern_stride, binning,
+                         pix_index, n_pix, subtract_mean, o, stream);
+    default:
+      return launch_prep(static_cast<const float*>(patterns), n_rows, height, width, pattern_stride, binning,
+                         pix_index, n_pix, subtract_mean, o, stream);
+  }
+}
+
+extern "C" int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int height, int width,
+                                  int64_t pattern_stride, int binning, const int32_t* pix_index,
+                                  int n_pix, int subtract_mean, float* out_f32, int64_t ld_f32,
+                                  void* out_lp, int lp_dtype, int64_t ld_lp, float* out_norm,
+                                  float* out_lp_scale, void* stream) {
+  return ebsd_prep_patterns_typed(patterns, EBSD_PAT_F32, n_rows, height, width, pattern_stride, binning,
+                                  pix_index, n_pix, subtract_mean, out_f32, ld_f32, out_lp, lp_dtype, ld_lp,
+                                  out_norm, out_lp_scale, stream);
 }
 
 extern "C" int ebsd_sample_master_pattern(const float* master_pattern, int mp_h, int mp_w2,

@@ -80,7 +80,7 @@ def _master_pattern_tensor(mp, binning: int, device) -> Tensor:
 
 def _pattern_source(experiment_patterns, device):
     pats = experiment_patterns.patterns
-    if pats.dtype != torch.float32:
+    if pats.dtype not in kernels.PATTERN_DTYPES:
         pats = pats.float()
     if pats.device.type == "cuda" and pats.device != device:
         pats = pats.to(device)

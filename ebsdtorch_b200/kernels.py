@@ -108,11 +108,17 @@ def project(master_pattern: torch.Tensor, rays_soa: torch.Tensor, quats: torch.T
          _stream(quats.device))
 
 
+PATTERN_DTYPES = {torch.float32: 0, torch.uint16: 1, torch.uint8: 2, torch.float16: 3}
+
+
 def prep_patterns(patterns: torch.Tensor, out: RowBuffers, binning: int = 1,
                   pix_index: Optional[torch.Tensor] = None, n_pix: Optional[int] = None,
                   subtract_mean: bool = True) -> None:
-    """K2: (n, H, W) fp32 patterns (row stride may exceed H*W) -> rows in `out`."""
-    _cuda(patterns, "patterns", torch.float32, contiguous=False)
+    """K2: (n, H, W) patterns (fp32, uint16 / uint8 counts or fp16; row stride
+    may exceed H*W) -> rows in `out`."""
+    if patterns.dtype not in PATTERN_DTYPES:
+        raise TypeError(f"patterns must be float32, uint16, uint8 or float16, got {patterns.dtype}")
+    _cuda(patterns, "patterns", patterns.dtype, contiguous=False)
     if patterns.dim() == 2:
         patterns = patterns.unsqueeze(1)
     n, h, w = patterns.shape
@@ -123,8 +129,9 @@ def prep_patterns(patterns: torch.Tensor, out: RowBuffers, binning: int = 1,
         n_pix = pix_index.numel()
     elif n_pix is None:
         n_pix = (h // binning) * (w // binning)
-    call("ebsd_prep_patterns", ptr(patterns), n, h, w, patterns.stride(0), int(binning), ptr(pix_index), int(n_pix),
-         int(bool(subtract_mean)), *out.args(n_pix), _stream(patterns.device))
+    call("ebsd_prep_patterns_typed", ptr(patterns), PATTERN_DTYPES[patterns.dtype], n, h, w, patterns.stride(0),
+         int(binning), ptr(pix_index), int(n_pix), int(bool(subtract_mean)), *out.args(n_pix),
+         _stream(patterns.device))
 
 
 def sample_master_pattern(master_pattern: torch.Tensor, xyz: torch.Tensor, normalize: bool) -> torch.Tensor:

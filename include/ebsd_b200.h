@@ -117,6 +117,20 @@ int ebsd_prep_patterns(const float* patterns, int64_t n_rows, int height, int wi
                        int64_t pattern_stride, int binning, const int32_t* pix_index, int n_pix,
                        int subtract_mean, float* out_f32, int64_t ld_f32, void* out_lp, int lp_dtype,
                        int64_t ld_lp, float* out_norm, float* out_lp_scale, void* stream);
+/* Same, for patterns stored as detector counts or half floats:
+ * pattern_dtype EBSD_PAT_F32 (float), EBSD_PAT_U16 (uint16), EBSD_PAT_U8
+ * (uint8) or EBSD_PAT_F16 (IEEE half); values are converted to FP32 before
+ * binning. pattern_stride is in elements. (The reference keeps its
+ * ExperimentPatterns in float; integer counts halve or quarter the bytes read
+ * and copied.) */
+#define EBSD_PAT_F32 0
+#define EBSD_PAT_U16 1
+#define EBSD_PAT_U8 2
+#define EBSD_PAT_F16 3
+int ebsd_prep_patterns_typed(const void* patterns, int pattern_dtype, int64_t n_rows, int height, int width,
+                             int64_t pattern_stride, int binning, const int32_t* pix_index, int n_pix,
+                             int subtract_mean, float* out_f32, int64_t ld_f32, void* out_lp, int lp_dtype,
+                             int64_t ld_lp, float* out_norm, float* out_lp_scale, void* stream);
 
 /* Bilinear sample of the side-by-side master pattern at n points on the
  * sphere (xyz, n x 3 fp32; normalised first when `normalize`), grid_sample

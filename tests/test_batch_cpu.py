@@ -1,0 +1,55 @@
+"""Host-side parts of batched indexing and the synthetic phases (no GPU)."""
+
+import json
+
+import torch
+
+
+def test_launch_tuner_picks_fastest_and_caches(tmp_path):
+    from ebsdtorch_b200.batch import LAUNCH_SHAPES, LaunchTuner
+
+    calls = []
+    cost = {i: 5.0 - 0.5 * i for i in range(len(LAUNCH_SHAPES))}
+
+    def time_shape(shape):
+        i = [dict(s) for s in LAUNCH_SHAPES].index(shape)
+        calls.append(i)
+        return cost[i]
+
+    path = tmp_path / "tune.json"
+    t = LaunchTuner(cache_file=str(path), repeats=2)
+    key = LaunchTuner.key(16384, 328720, "bf16", 32, True, 148)
+    best = t.pick(key, time_shape)
+    assert best == dict(LAUNCH_SHAPES[-1])
+    assert len(calls) == 3 * len(LAUNCH_SHAPES)  # warm-up + 2 repeats each
+    assert t.pick(key, time_shape) == best and len(calls) == 3 * len(LAUNCH_SHAPES)
+    saved = json.loads(path.read_text())
+    assert saved[key]["shape"] == best
+    t2 = LaunchTuner(cache_file=str(path))
+
+    def never(shape):
+        raise AssertionError("re-timed a cached shape")
+
+    assert t2.pick(key, never) == best
+    assert LaunchTuner.key(3600, 36829, "fp8", 32, False, 148) != key
+
+
+def test_synthetic_master_pattern_bands_are_closed_under_the_laue_group():
+    """Every band normal of a non-cubic synthetic phase maps to a band normal
+    (up to sign) under each rotation of its Laue group, so the pattern has
+    the group's symmetry and FZ dictionaries index it correctly."""
+    from ebsdtorch_b200 import synthetic
+
+    for laue, order in ((5, 8), (9, 12), (7, 6), (3, 4)):
+        rots = synthetic.laue_rotations(laue)
+        assert rots.shape[0] == order
+        g = torch.Generator().manual_seed(0)
+        nv = torch.randn(3, generator=g, dtype=torch.float64)
+        nv = nv / nv.norm()
+        orbit = [synthetic._qrot(q, nv) for q in rots]
+        for q in rots:
+            for o in orbit:
+                m = synthetic._qrot(q, o)
+                assert max(abs(float(m @ x)) for x in orbit) > 1 - 1e-9
+    img = synthetic.synthetic_master_pattern(33, seed=4, laue_group=9)
+    assert img.shape == (33, 66) and torch.isfinite(img).all()

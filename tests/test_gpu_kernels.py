@@ -205,6 +205,58 @@ def test_match_and_rescore_match_oracle(lp, nq, nd, p, k):
     assert np.abs(val - ref_v).max() <= 1e-5 * np.abs(ref_v).max()
 
 
+@pytest.mark.parametrize("lp,shape", [
+    ("bf16", dict(persistent=True, splits=4)),
+    ("bf16", dict(persistent=True, splits=2, tile_n=128)),
+    ("bf16", dict(tile_n=128)),
+    ("bf16", dict(wave_tiles=2, splits=3)),
+    ("fp8", dict(persistent=True, splits=8)),
+    ("fp8", dict(tile_n=128, splits=5)),
+])
+def test_match_launch_shapes_give_identical_results(lp, shape):
+    """Every launch shape the batch autotuner may pick (128- or 256-row tiles,
+    persistent or one-wave launches, any number of dictionary ranges) returns
+    exactly the default shape's top-k."""
+    from ebsdtorch_b200 import kernels
+    from ebsdtorch_b200.engine import Searcher, SearchConfig
+
+    p, nd, nq, k = 320, 5000, 2300, 6
+    d = _rows(nd, p, 11)
+    q = d[np.arange(nq) * 2] + 0.4 * _rows(nq, p, 12)
+    dt, qt = torch.from_numpy(d).float().to(DEV), torch.from_numpy(q).float().to(DEV)
+
+    def fill_d(d0, d1, bufs):
+        kernels.prep_patterns(dt[d0:d1].reshape(d1 - d0, 1, p), bufs, subtract_mean=False)
+
+    def fill_q(q0, q1, bufs):
+        kernels.prep_patterns(qt[q0:q1].reshape(q1 - q0, 1, p), bufs, subtract_mean=False)
+
+    base_i, base_v = Searcher(nd, nq, p, k, SearchConfig(precision=lp), DEV).run(fill_d, fill_q)
+    i2, v2 = Searcher(nd, nq, p, k, SearchConfig(precision=lp, **shape), DEV).run(fill_d, fill_q)
+    assert torch.equal(base_i, i2)
+    assert torch.equal(base_v, v2)
+
+
+def test_prep_patterns_integer_counts():
+    """uint16 / uint8 / fp16 detector counts prepare to the same rows as the
+    same values in float32."""
+    from ebsdtorch_b200 import kernels
+    from ebsdtorch_b200.kernels import RowBuffers
+
+    counts = torch.randint(0, 250, (9, 20, 24), dtype=torch.int32)
+    ref = torch.empty((9, 480), device=DEV)
+    kernels.prep_patterns(counts.float().to(DEV), RowBuffers(f32=ref))
+    for dt in (torch.uint16, torch.uint8, torch.float16):
+        out = torch.empty((9, 480), device=DEV)
+        kernels.prep_patterns(counts.to(dt).to(DEV), RowBuffers(f32=out))
+        assert torch.equal(out, ref), dt
+    b2 = torch.empty((9, 120), device=DEV)
+    r2 = torch.empty((9, 120), device=DEV)
+    kernels.prep_patterns(counts.to(torch.uint16).to(DEV), RowBuffers(f32=b2), binning=2)
+    kernels.prep_patterns(counts.float().to(DEV), RowBuffers(f32=r2), binning=2)
+    assert torch.equal(b2, r2)
+
+
 def test_match_chunked_dictionary_and_queries():
     """Dictionary chunks with a running merge and several query chunks."""
     from ebsdtorch_b200 import kernels
