@@ -53,7 +53,9 @@ def test_batch_matches_per_map_fp32_search_and_graph_replays():
     b = BatchIndexer(jobs, dictionary_resolution_degrees={11: 4.0, 5: 5.0})
     b.run(use_graph=False)
     plan = b.describe()
-    assert len(plan) == 6  # (phase, detector, top_k, rescore) sub-groups
+    # (phase, detector, top_k, rescore) sub-groups: the two 32x32 4/mmm maps
+    # with top-2 and FP32 re-score are searched together
+    assert len(plan) == 5 and sum(e["maps"] for e in plan) == 6
     for entry in plan:
         la = entry["launch"]
         assert any(la["tile_n"] == (s.get("tile_n") or 256) and la["persistent"] == s.get("persistent", False)
