@@ -217,6 +217,12 @@ class BatchIndexer:
                                        query_chunk=min(self.query_chunk, round_up(sub.n_queries, TILE_Q)),
                                        workspace_bytes=_NO_BUDGET_LIMIT)
         self._phase_of_map = {m: g.phase for g in self.groups for sub in g.subgroups.values() for m in sub.maps}
+        # one arena for the dictionary rows of every group: groups run one
+        # after the other, and a single block (rather than one allocation per
+        # group shape) keeps the graph's memory at the largest group
+        self._arena_bytes = max(RowSet.storage_bytes(self.phases[g.phase]["ori"].shape[0], g.rays.shape[1], TILE_D,
+                                                     LP_DTYPES[g.precision], g.rescore) for g in self.groups)
+        self._arena: Optional[torch.Tensor] = None
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.graph: Optional[torch.cuda.CUDAGraph] = None
         self._outputs = None
@@ -260,7 +266,10 @@ class BatchIndexer:
     def _dictionary(self, g: _Group) -> RowSet:
         ph = self.phases[g.phase]
         ori = ph["ori"]
-        rows = RowSet(ori.shape[0], g.rays.shape[1], TILE_D, LP_DTYPES[g.precision], g.rescore, self.device)
+        if self._arena is None:
+            self._arena = torch.empty(self._arena_bytes, dtype=torch.uint8, device=self.device)
+        rows = RowSet(ori.shape[0], g.rays.shape[1], TILE_D, LP_DTYPES[g.precision], g.rescore, self.device,
+                      storage=self._arena)
         kernels.project(ph["mp"], g.rays, ori, rows.buffers(0, ori.shape[0]))
         return rows
 
@@ -351,6 +360,7 @@ class BatchIndexer:
             exp.combine_indexing_results(higher_is_better=True)
 
     def release_graph(self) -> None:
-        """Drop the captured graph and its memory pool."""
+        """Drop the captured graph, its memory pool and the dictionary arena."""
         self.graph = None
         self._outputs = None
+        self._arena = None

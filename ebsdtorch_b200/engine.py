@@ -75,14 +75,55 @@ def _pow2_at_least(n: int) -> int:
 class RowSet:
     """Low-precision + FP32 rows of a dictionary (or query) block on the GPU."""
 
-    def __init__(self, n_rows: int, n_pix: int, pad_rows: int, lp_dtype: int, keep_f32: bool, device):
+    def __init__(self, n_rows: int, n_pix: int, pad_rows: int, lp_dtype: int, keep_f32: bool, device,
+                 storage: Optional[torch.Tensor] = None):
+        """storage: optional uint8 device tensor of at least
+        storage_bytes(...) bytes to carve the buffers from (re-used between
+        dictionaries of different shapes); its padding rows are zeroed here."""
         self.n_rows, self.n_pix, self.lp_dtype = n_rows, n_pix, lp_dtype
         self.k_pad = round_up(n_pix, LP_KMULT[lp_dtype])
         rows_pad = round_up(max(n_rows, 1), pad_rows)
-        self.lp = torch.zeros((rows_pad, self.k_pad), dtype=LP_TORCH[lp_dtype], device=device)
-        self.f32 = torch.empty((n_rows, n_pix), dtype=torch.float32, device=device) if keep_f32 else None
-        self.norm = torch.zeros(rows_pad, dtype=torch.float32, device=device)
-        self.lp_scale = torch.ones(rows_pad, dtype=torch.float32, device=device) if lp_dtype != kernels.DT_BF16 else None
+        lp_t = LP_TORCH[lp_dtype]
+        if storage is None:
+            self.lp = torch.zeros((rows_pad, self.k_pad), dtype=lp_t, device=device)
+            self.f32 = torch.empty((n_rows, n_pix), dtype=torch.float32, device=device) if keep_f32 else None
+            self.norm = torch.zeros(rows_pad, dtype=torch.float32, device=device)
+            self.lp_scale = torch.ones(rows_pad, dtype=torch.float32, device=device) \
+                if lp_dtype != kernels.DT_BF16 else None
+            return
+        need = RowSet.storage_bytes(n_rows, n_pix, pad_rows, lp_dtype, keep_f32)
+        if storage.dtype != torch.uint8 or storage.numel() < need:
+            raise ValueError(f"row storage holds {storage.numel()} bytes, {need} needed")
+        views, off = [], 0
+        for shape, dt in RowSet._layout(n_rows, n_pix, pad_rows, lp_dtype, keep_f32):
+            nbytes = math.prod(shape) * torch.empty((), dtype=dt).element_size()
+            views.append(storage[off:off + nbytes].view(dt).view(shape) if nbytes else None)
+            off = round_up(off + nbytes, 256)
+        self.lp, self.f32, self.norm, self.lp_scale = views
+        if not keep_f32:
+            self.f32 = None
+        if lp_dtype == kernels.DT_BF16:
+            self.lp_scale = None
+        else:
+            self.lp_scale.fill_(1.0)
+        # rows beyond n_rows take part in the tensor-core tiles: zero them
+        self.lp[n_rows:].zero_()
+        self.norm[n_rows:].zero_()
+
+    @staticmethod
+    def _layout(n_rows: int, n_pix: int, pad_rows: int, lp_dtype: int, keep_f32: bool):
+        k_pad = round_up(n_pix, LP_KMULT[lp_dtype])
+        rows_pad = round_up(max(n_rows, 1), pad_rows)
+        return [((rows_pad, k_pad), LP_TORCH[lp_dtype]), ((n_rows if keep_f32 else 0, n_pix), torch.float32),
+                ((rows_pad,), torch.float32), ((rows_pad if lp_dtype != kernels.DT_BF16 else 0,), torch.float32)]
+
+    @staticmethod
+    def storage_bytes(n_rows: int, n_pix: int, pad_rows: int, lp_dtype: int, keep_f32: bool) -> int:
+        """Bytes of `storage` a RowSet of this shape needs (256-byte aligned parts)."""
+        off = 0
+        for shape, dt in RowSet._layout(n_rows, n_pix, pad_rows, lp_dtype, keep_f32):
+            off = round_up(off + math.prod(shape) * torch.empty((), dtype=dt).element_size(), 256)
+        return off
 
     def buffers(self, r0: int, r1: int, with_f32: bool = True) -> RowBuffers:
         return RowBuffers(
