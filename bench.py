@@ -355,6 +355,36 @@ def run_ours(args, wl):
                            "of 8192, timed on the same GPU for a query subset and extrapolated"}
         del q_sub
 
+    # ---- the e4m3 path on the same patterns (device-resident, same timing) ----
+    fp8 = None
+    if args.precision == "bf16" and not args.no_fp8:
+        exp8 = ExperimentPatterns(pats)
+        kw8 = dict(kw, precision="fp8")
+
+        def step8():
+            torch.manual_seed(0)
+            dictionary_index_orientations(mp, geom, exp8, **kw8)
+
+        step8()
+        torch.cuda.synchronize()
+        _barrier(dist)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            step8()
+        f1.record()
+        torch.cuda.synchronize()
+        _barrier(dist)
+        t8 = _max_over_ranks(f0.elapsed_time(f1) / 1e3, dist, dev)
+        i8 = exp8.raw_indexing_indices[0][:, 0]
+        fp8 = {"value": n * wl["Q"] * args.steps / t8, "unit": UNIT, "ms_per_step": t8 / args.steps * 1e3,
+               "same_top1_index_as_bf16": float((i8 == exp.raw_indexing_indices[0][:, 0]).float().mean()),
+               "precision": "e4m3 match (per-row absmax scale) + FP32 re-score of top-32"}
+        if fp32_cmp is not None:
+            fp8["same_top1_index_as_plain_fp32_di"] = float((i8[:n_sub] == ref_idx[:, 0]).float().mean())
+            fp8["speedup_vs_plain_fp32_gpu_di"] = fp8["value"] / n / fp32_cmp["plain_fp32_gpu_di_rate"]
+        del exp8
+
     # ---- end to end: host (pinned) patterns, H2D + D2H inside the timed region ----
     e2e = None
     if not args.no_e2e:
@@ -406,6 +436,7 @@ def run_ours(args, wl):
                      "share_of_step": match_share},
         "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
         "plain_fp32_di": fp32_cmp,
+        "fp8": fp8,
         "clocks": clk,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -650,6 +681,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
+    ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
     ap.add_argument("--fp32-subset", type=int, default=4096)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (config 3) instead")
