@@ -123,49 +123,57 @@ __device__ __forceinline__ bool better(float v, int64_t i, float bv, int64_t bi)
   return i >= 0 && (bi < 0 || v > bv || (v == bv && i < bi));
 }
 
-// Dot of the shared-memory FP32 query row with one low-precision row covering
+// Dot of the shared-memory bf16 query row with one low-precision row covering
 // n_vec 16-byte chunks (zero padded; the query is padded with zeros). One
 // candidate row per warp measured fastest on B200 (two or four rows per warp
 // interleaved, or deeper unrolling, were 5-30 % slower).
 template <int LP>
-__device__ __forceinline__ float lp_dot(const float* qrow, const uint4* __restrict__ d, int n_vec, int lane) {
+__device__ __forceinline__ float lp_dot(const __nv_bfloat16* qh, const uint4* __restrict__ d, int n_vec, int lane) {
+  // qh: the query row in bf16 (shared memory): 16 bytes of query per 16 bytes
+  // of bf16 row instead of 32, which halves the shared-memory side of the
+  // L1/shared pipe these stages are bound by; products and sums stay FP32
   float acc = 0.f;
+  const uint4* q16 = reinterpret_cast<const uint4*>(qh);
   for (int v = lane; v < n_vec; v += 32) {
     const uint4 u = __ldg(d + v);
     const uint32_t w[4] = {u.x, u.y, u.z, u.w};
     if constexpr (LP == EBSD_DT_BF16) {
-      const float4 qa = reinterpret_cast<const float4*>(qrow)[2 * v];
-      const float4 qb = reinterpret_cast<const float4*>(qrow)[2 * v + 1];
-      const float qv[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
+      const uint4 qv = q16[v];
+      const uint32_t qw[4] = {qv.x, qv.y, qv.z, qv.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[e]));
-        acc = fmaf(f.x, qv[2 * e], acc);
-        acc = fmaf(f.y, qv[2 * e + 1], acc);
+        const float2 g = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&qw[e]));
+        acc = fmaf(f.x, g.x, acc);
+        acc = fmaf(f.y, g.y, acc);
       }
     } else {
+      const uint4 qa = q16[2 * v], qb = q16[2 * v + 1];
+      const uint32_t qw[8] = {qa.x, qa.y, qa.z, qa.w, qb.x, qb.y, qb.z, qb.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const float4 q4 = reinterpret_cast<const float4*>(qrow)[4 * v + e];
         const __half2_raw lo = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[e] & 0xffffu), __NV_E4M3);
         const __half2_raw hi = __nv_cvt_fp8x2_to_halfraw2((__nv_fp8x2_storage_t)(w[e] >> 16), __NV_E4M3);
         const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&lo));
         const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&hi));
-        acc = fmaf(a.x, q4.x, acc);
-        acc = fmaf(a.y, q4.y, acc);
-        acc = fmaf(b.x, q4.z, acc);
-        acc = fmaf(b.y, q4.w, acc);
+        const float2 g0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&qw[2 * e]));
+        const float2 g1 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&qw[2 * e + 1]));
+        acc = fmaf(a.x, g0.x, acc);
+        acc = fmaf(a.y, g0.y, acc);
+        acc = fmaf(b.x, g1.x, acc);
+        acc = fmaf(b.y, g1.y, acc);
       }
     }
   }
   return warp_sum(acc);
 }
 
-// FP32 dot of the shared-memory query row with one FP32 row; 16-byte loads,
-// four in flight per lane, when the row is 16-byte aligned and n_pix % 4 == 0.
+// FP32 dot of the query row (shared or global memory) with one FP32 row;
+// 16-byte loads, four in flight per lane, when both rows are 16-byte aligned
+// and n_pix % 4 == 0.
 __device__ __forceinline__ float f32_dot(const float* qrow, const float* __restrict__ drow, int n_pix, int lane) {
   float acc = 0.f;
-  if ((n_pix & 3) == 0 && (reinterpret_cast<uintptr_t>(drow) & 15) == 0) {
+  if ((n_pix & 3) == 0 && ((reinterpret_cast<uintptr_t>(drow) | reinterpret_cast<uintptr_t>(qrow)) & 15) == 0) {
     const float4* d4 = reinterpret_cast<const float4*>(drow);
     const float4* q4 = reinterpret_cast<const float4*>(qrow);
     const int n4 = n_pix >> 2;
@@ -200,7 +208,9 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
     int edge, const int32_t* __restrict__ cell_to_row, const float4* __restrict__ dict_quats, const LocalRows rows,
     int64_t n_dict, int n_pix, int n_pix_pad, int laue, int radius, float cos_half_max, float fz_slack, int max_cand,
     int64_t* __restrict__ out_idx, float* __restrict__ out_score, int32_t* __restrict__ out_ncand) {
-  extern __shared__ float qrow[];
+  extern __shared__ __align__(16) uint8_t qsm[];
+  float* qrow = reinterpret_cast<float*>(qsm);                  // LP 0: FP32 query row
+  __nv_bfloat16* qh = reinterpret_cast<__nv_bfloat16*>(qsm);    // LP rows: bf16 query row
   __shared__ int cand[kMaxLocalCand];
   __shared__ int base_cell[24][3];
   __shared__ float4 copy_q[24];
@@ -212,7 +222,13 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
   __shared__ int64_t sel[kRescoreMax];
   const int64_t q = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-  for (int p = tid; p < n_pix_pad; p += blockDim.x) qrow[p] = p < n_pix ? q_f32[q * ld_q + p] : 0.f;
+  for (int p = tid; p < n_pix_pad; p += blockDim.x) {
+    const float v = p < n_pix ? q_f32[q * ld_q + p] : 0.f;
+    if constexpr (LP == 0)
+      qrow[p] = v;
+    else
+      qh[p] = __float2bfloat16_rn(v);
+  }
   if (tid == 0) n_cand = 0;
   const double kHalf = 1.0725146985555127, step = 2.0 * kHalf / edge;
   bool my_ok = false;
@@ -306,7 +322,7 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
     for (int c = wid; c < nc; c += kLocalWarps) {
       const int64_t row = cand[c];
       const uint4* d = reinterpret_cast<const uint4*>(lp_base + row * rows.ld_lp * esz);
-      const float v = lp_dot<LP>(qrow, d, n_vec, lane) * __ldg(rows.norm + row) *
+      const float v = lp_dot<LP>(qh, d, n_vec, lane) * __ldg(rows.norm + row) *
                       (rows.lp_scale ? __ldg(rows.lp_scale + row) : 1.f);
       keep_best<kRescoreMax>(bv, bi, v, row);
     }
@@ -361,7 +377,9 @@ __global__ void __launch_bounds__(kLocalThreads) k_local_search(
       // FP32 re-score: warp w takes the w-th selected row
       if (wid < n_sel) {
         const int64_t row = sel[wid];
-        const float acc = row >= 0 ? f32_dot(qrow, rows.f32 + row * rows.ld_f32, n_pix, lane) : -INFINITY;
+        // the FP32 query row from global memory (L2-resident after the fill)
+        const float acc = row >= 0 ? f32_dot(q_f32 + q * ld_q, rows.f32 + row * rows.ld_f32, n_pix, lane)
+                                   : -INFINITY;
         if (lane == 0) {
           best_v[wid][0] = acc;
           best_i[wid][0] = row;
@@ -456,7 +474,7 @@ extern "C" int ebsd_local_search(const float* q_f32, int64_t ld_q, int64_t n_que
   LaueTable t{};
   build_laue_table(laue_id, &t);
   LocalRows rows{d_f32, ld_d, d_lp, ld_lp, d_norm, d_lp_scale, n_rescore};
-  const size_t smem = (size_t)n_pix_pad * sizeof(float);
+  const size_t smem = (size_t)n_pix_pad * (d_lp ? sizeof(__nv_bfloat16) : sizeof(float));
   auto run = [&](auto kern) -> int {
     EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     kern<<<(int)n_queries, kLocalThreads, smem, as_stream(stream)>>>(
