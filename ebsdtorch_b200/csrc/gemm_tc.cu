@@ -102,7 +102,7 @@ __device__ __forceinline__ void report_timeout(const GemmParams& p, volatile int
 // MODE 0: top-k epilogue. MODE 1: store epilogue. MODE 2: convolution
 // epilogue, out[col, row] = act(acc[row, col] + bias[row]) stored transposed
 // in bf16 (and FP32 when asked).
-template <int KIND, int MODE, int KC, int BN>
+template <int KIND, int MODE, int KC, int BN, bool PERSIST>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const GemmParams p) {
@@ -125,13 +125,19 @@ __global__ void __launch_bounds__(THREADS, 1)
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // work unit -> (query tile, dictionary tile range)
-  auto unit_tile = [&](int u) { return u / p.splits; };
-  auto unit_range = [&](int u, int& n_begin, int& n_end) {
-    const int split = u - (u / p.splits) * p.splits;
-    n_begin = (int)((int64_t)split * p.n_tiles / p.splits);
-    n_end = (int)((int64_t)(split + 1) * p.n_tiles / p.splits);
+  // work unit -> (query tile, dictionary tile range); the lambdas capture
+  // copies of the two fields rather than the kernel parameter itself
+  const int n_splits = p.splits, n_tiles = p.n_tiles;
+  auto unit_tile = [=](int u) { return u / n_splits; };
+  auto unit_range = [=](int u, int& n_begin, int& n_end) {
+    const int split = u - (u / n_splits) * n_splits;
+    n_begin = (int)((int64_t)split * n_tiles / n_splits);
+    n_end = (int)((int64_t)(split + 1) * n_tiles / n_splits);
   };
+  // units of this CTA: blockIdx.x, + gridDim.x, ... when persistent; else
+  // only blockIdx.x
+  const int u_step = PERSIST ? (int)gridDim.x : 1;
+  const int u_end = PERSIST ? p.units : (int)blockIdx.x + 1;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -162,12 +168,13 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t stage = 0, phase = 0;
       int64_t issued = 0;
       bool ok = true;
-      for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+      const int k_iters = p.k_iters;
+      auto produce_unit = [&](int u) {
         const int a_row = unit_tile(u) * BM;
         int n_begin, n_end;
         unit_range(u, n_begin, n_end);
         for (int n = n_begin; n < n_end && ok; ++n) {
-          for (int k = 0; k < p.k_iters; ++k) {
+          for (int k = 0; k < k_iters; ++k) {
             if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
               ok = false;
               break;
@@ -184,6 +191,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
           }
         }
+      };
+      // one unit: straight-line code (a unit loop in the producer or MMA
+      // thread measured 15 % slower on one-wave launches)
+      if constexpr (PERSIST) {
+        for (int u = blockIdx.x; u < u_end && ok; u += u_step) produce_unit(u);
+      } else {
+        produce_unit(blockIdx.x);
       }
       if (!ok) {
         report_timeout(p, abort_flag);
@@ -211,7 +225,8 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t acc_phase = 0;
       bool ok = true, any = false;
       constexpr uint32_t idesc = make_idesc<KIND, BN>();
-      for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+      const int k_iters = p.k_iters;
+      auto mma_unit = [&](int u) {
         int n_begin, n_end;
         unit_range(u, n_begin, n_end);
         for (int n = n_begin; n < n_end && ok; ++n) {
@@ -221,7 +236,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           }
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
-          for (int k = 0; k < p.k_iters; ++k) {
+          for (int k = 0; k < k_iters; ++k) {
             if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
               ok = false;
               break;
@@ -229,7 +244,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             tc_fence_after();
             const uint32_t a_addr = sbase + stage * STAGE_BYTES;
             const uint32_t b_addr = a_addr + A_BYTES;
-  #pragma unroll
+#pragma unroll
             for (int kk = 0; kk < BKB / 32; ++kk) {
               tc_mma<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32),
                            idesc, (k | kk) != 0 ? 1u : 0u);
@@ -248,6 +263,11 @@ __global__ void __launch_bounds__(THREADS, 1)
             acc_phase ^= 1u;
           }
         }
+      };
+      if constexpr (PERSIST) {
+        for (int u = blockIdx.x; u < u_end && ok; u += u_step) mma_unit(u);
+      } else {
+        mma_unit(blockIdx.x);
       }
       if (!ok) {
         report_timeout(p, abort_flag);
@@ -271,12 +291,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     int acc = 0;
     uint32_t acc_phase = 0;
     bool ok = true;
-    for (int u = blockIdx.x; u < p.units && ok; u += gridDim.x) {
+    for (int u = blockIdx.x; u < u_end && ok; u += u_step) {
       const int m_tile = unit_tile(u);
-      const int split = u - m_tile * p.splits;
+      const int split = u - m_tile * n_splits;
       int n_begin, n_end;
       unit_range(u, n_begin, n_end);
-  #pragma unroll
+#pragma unroll
       for (int j = 0; j < KC; ++j) {
         bv[j] = -INFINITY;
         bi[j] = -1;
@@ -290,7 +310,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         tc_fence_after();
         const int64_t tile_col = (int64_t)n * BN;
-  #pragma unroll 1
+#pragma unroll 1
         for (int c = 0; c < BN / 32; ++c) {
           __syncwarp();
           float v[32];
@@ -302,7 +322,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (col0 + 32 <= p.n_valid) {
               if (p.col_scale) {
                 const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
-  #pragma unroll
+#pragma unroll
                 for (int j4 = 0; j4 < 8; ++j4) {
                   const float4 s4 = __ldg(cs + j4);
                   v[4 * j4 + 0] *= s4.x;
@@ -312,17 +332,17 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
               }
             } else {
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 32; ++j) {
                 const bool valid = col0 + j < p.n_valid;
                 const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
                 v[j] = valid ? v[j] * sc : -INFINITY;
               }
             }
-  #pragma unroll
+#pragma unroll
             for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
             if (mask) {
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 32; ++j) scratch[j * EPI_THREADS + etid] = v[j];
               while (mask) {
                 const int j = __ffs(mask) - 1;
@@ -337,7 +357,7 @@ __global__ void __launch_bounds__(THREADS, 1)
               const float b = p.bias ? __ldg(p.bias + grow) : 0.f;
               // the warp's 32 threads own 32 consecutive channels: each store
               // instruction writes 32 consecutive values of one pixel
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 32; ++j) {
                 const int64_t col = col0 + j;
                 if (col < p.n_valid) {
@@ -352,7 +372,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             const int64_t grow = (int64_t)m_tile * BM + row;
             if (grow < p.m_valid) {
               float* dst = p.C + grow * p.ldc;
-  #pragma unroll
+#pragma unroll
               for (int j = 0; j < 32; ++j) {
                 const int64_t col = col0 + j;
                 if (col < p.n_valid) {
@@ -374,7 +394,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (ok) {
           const int64_t q = (int64_t)m_tile * BM + row;
           const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
-  #pragma unroll
+#pragma unroll
           for (int j = 0; j < KC; ++j) {
             p.part_val[base + j] = bv[j];
             p.part_idx[base + j] = bi[j];
@@ -442,10 +462,10 @@ static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t ro
   return 0;
 }
 
-template <int KIND, int MODE, int KC, int BN>
+template <int KIND, int MODE, int KC, int BN, bool PERSIST = false>
 static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
                   cudaStream_t s) {
-  auto kern = k_tc_gemm<KIND, MODE, KC, BN>;
+  auto kern = k_tc_gemm<KIND, MODE, KC, BN, PERSIST>;
   constexpr int smem = Tile<BN>::SMEM_BYTES;
   EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   kern<<<grid, THREADS, smem, s>>>(a, b, p);
@@ -453,20 +473,30 @@ static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& 
   return 0;
 }
 
-template <int KIND, int BN>
+template <int KIND, int BN, bool PERSIST>
 static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
                        int grid, cudaStream_t s) {
   switch (kc) {
-    case 1: return launch<KIND, 0, 1, BN>(a, b, p, grid, s);
-    case 2: return launch<KIND, 0, 2, BN>(a, b, p, grid, s);
-    case 4: return launch<KIND, 0, 4, BN>(a, b, p, grid, s);
-    case 8: return launch<KIND, 0, 8, BN>(a, b, p, grid, s);
-    case 16: return launch<KIND, 0, 16, BN>(a, b, p, grid, s);
-    case 32: return launch<KIND, 0, 32, BN>(a, b, p, grid, s);
-    case 64: return launch<KIND, 0, 64, BN>(a, b, p, grid, s);
+    case 1: return launch<KIND, 0, 1, BN, PERSIST>(a, b, p, grid, s);
+    case 2: return launch<KIND, 0, 2, BN, PERSIST>(a, b, p, grid, s);
+    case 4: return launch<KIND, 0, 4, BN, PERSIST>(a, b, p, grid, s);
+    case 8: return launch<KIND, 0, 8, BN, PERSIST>(a, b, p, grid, s);
+    case 16: return launch<KIND, 0, 16, BN, PERSIST>(a, b, p, grid, s);
+    case 32: return launch<KIND, 0, 32, BN, PERSIST>(a, b, p, grid, s);
+    case 64: return launch<KIND, 0, 64, BN, PERSIST>(a, b, p, grid, s);
   }
   set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
   return EBSD_ERR_ARG;
+}
+
+template <int KIND>
+static int launch_topk_shape(int kc, int tile_n, bool persist, const CUtensorMap& a, const CUtensorMap& b,
+                             const GemmParams& p, int grid, cudaStream_t s) {
+  if (tile_n == 128)
+    return persist ? launch_topk<KIND, 128, true>(kc, a, b, p, grid, s)
+                   : launch_topk<KIND, 128, false>(kc, a, b, p, grid, s);
+  return persist ? launch_topk<KIND, 256, true>(kc, a, b, p, grid, s)
+                 : launch_topk<KIND, 256, false>(kc, a, b, p, grid, s);
 }
 
 static int check_operands(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,
@@ -541,14 +571,13 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   p.slot_base = slot_base;
   p.index_base = index_base;
   p.status = d_status;
-  // max_ctas > 0: persistent launch, each CTA loops over units
-  const int grid = max_ctas > 0 ? std::min(p.units, max_ctas) : p.units;
+  // max_ctas > 0 and fewer CTAs than units: persistent launch, each CTA
+  // loops over its units
+  const bool persist = max_ctas > 0 && max_ctas < p.units;
+  const int grid = persist ? max_ctas : p.units;
   cudaStream_t s = as_stream(stream);
-  if (tile_n == 128)
-    return lp_dtype == EBSD_DT_BF16 ? launch_topk<0, 128>(n_cand, ta, tb, p, grid, s)
-                                    : launch_topk<1, 128>(n_cand, ta, tb, p, grid, s);
-  return lp_dtype == EBSD_DT_BF16 ? launch_topk<0, 256>(n_cand, ta, tb, p, grid, s)
-                                  : launch_topk<1, 256>(n_cand, ta, tb, p, grid, s);
+  return lp_dtype == EBSD_DT_BF16 ? launch_topk_shape<0>(n_cand, tile_n, persist, ta, tb, p, grid, s)
+                                  : launch_topk_shape<1>(n_cand, tile_n, persist, ta, tb, p, grid, s);
 }
 
 extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
