@@ -15,55 +15,12 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "sampling.cuh"
 
 namespace ebsd {
 
 constexpr int kRowThreads = 512;
 constexpr int kMaxRowPix = 57344;  // 224 KiB of fp32 in shared memory
-
-__device__ __forceinline__ float2 lambert_side_by_side(float x, float y, float z) {
-  const float fac = sqrtf(fmaxf(2.0f * (1.0f - fabsf(z)), 0.0f));
-  const bool cond = fabsf(y) <= fabsf(x);
-  const float big = cond ? x : y;
-  const float sml = cond ? y : x;
-  const float sgn = big < 0.0f ? -1.0f : 1.0f;
-  const float simple = sgn * fac * 0.70710678118654752f;  // 2 / sqrt(8)
-  const float arct = sgn * fac * atan2f(sml * sgn, fabsf(big)) * 0.90031631615710607f;  // 2 sqrt2/pi
-  float u = cond ? simple : arct;
-  const float v = cond ? arct : simple;
-  u = u / 2.0f - 0.5f + (z < 0.0f ? 1.0f : 0.0f);
-  return make_float2(u, v);
-}
-
-// grid_sample(bilinear, align_corners=False, padding_mode="border") of one
-// point (u, v) in [-1, 1]^2 on an (h, w) image.
-__device__ __forceinline__ float sample_border(const float* __restrict__ img, int h, int w, float u,
-                                               float v) {
-  float ix = ((u + 1.0f) * (float)w - 1.0f) / 2.0f;
-  float iy = ((v + 1.0f) * (float)h - 1.0f) / 2.0f;
-  ix = fminf(fmaxf(ix, 0.0f), (float)(w - 1));
-  iy = fminf(fmaxf(iy, 0.0f), (float)(h - 1));
-  const float fx0 = floorf(ix), fy0 = floorf(iy);
-  const int x0 = (int)fx0, y0 = (int)fy0;
-  const int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
-  const float wnw = (fx0 + 1.0f - ix) * (fy0 + 1.0f - iy);
-  const float wne = (ix - fx0) * (fy0 + 1.0f - iy);
-  const float wsw = (fx0 + 1.0f - ix) * (iy - fy0);
-  const float wse = (ix - fx0) * (iy - fy0);
-  const float* r0 = img + (int64_t)y0 * w;
-  const float* r1 = img + (int64_t)y1 * w;
-  return __ldg(r0 + x0) * wnw + __ldg(r0 + x1) * wne + __ldg(r1 + x0) * wsw + __ldg(r1 + x1) * wse;
-}
-
-// Rotate v by unit quaternion q = (w, x, y, z): v + w t + q_vec x t,
-// t = 2 q_vec x v (equal to q (0, v) q* for unit q).
-__device__ __forceinline__ float3 rotate(float4 q, float vx, float vy, float vz) {
-  const float tx = 2.0f * (q.z * vz - q.w * vy);
-  const float ty = 2.0f * (q.w * vx - q.y * vz);
-  const float tz = 2.0f * (q.y * vy - q.z * vx);
-  return make_float3(vx + q.x * tx + (q.z * tz - q.w * ty), vy + q.x * ty + (q.w * tx - q.y * tz),
-                     vz + q.x * tz + (q.y * ty - q.z * tx));
-}
 
 struct RowOut {
   float* f32;

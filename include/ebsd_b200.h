@@ -262,6 +262,25 @@ int ebsd_split3_bf16(const float* X, int64_t n_rows, int n_cols, int64_t ld, con
 int ebsd_disori_angle(const float* q1, const float* q2, int64_t n, int laue_id, float* out,
                       void* stream);
 
+/* ---- orientation grid refinement (the step after DI) ------------------------
+ * Replaces orientation_grid_refinement's per-batch loop (refining.py:71-244)
+ * for one phase: for each pattern i, n_iter times, the n_grid (odd) local
+ * cubochoric offsets grid_cu (get_local_orientation_grid, refining.py:13-68)
+ * times the pattern's current scale become rotations cu2qu(.) composed with
+ * the current orientation, moved to the FZ (fz_left 0: the reference's
+ * ori_to_fz_laue, q g; 1: g q, which keeps the pattern), simulated with
+ * grid_sample(align_corners=True) on the master pattern (mp_h x mp_w2, binned
+ * already when binning), mean-subtracted and dotted with exp_rows[i] (zero-
+ * mean FP32, row stride ld_e); the best becomes current and, when it is the
+ * grid centre, the scale is multiplied by shrink. coords_soa (3 x n_pix): unit
+ * rays, or un-normalised detector coordinates when offsets (n x 2, the scan
+ * positions, average_pattern_center=False) is given. Writes q_out (n x 4,
+ * may alias q_in) and dots (n x n_iter) = the best score of each iteration. */
+int ebsd_refine_grid(const float* master_pattern, int mp_h, int mp_w2, const float* coords_soa, int n_pix,
+                     const float* offsets, const float* exp_rows, int64_t ld_e, const float* q_in, int64_t n,
+                     const float* grid_cu, int n_grid, int laue_id, int fz_left, int n_iter, float shrink,
+                     float* q_out, float* dots, void* stream);
+
 /* ---- local dictionary search around orientation proposals --------------------
  * No counterpart in the reference (search step of the learned-proposal path).
  * cell_to_row (edge^3 int32): dictionary row of each cubochoric grid cell or

@@ -481,15 +481,20 @@ def rosca_lambert_side_by_side(p: np.ndarray) -> np.ndarray:
     return np.stack((u, v), axis=-1)
 
 
-def grid_sample_border(img: np.ndarray, uv: np.ndarray) -> np.ndarray:
+def grid_sample_border(img: np.ndarray, uv: np.ndarray, align_corners: bool = False) -> np.ndarray:
     """Bilinear sampling of a (H, W) image at normalised (x, y) in [-1, 1],
-    align_corners=False, padding_mode='border' -- the semantics of
-    torch.nn.functional.grid_sample used by master_pattern.py:197-206.
-    Pixel coordinate = ((c + 1) * size - 1) / 2, clamped to [0, size - 1]."""
+    padding_mode='border' -- the semantics of torch.nn.functional.grid_sample
+    used by master_pattern.py:197-206. Pixel coordinate ((c + 1) * size - 1) / 2
+    (align_corners=False, dictionary indexing) or (c + 1) / 2 * (size - 1)
+    (align_corners=True, refining.py:206), clamped to [0, size - 1]."""
     H, W = img.shape
     dt = uv.dtype.type
-    fx = ((uv[..., 0] + dt(1.0)) * dt(W) - dt(1.0)) / dt(2.0)
-    fy = ((uv[..., 1] + dt(1.0)) * dt(H) - dt(1.0)) / dt(2.0)
+    if align_corners:
+        fx = (uv[..., 0] + dt(1.0)) / dt(2.0) * dt(W - 1)
+        fy = (uv[..., 1] + dt(1.0)) / dt(2.0) * dt(H - 1)
+    else:
+        fx = ((uv[..., 0] + dt(1.0)) * dt(W) - dt(1.0)) / dt(2.0)
+        fy = ((uv[..., 1] + dt(1.0)) * dt(H) - dt(1.0)) / dt(2.0)
     fx = np.clip(fx, 0, W - 1)
     fy = np.clip(fy, 0, H - 1)
     x0 = np.floor(fx).astype(np.int64)
@@ -913,3 +918,89 @@ def inv_rosca_lambert_north(uv: np.ndarray) -> np.ndarray:
     xo = np.copysign(np.where(cond, xh, yh), uv[..., 0])
     yo = np.copysign(np.where(cond, yh, xh), uv[..., 1])
     return np.stack((xo, yo, zo), axis=-1)
+
+
+# --------------------------------------------------------------------------
+# Orientation grid refinement (the first "next" step after DI)
+# --------------------------------------------------------------------------
+
+
+def local_orientation_grid(semi_edge_deg: float, radius: int, axial: int = 3) -> np.ndarray:
+    """(G, 3) cubochoric offsets of the local grid (refining.py:13-68): a
+    (2 radius + 1)^3 cube of semi-edge semi_edge_deg * pi^(2/3) / 360, all
+    points (axial 3), points with a zero coordinate (2) or on the axes (1)."""
+    s = semi_edge_deg * math.pi ** (2.0 / 3.0) / 360.0
+    c = np.linspace(-s, s, 2 * radius + 1)
+    cu = np.stack(np.meshgrid(c, c, c, indexing="ij"), axis=-1).reshape(-1, 3)
+    if axial == 2:
+        cu = cu[np.any(cu == 0, axis=-1)]
+    elif axial == 1:
+        cu = cu[np.sum(cu == 0, axis=-1) >= 2]
+    elif axial != 3:
+        raise ValueError("axial_grid_dimension must be 1, 2, or 3.")
+    return cu
+
+
+def ori_to_fz_laue_right(q: np.ndarray, laue_id: int) -> np.ndarray:
+    """The reference's orientation FZ reduction (laue_fz_ori.py:36-81): the
+    operator g maximising |(q g).w| is applied on the RIGHT, q g (qu_prod
+    then w >= 0)."""
+    g = laue_elements(laue_id)
+    prods = _qmul(q[..., None, :], g)
+    best = np.argmax(np.abs(prods[..., 0]), axis=-1)
+    return qu_std(np.take_along_axis(prods, best[..., None, None], axis=-2)[..., 0, :])
+
+
+def ori_to_fz_laue_left(q: np.ndarray, laue_id: int) -> np.ndarray:
+    """FZ reduction by the left product g q (the operator maximising |w|),
+    which keeps the simulated pattern: pattern(g q) == pattern(q)."""
+    g = laue_elements(laue_id)
+    prods = _qmul(g, q[..., None, :])
+    best = np.argmax(np.abs(prods[..., 0]), axis=-1)
+    return qu_std(np.take_along_axis(prods, best[..., None, None], axis=-2)[..., 0, :])
+
+
+def orientation_grid_refinement(master_pattern: np.ndarray, coords: np.ndarray, exp_rows: np.ndarray,
+                                q0: np.ndarray, laue_id: int, semi_edge_deg: float, n_iter: int = 3,
+                                axial: int = 3, radius: int = 1, shrink: float = 0.5,
+                                offsets: Optional[np.ndarray] = None, fz: str = "reference"):
+    """Grid refinement of one phase (refining.py:71-244), float64.
+
+    coords: (P, 3) detector coordinates in the sample frame (unit rays when
+    offsets is None; with offsets (n, 2), per pattern normalize(coords +
+    (offset, 0)), refining.py:117-128). exp_rows: (n, P) zero-mean patterns.
+    Each iteration composes the grid with the current orientation
+    (cu2qu(grid) q), reduces to the FZ (fz "reference": ori_to_fz_laue_right,
+    "left": ori_to_fz_laue_left), simulates with align_corners=True sampling,
+    subtracts each simulation's mean, takes the best dot product, moves there
+    and halves (shrink) the pattern's grid when the centre stayed best.
+    Returns (orientations (n, 4), best dots (n, n_iter))."""
+    grid = local_orientation_grid(semi_edge_deg, radius, axial)
+    n_grid = grid.shape[0]
+    centre = (n_grid - 1) // 2
+    n = q0.shape[0]
+    scale = np.ones(n)
+    q = np.asarray(q0, dtype=np.float64)
+    dots = np.zeros((n, n_iter))
+    reduce = ori_to_fz_laue_right if fz == "reference" else ori_to_fz_laue_left
+    for j in range(n_iter):
+        qg = cu2qu(grid[None] * scale[:, None, None])
+        qa = reduce(qu_std(_qmul(qg, q[:, None, :])), laue_id)
+        best_v = np.empty(n)
+        best_i = np.empty(n, dtype=np.int64)
+        for i in range(n):
+            if offsets is None:
+                rays = coords
+            else:
+                c = coords + np.concatenate((offsets[i], [0.0]))[None]
+                rays = c / np.linalg.norm(c, axis=-1, keepdims=True)
+            rot = qu_apply(qa[i][:, None, :], rays[None])
+            sims = grid_sample_border(master_pattern, rosca_lambert_side_by_side(rot), align_corners=True)
+            sims = sims - sims.mean(axis=-1, keepdims=True)
+            d = sims @ exp_rows[i]
+            best_i[i] = int(np.argmax(d))
+            best_v[i] = d[best_i[i]]
+        dots[:, j] = best_v
+        q = qa[np.arange(n), best_i]
+        scale = np.where(best_i == centre, scale * shrink, scale)
+    return q, dots

@@ -12,7 +12,7 @@ modified. The PCA variant is also loaded with line 355's component slice
 ``[:, -n : -n + 300]`` replaced by ``[:, -n:]`` (the "top" slice).
 
 Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
-outputs of one case. The files are small (< 1 MB each) and committed.
+outputs of one case (``--refinement-only`` writes just refine.npz). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -55,6 +55,70 @@ def smooth_master_pattern(seed: int, n: int) -> torch.Tensor:
     base = torch.rand((1, 1, 2 * n // 4 + 2, 2 * (2 * n // 4) + 2), generator=g)
     mp = torch.nn.functional.interpolate(base, size=(n, 2 * n), mode="bicubic", align_corners=True)[0, 0]
     return mp.contiguous().float()
+
+
+def refinement_goldens(root: str = "/root/reference"):
+    """Orientation grid refinement (ebsd/refining.py): local grids and three
+    refinement cases (kernel radius, axial grid, binning, shrink factor,
+    pattern-centre mode), float32 matching."""
+    sys.path.insert(0, root)
+    from ebsdtorch.ebsd.refining import get_local_orientation_grid, orientation_grid_refinement
+    from ebsdtorch.s2_and_so3.sampling import so3_uniform_quat
+    from ebsdtorch.s2_and_so3.quaternions import qu_prod
+    from ebsdtorch.s2_and_so3.orientations import ax2qu
+    from ebsdtorch.ebsd.geometry import EBSDGeometry
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.s2_and_so3.quaternions import qu_apply
+
+    out = {}
+    for i, (e, r, a) in enumerate(((2.0, 1, 3), (1.0, 2, 2), (1.5, 2, 1), (3.0, 3, 3))):
+        out[f"grid{i}"] = get_local_orientation_grid(e, r, a).numpy()
+        out[f"grid{i}_args"] = np.array([e, r, a], dtype=np.float64)
+    cases = [
+        dict(det=(20, 20), seed=31, n=14, b=1, edge=2.0, radius=1, axial=3, n_iter=3, shrink=0.5, avg=True),
+        dict(det=(24, 20), seed=32, n=9, b=2, edge=1.5, radius=2, axial=2, n_iter=4, shrink=0.6, avg=True),
+        dict(det=(16, 16), seed=33, n=7, b=1, edge=2.5, radius=1, axial=1, n_iter=3, shrink=0.5, avg=False),
+    ]
+    for ci, c in enumerate(cases):
+        torch.manual_seed(c["seed"])
+        mp_t = smooth_master_pattern(c["seed"], 41)
+        mp = MasterPattern(mp_t.clone(), laue_group=11)
+        geom = EBSDGeometry(c["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+        truth = so3_uniform_quat(c["n"], torch.device("cpu"))
+        dc = geom.get_coords_sample_frame(binning=(1, 1))
+        dc = dc / dc.norm(dim=-1, keepdim=True)
+        with torch.no_grad():
+            pats = mp.interpolate(qu_apply(truth[:, None, :], dc[None]), normalize_coords=False).reshape(
+                c["n"], *c["det"])
+            pats = pats + 0.01 * torch.randn_like(pats)
+        # starting orientations: the truth rotated by 1-2.5 degrees about random axes
+        ax = torch.randn((c["n"], 3))
+        ax = ax / ax.norm(dim=1, keepdim=True)
+        ang = torch.deg2rad(1.0 + 1.5 * torch.rand(c["n"]))
+        start = qu_prod(ax2qu(torch.cat((ax, ang[:, None]), dim=1)), truth)
+        exp = ExperimentPatterns(pats.clone())
+        exp.set_orientations(start.clone())
+        exp.phases = torch.zeros(c["n"], dtype=torch.int64)
+        spatial = None
+        if not c["avg"]:
+            spatial = 3.0 * torch.randn((c["n"], 2))
+            exp.set_spatial_coords(spatial.clone())
+        with contextlib.redirect_stdout(io.StringIO()):
+            dots = orientation_grid_refinement(
+                mp, geom, exp, grid_semi_edge_in_degrees=c["edge"], batch_size=5, virtual_binning=c["b"],
+                n_iter=c["n_iter"], axial_grid_dimension=c["axial"], kernel_radius_in_steps=c["radius"],
+                shrink_factor=c["shrink"], average_pattern_center=c["avg"], match_dtype=torch.float32)
+        out[f"case{ci}_master_pattern"] = mp_t.numpy()
+        out[f"case{ci}_patterns"] = pats.numpy()
+        out[f"case{ci}_truth"] = truth.numpy()
+        out[f"case{ci}_start"] = start.numpy()
+        out[f"case{ci}_spatial"] = spatial.numpy() if spatial is not None else np.zeros((0, 2), np.float32)
+        out[f"case{ci}_refined"] = exp.orientations.numpy()
+        out[f"case{ci}_dots"] = dots[0].numpy()
+        out[f"case{ci}_meta"] = np.array([*c["det"], c["b"], c["edge"], c["radius"], c["axial"], c["n_iter"],
+                                          c["shrink"], float(c["avg"])], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "refine.npz"), **out)
 
 
 def main(root: str = "/root/reference"):
@@ -273,4 +337,9 @@ def main(root: str = "/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    args = sys.argv[1:]
+    if args and args[0] == "--refinement-only":
+        refinement_goldens(*args[1:])
+    else:
+        main(*args)
+        refinement_goldens(*args)

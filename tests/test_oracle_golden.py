@@ -216,3 +216,63 @@ def test_symmetry_acts_on_the_left():
     g = O.laue_elements(11)[1]  # 180 deg about z: maps lattice points onto lattice points exactly
     assert np.abs(O.project_patterns(mp, rays, O._qmul(g, q)[None])[0] - base).max() < 1e-3
     assert np.abs(O.project_patterns(mp, rays, O._qmul(q, g)[None])[0] - base).max() > 0.1
+
+
+# ------------------------------------------------- orientation grid refinement
+
+
+def test_local_orientation_grid_matches_reference(golden):
+    g = golden("refine")
+    for i in range(4):
+        e, r, a = g[f"grid{i}_args"]
+        mine = O.local_orientation_grid(float(e), int(r), int(a))
+        assert mine.shape == g[f"grid{i}"].shape
+        assert np.abs(mine - g[f"grid{i}"]).max() < 1e-7
+
+
+def _refine_case(g, ci):
+    det0, det1, b, edge, radius, axial, n_iter, shrink, avg = g[f"case{ci}_meta"]
+    det, b = (int(det0), int(det1)), int(b)
+    mp = O.avg_pool(g[f"case{ci}_master_pattern"].astype(np.float64), b)
+    coords = O.detector_coords_sample_frame(det, (0.5, 0.5, 0.6), (0.0, 70.0, 0.0), binning=(b, b))
+    rows = O.prep_patterns(g[f"case{ci}_patterns"].astype(np.float64), b)
+    off = None if avg else g[f"case{ci}_spatial"].astype(np.float64)
+    if avg:
+        coords = O.unit_rays(coords)
+    return O.orientation_grid_refinement(mp, coords, rows, g[f"case{ci}_start"].astype(np.float64), 11, float(edge),
+                                         int(n_iter), int(axial), int(radius), float(shrink), offsets=off)
+
+
+@pytest.mark.parametrize("ci", [0, 1, 2])
+def test_refinement_oracle_matches_reference(golden, ci):
+    """The FP64 restatement of orientation_grid_refinement reproduces the
+    reference's refined orientations and per-iteration best dot products
+    (radius 1 and 2, full / biaxial / uniaxial grids, binning 2, per-pattern
+    source points; float32 reference)."""
+    g = golden("refine")
+    q, dots = _refine_case(g, ci)
+    ref = g[f"case{ci}_refined"].astype(np.float64)
+    err = np.minimum(np.abs(q - ref).max(1), np.abs(q + ref).max(1))
+    assert err.max() < 5e-5
+    ref_d = g[f"case{ci}_dots"]
+    assert np.abs(dots - ref_d).max() <= 2e-4 * np.abs(ref_d).max()
+
+
+def test_left_fz_reduction_keeps_the_pattern():
+    """The left reduction g q moves a rotation into the FZ without changing
+    its simulated pattern (up to interpolation on the Lambert grid); the
+    reference's right product q g changes it."""
+    from ebsdtorch_b200 import synthetic
+
+    rng = np.random.default_rng(3)
+    rays = O.unit_rays(O.detector_coords_sample_frame((12, 12), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0)))
+    q = rng.standard_normal((40, 4))
+    q = O.qu_std(q / np.linalg.norm(q, axis=1, keepdims=True))
+    # noise-free cubic bands: exactly m-3m symmetric
+    mp = synthetic.synthetic_master_pattern(257, seed=2, noise=0.0).numpy().astype(np.float64)
+    left = O.ori_to_fz_laue_left(q, 11)
+    right = O.ori_to_fz_laue_right(q, 11)
+    assert np.all(O.ori_in_fz_laue(left, 11))
+    p0 = O.project_patterns(mp, rays, q)
+    assert np.abs(O.project_patterns(mp, rays, left) - p0).max() < 0.05
+    assert np.abs(O.project_patterns(mp, rays, right) - p0).max() > 0.3
