@@ -82,7 +82,9 @@ __global__ void k_conv_c1(const __nv_bfloat16* __restrict__ x, int H, int W, int
       const int iy = 2 * oy - 1 + t / 3, ix = 2 * ox - 1 + t % 3;
       xv[t] = (iy >= 0 && iy < H && ix >= 0 && ix < W) ? __bfloat162float(x[((int64_t)b * H + iy) * W + ix]) : 0.f;
     }
-#pragma unroll
+    // one 8-channel group at a time: fully unrolled over all COUT channels
+    // the kernel needed 186 registers (one CTA per SM)
+#pragma unroll 1
     for (int c = 0; c < COUT; c += 8) {
       float o[8];
 #pragma unroll

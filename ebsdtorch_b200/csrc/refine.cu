@@ -10,7 +10,7 @@
 // and a pattern whose grid centre stayed best has its grid scaled by
 // shrink_factor.
 //
-// B200 design: one CTA per pattern runs all iterations; the experimental row
+// B200 design: one CTA (512 threads) per pattern runs all iterations; the experimental row
 // stays in shared memory, the candidate rotations are built in FP64 by the
 // first threads, and the candidates are simulated on the fly (no dictionary)
 // and scored 16 at a time per pass over the pixels, each thread carrying 16
@@ -30,7 +30,7 @@
 
 namespace ebsd {
 
-constexpr int kRefThreads = 256;
+constexpr int kRefThreads = 512;
 constexpr int kRefGroup = 16;      // candidates scored per pass over the pixels
 constexpr int kMaxRefGrid = 343;   // (2 * 3 + 1)^3
 constexpr int kMaxRefPix = 40960;  // FP32 pattern row in shared memory (160 KiB)
