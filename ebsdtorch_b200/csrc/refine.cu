@@ -10,9 +10,9 @@
 // and a pattern whose grid centre stayed best has its grid scaled by
 // shrink_factor.
 //
-// B200 design: one CTA (512 threads) per pattern runs all iterations; the experimental row
-// stays in shared memory, the candidate rotations are built in FP64 by the
-// first threads, and the candidates are simulated on the fly (no dictionary)
+// B200 design: one CTA (512 threads) per pattern runs all iterations; the
+// experimental row stays in shared memory, the candidate rotations are built
+// in FP64 by the first threads, and the candidates are simulated on the fly (no dictionary)
 // and scored 16 at a time per pass over the pixels, each thread carrying 16
 // (dot, sum) accumulators; the simulation mean is folded in as
 // dot - sum(sim) / P * sum(exp). Scores are FP32 (the reference uses
