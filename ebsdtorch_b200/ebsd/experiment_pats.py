@@ -17,6 +17,9 @@ from torch import Tensor
 from torch.nn import Module
 
 from .. import kernels
+from ..preprocessing import patterns as _pre
+from ..preprocessing.clahe import clahe_grayscale
+from ..preprocessing.nlpar import nlpar
 
 
 class ExperimentPatterns(Module):
@@ -85,6 +88,34 @@ class ExperimentPatterns(Module):
 
     def get_orientations(self, indices: Optional[Tensor] = None) -> Tensor:
         return self.orientations if indices is None else self.orientations[indices]
+
+    # ---- preprocessing (experiment_pats.py:223-316): GPU passes in FP32;
+    # integer or FP64 patterns become FP32, host patterns stay on the host
+
+    def subtract_overall_background(self) -> None:
+        """Subtract the scan's mean pattern from every pattern."""
+        self.patterns = _pre.subtract_overall_background(self.patterns)
+
+    def contrast_enhance_clahe(self, clip_limit: float = 40.0, tile_grid_size: int = 4, n_bins: int = 64) -> None:
+        """CLAHE of every pattern (clahe_grayscale)."""
+        self.patterns = clahe_grayscale(self.patterns, clip_limit=clip_limit, n_bins=n_bins,
+                                        grid_shape=(tile_grid_size, tile_grid_size))
+
+    def normalize_per_pattern(self, norm_type: str = "minmax") -> None:
+        """"minmax", "zeromean" or "standard" normalisation of every pattern."""
+        self.patterns = _pre.normalize_per_pattern(self.patterns, norm_type)
+
+    def standard_clean(self) -> None:
+        """Background subtraction, min-max, CLAHE, min-max, fused into one
+        pass over the patterns after the mean pattern."""
+        self.patterns = _pre.standard_clean(self.patterns)
+
+    def do_nlpar(self, k_rad: int = 3, coeff: float = 0.375) -> None:
+        """Non-local pattern averaging over the 2D scan."""
+        if len(self.spatial_shape) != 2:
+            raise ValueError(f"NLPAR only supported for 2D EBSD scans, got {self.spatial_shape}")
+        self.patterns = nlpar(self.patterns.view(tuple(self.spatial_shape) + tuple(self.pattern_shape)), k_rad=k_rad,
+                              coeff=coeff).view(-1, *self.pattern_shape)
 
     def get_patterns(self, indices: Tensor, binning: int):
         """Patterns at `indices`, b x b average pooled (experiment_pats.py:318-346)."""

@@ -281,6 +281,47 @@ int ebsd_refine_grid(const float* master_pattern, int mp_h, int mp_w2, const flo
                      const float* grid_cu, int n_grid, int laue_id, int fz_left, int n_iter, float shrink,
                      float* q_out, float* dots, void* stream);
 
+/* ---- experimental-pattern preprocessing --------------------------------------
+ * FP32 patterns as n rows of n_pix pixels (row stride ld). */
+
+/* mean[c] = mean over the n rows of column c (FP64 sums: partial holds
+ * n_splits x n_pix doubles). With ebsd_subtract_pattern this replaces
+ * ExperimentPatterns.subtract_overall_background (experiment_pats.py:223-232). */
+int ebsd_pattern_mean(const float* patterns, int64_t n, int n_pix, int64_t ld, double* partial, int n_splits,
+                      float* mean, void* stream);
+/* patterns[r, c] -= v[c] in place. */
+int ebsd_subtract_pattern(float* patterns, int64_t n, int n_pix, int64_t ld, const float* v, void* stream);
+/* ExperimentPatterns.normalize_per_pattern (experiment_pats.py:255-285), in
+ * place: mode 0 "minmax" (x - min) / (1e-4 + max - min), 1 "zeromean", 2
+ * "standard" (zero mean, divided by the unbiased standard deviation). */
+int ebsd_normalize_patterns(float* patterns, int64_t n, int n_pix, int64_t ld, int mode, void* stream);
+/* clahe_grayscale (preprocessing/clahe.py:17-130) on n images of height x
+ * width (row stride ld, written to out with stride ld_out; in place allowed
+ * when ld == ld_out): clip_limit, n_bins and the grid_h x grid_w tile grid as
+ * the reference takes them. Fused extras for standard_clean
+ * (experiment_pats.py:287-297): subtract (n_pix, or NULL) is subtracted and
+ * minmax_in applies the min-max normalisation before the equalisation,
+ * minmax_out after it. grid_h * grid_w * n_bins * 8 bytes of tables must fit
+ * in 220 KiB of shared memory; images that fit beside them are staged there
+ * (one read, one write per pixel). */
+int ebsd_clahe(const float* images, int64_t n, int height, int width, int64_t ld, const float* subtract,
+               int minmax_in, float clip_limit, int n_bins, int grid_h, int grid_w, int minmax_out, float* out,
+               int64_t ld_out, void* stream);
+/* NLPAR window passes (nlpar.py:94-121 and 185-191) over a scan_h x scan_w
+ * scan of patterns (row (y * scan_w + x), stride ld; zero outside the scan).
+ * offsets (n_off_total x 2 int32, device) are the window offsets (di, dj),
+ * |di|, |dj| <= k_rad <= 7, in the reference's order; one call covers offsets
+ * o0 .. o0 + n_off - 1 (n_off <= 128). ebsd_nlpar_dists writes
+ * dists[pt, o] = sum_p (x[pt + off_o, p] - x[pt, p])^2 (scan_h * scan_w x
+ * n_off_total); ebsd_nlpar_average writes (accumulate 0) or adds
+ * (accumulate 1) out[pt, p] = sum_o weights[pt, o] x[pt + off_o, p]. An
+ * offset outside the window yields NaN. */
+int ebsd_nlpar_dists(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
+                     const int* offsets, int o0, int n_off, int n_off_total, float* dists, void* stream);
+int ebsd_nlpar_average(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
+                       const int* offsets, int o0, int n_off, int n_off_total, const float* weights, int accumulate,
+                       float* out, int64_t ld_out, void* stream);
+
 /* ---- local dictionary search around orientation proposals --------------------
  * No counterpart in the reference (search step of the learned-proposal path).
  * cell_to_row (edge^3 int32): dictionary row of each cubochoric grid cell or

@@ -1004,3 +1004,154 @@ def orientation_grid_refinement(master_pattern: np.ndarray, coords: np.ndarray, 
         q = qa[np.arange(n), best_i]
         scale = np.where(best_i == centre, scale * shrink, scale)
     return q, dots
+
+
+# --------------------------------------------------------------------------
+# Pattern preprocessing (experiment_pats.py:223-316, preprocessing/)
+# --------------------------------------------------------------------------
+
+
+def subtract_overall_background(pats: np.ndarray) -> np.ndarray:
+    """Subtract the mean pattern of the scan (experiment_pats.py:223-232)."""
+    return pats - pats.mean(axis=0, keepdims=True)
+
+
+def normalize_per_pattern(pats: np.ndarray, norm_type: str = "minmax") -> np.ndarray:
+    """Per-pattern normalisation (experiment_pats.py:255-285); 'standard'
+    divides by the unbiased standard deviation, as torch.std does."""
+    x = pats.reshape(pats.shape[0], -1)
+    if norm_type == "minmax":
+        mn, mx = x.min(axis=1, keepdims=True), x.max(axis=1, keepdims=True)
+        x = (x - mn) / (1e-4 + mx - mn)
+    elif norm_type == "zeromean":
+        x = x - x.mean(axis=1, keepdims=True)
+    elif norm_type == "standard":
+        x = x - x.mean(axis=1, keepdims=True)
+        x = x / x.std(axis=1, ddof=1, keepdims=True)
+    else:
+        raise ValueError(norm_type)
+    return x.reshape(pats.shape)
+
+
+def clahe(x: np.ndarray, clip_limit: float = 40.0, n_bins: int = 64, grid=(4, 4)) -> np.ndarray:
+    """Contrast-limited adaptive histogram equalisation of (B, H, W) images
+    in [0, 1] (preprocessing/clahe.py:17-130): per tile (the image reflect-
+    padded on the bottom/right to a multiple of the grid) a histogram of
+    floor(x (n_bins - 1)), clipped at max(clip_limit tile_px // n_bins, 1)
+    with the excess spread evenly and the remainder one count to each of the
+    first bins, cumulated into a CDF; each pixel is then read from the
+    (tile-y, tile-x, bin) CDF volume by trilinear interpolation with
+    align_corners=False / border semantics (grid_sample)."""
+    B, H, W = x.shape
+    gh, gw = grid
+    th, tw = math.ceil(H / gh), math.ceil(W / gw)
+    vpt = th * tw
+    ph = gh - H % gh if H % gh else 0
+    pw = gw - W % gw if W % gw else 0
+    xp = np.pad(x, ((0, 0), (0, ph), (0, pw)), mode="reflect")
+    cdfs = np.zeros((B, gh, gw, n_bins))
+    for ty in range(gh):
+        for tx in range(gw):
+            tile = xp[:, ty * th:(ty + 1) * th, tx * tw:(tx + 1) * tw].reshape(B, -1)
+            idx = (tile.astype(np.float32) * np.float32(n_bins - 1)).astype(np.int64)
+            hist = np.stack([np.bincount(r, minlength=n_bins)[:n_bins] for r in idx]).astype(np.float64)
+            hist = hist / hist.sum(axis=1, keepdims=True) * vpt
+            if clip_limit > 0:
+                limit = max(clip_limit * vpt // n_bins, 1)
+                hist = np.minimum(hist, limit)
+                clipped = vpt - hist.sum(axis=1)
+                residual = np.remainder(clipped, n_bins)
+                hist = hist + ((clipped - residual) / n_bins)[:, None]
+                hist = hist + (np.arange(n_bins)[None] < residual[:, None])
+            cdfs[:, ty, tx] = np.clip(np.cumsum(hist, axis=1) / vpt, 0.0, 1.0)
+
+    def coord(c, size):
+        return np.clip(((c + 1.0) * size - 1.0) / 2.0, 0.0, size - 1.0)
+
+    fb = coord(x * 2.0 - 1.0, n_bins)                        # (B, H, W)
+    fx = coord(np.linspace(-1.0, 1.0, W, dtype=np.float32).astype(np.float64), gw)  # (W,)
+    fy = coord(np.linspace(-1.0, 1.0, H, dtype=np.float32).astype(np.float64), gh)  # (H,)
+    b0 = np.floor(fb).astype(np.int64)
+    x0 = np.floor(fx).astype(np.int64)
+    y0 = np.floor(fy).astype(np.int64)
+    b1, x1, y1 = np.minimum(b0 + 1, n_bins - 1), np.minimum(x0 + 1, gw - 1), np.minimum(y0 + 1, gh - 1)
+    wb, wx, wy = fb - b0, (fx - x0)[None, None, :], (fy - y0)[None, :, None]
+    bi = np.arange(B)[:, None, None]
+    yy0, yy1 = y0[None, :, None], y1[None, :, None]
+    xx0, xx1 = x0[None, None, :], x1[None, None, :]
+    out = 0.0
+    for yv, wyv in ((yy0, 1 - wy), (yy1, wy)):
+        for xv, wxv in ((xx0, 1 - wx), (xx1, wx)):
+            for bv, wbv in ((b0, 1 - wb), (b1, wb)):
+                out = out + cdfs[bi, yv, xv, bv] * wyv * wxv * wbv
+    return out
+
+
+def standard_clean(pats: np.ndarray) -> np.ndarray:
+    """Background, min-max, CLAHE, min-max (experiment_pats.py:287-297)."""
+    x = normalize_per_pattern(subtract_overall_background(pats), "minmax")
+    return normalize_per_pattern(clahe(x), "minmax")
+
+
+def nlpar_offsets(k_rad: int):
+    """Window offsets in the reference's order (nlpar.py:77-91): sorted by
+    L1 norm with torch.argsort, whose order among equal norms is the one the
+    reference gets (it decides which 8 offsets estimate the noise)."""
+    import torch
+
+    oc = torch.stack(torch.meshgrid(torch.arange(-k_rad, k_rad + 1), torch.arange(-k_rad, k_rad + 1),
+                                    indexing="ij"), dim=-1).reshape(-1, 2)
+    return oc[torch.argsort(torch.sum(torch.abs(oc), dim=-1))].numpy()
+
+
+def nlpar(data: np.ndarray, k_rad: int = 5, coeff: float = 0.375, coeff_fit_tol: float = 1e-6,
+          center_logit_bias: float = 0.0) -> np.ndarray:
+    """Non-local pattern averaging of a (h, w, H, W) scan (nlpar.py:19-192,
+    Brewick et al. 2019), float64."""
+    hs, ws = data.shape[:2]
+    P = data.shape[2] * data.shape[3]
+    off = nlpar_offsets(k_rad)
+    K = off.shape[0]
+    flat = data.reshape(hs, ws, P).astype(np.float64)
+    pad = np.zeros((hs + 2 * k_rad, ws + 2 * k_rad, P))
+    pad[k_rad:k_rad + hs, k_rad:k_rad + ws] = flat
+    oob = np.ones((hs + 2 * k_rad, ws + 2 * k_rad), dtype=bool)
+    oob[k_rad:k_rad + hs, k_rad:k_rad + ws] = False
+    dists = np.empty((hs, ws, K))
+    mask = np.empty((hs, ws, K), dtype=bool)
+    for i, (di, dj) in enumerate(off):
+        nb = pad[k_rad + di:k_rad + di + hs, k_rad + dj:k_rad + dj + ws]
+        dists[:, :, i] = ((nb - flat) ** 2).sum(-1)
+        mask[:, :, i] = oob[k_rad + di:k_rad + di + hs, k_rad + dj:k_rad + dj + ws]
+    sigma = np.sqrt(dists[:, :, 1:9].min(-1) / (2 * P))
+    sp = np.ones((hs + 2 * k_rad, ws + 2 * k_rad))
+    sp[k_rad:k_rad + hs, k_rad:k_rad + ws] = sigma
+    for i, (di, dj) in enumerate(off):
+        so = sp[k_rad + di:k_rad + di + hs, k_rad + dj:k_rad + dj + ws]
+        s2 = sigma ** 2 + so ** 2
+        dists[:, :, i] = (dists[:, :, i] - P * s2) / (2 ** 0.5 * P ** 0.5 * s2)
+    weights = -np.maximum(dists, 0.0)
+    g = 1.0
+    nn = weights[:, :, :9]
+    # on degenerate scans (most of the window outside) the fit runs away, as
+    # the reference's does; the large coefficient then flattens the weights
+    with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+        for _ in range(10):
+            g2 = g ** 2
+            e = np.exp(nn / g2)
+            obj = np.mean(e[:, :, 0] / e.sum(-1)) - coeff
+            grad = np.mean(-2 * np.exp(nn[:, :, 0] / g2) * ((nn[:, :, :1] * e).sum(-1) - (nn * e).sum(-1))
+                           / (g ** 3 * e.sum(-1) ** 2))
+            g -= obj / grad
+            if abs(obj) < coeff_fit_tol:
+                break
+    weights = weights / g ** 2
+    if center_logit_bias > 0:
+        weights[:, :, 0] += center_logit_bias
+    weights = np.where(mask, -np.inf, weights)
+    weights = np.exp(weights - weights.max(-1, keepdims=True))
+    weights /= weights.sum(-1, keepdims=True)
+    out = np.zeros_like(flat)
+    for i, (di, dj) in enumerate(off):
+        out += pad[k_rad + di:k_rad + di + hs, k_rad + dj:k_rad + dj + ws] * weights[:, :, i:i + 1]
+    return out.reshape(data.shape)

@@ -12,7 +12,8 @@ modified. The PCA variant is also loaded with line 355's component slice
 ``[:, -n : -n + 300]`` replaced by ``[:, -n:]`` (the "top" slice).
 
 Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
-outputs of one case (``--refinement-only`` writes just refine.npz). The files are small (< 1 MB each) and committed.
+outputs of one case (``--refinement-only`` / ``--preprocessing-only`` write
+just refine.npz / preprocess.npz). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -119,6 +120,53 @@ def refinement_goldens(root: str = "/root/reference"):
         out[f"case{ci}_meta"] = np.array([*c["det"], c["b"], c["edge"], c["radius"], c["axial"], c["n_iter"],
                                           c["shrink"], float(c["avg"])], dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, "refine.npz"), **out)
+
+
+def preprocessing_goldens(root: str = "/root/reference"):
+    """Pattern preprocessing (experiment_pats.py:223-316, preprocessing/
+    clahe.py, nlpar.py): overall background, per-pattern normalisation,
+    CLAHE (divisible and reflect-padded sizes), standard_clean, NLPAR."""
+    sys.path.insert(0, root)
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.preprocessing.clahe import clahe_grayscale
+    from ebsdtorch.preprocessing.nlpar import nlpar
+
+    out = {}
+    g = torch.Generator().manual_seed(71)
+    base = torch.rand((1, 1, 12, 12), generator=g)
+    img = torch.nn.functional.interpolate(base, size=(40, 36), mode="bicubic", align_corners=True)[0, 0]
+    pats = (img[None] * 200 + 40 * torch.rand((11, 40, 36), generator=g)).float()
+    out["pats"] = pats.numpy()
+    e = ExperimentPatterns(pats.clone())
+    e.subtract_overall_background()
+    out["background"] = e.patterns.numpy()
+    for mode in ("minmax", "zeromean", "standard"):
+        e = ExperimentPatterns(pats.clone())
+        e.normalize_per_pattern(norm_type=mode)
+        out[f"norm_{mode}"] = e.patterns.numpy()
+    unit = pats - pats.amin(dim=(1, 2), keepdim=True)
+    unit = unit / unit.amax(dim=(1, 2), keepdim=True)
+    out["unit"] = unit.numpy()
+    for name, (clip, bins, grid) in {"clahe_a": (40.0, 64, (4, 4)), "clahe_b": (2.0, 32, (3, 5)),
+                                     "clahe_c": (0.0, 16, (2, 2))}.items():
+        out[name] = clahe_grayscale(unit[:, None].clone(), clip_limit=clip, n_bins=bins, grid_shape=grid)[:, 0].numpy()
+        out[name + "_args"] = np.array([clip, bins, *grid], dtype=np.float64)
+    e = ExperimentPatterns(pats.clone())
+    e.standard_clean()
+    out["standard_clean"] = e.patterns.numpy()
+    # NLPAR on a 7 x 9 scan of 16 x 12 patterns: smooth grains plus noise
+    scan = torch.zeros((7, 9, 16, 12))
+    for k, (a, b) in enumerate(((0, 4), (4, 9))):
+        bp = torch.nn.functional.interpolate(torch.rand((1, 1, 5, 5), generator=g), size=(16, 12), mode="bicubic",
+                                             align_corners=True)[0, 0]
+        scan[:, a:b] = bp * 100
+    scan[3:, 2:6] += 30
+    scan = scan + 8 * torch.randn(scan.shape, generator=g)
+    out["nlpar_in"] = scan.numpy()
+    for name, (k, c) in {"nlpar_a": (1, 0.375), "nlpar_b": (3, 0.5)}.items():
+        out[name] = nlpar(scan.clone(), k_rad=k, coeff=c).numpy()
+        out[name + "_args"] = np.array([k, c], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "preprocess.npz"), **out)
 
 
 def main(root: str = "/root/reference"):
@@ -340,6 +388,9 @@ if __name__ == "__main__":
     args = sys.argv[1:]
     if args and args[0] == "--refinement-only":
         refinement_goldens(*args[1:])
+    elif args and args[0] == "--preprocessing-only":
+        preprocessing_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
+        preprocessing_goldens(*args)

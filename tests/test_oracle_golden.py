@@ -276,3 +276,60 @@ def test_left_fz_reduction_keeps_the_pattern():
     p0 = O.project_patterns(mp, rays, q)
     assert np.abs(O.project_patterns(mp, rays, left) - p0).max() < 0.05
     assert np.abs(O.project_patterns(mp, rays, right) - p0).max() > 0.3
+
+
+# ---- experimental-pattern preprocessing -----------------------------------
+
+
+def _rel(a, b):
+    return float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def test_background_and_normalisation_oracle_match_reference(golden):
+    """subtract_overall_background and the three normalize_per_pattern modes
+    (experiment_pats.py:223-285) on 11 patterns of 40 x 36."""
+    g = golden("preprocess")
+    pats = g["pats"].astype(np.float64)
+    assert _rel(O.subtract_overall_background(pats), g["background"]) < 1e-5
+    for mode, tol in (("minmax", 1e-6), ("zeromean", 1e-5), ("standard", 1e-5)):
+        assert _rel(O.normalize_per_pattern(pats, mode), g[f"norm_{mode}"]) < tol, mode
+
+
+@pytest.mark.parametrize("name", ["clahe_a", "clahe_b", "clahe_c"])
+def test_clahe_oracle_matches_reference(golden, name):
+    """clahe_grayscale (clahe.py:17-130): clip 40 / 64 bins / 4 x 4 grid
+    (reflect padding on both axes), clip 2 / 32 bins / 3 x 5 grid, and no
+    clipping / 16 bins / 2 x 2 grid."""
+    g = golden("preprocess")
+    clip, bins, gh, gw = g[name + "_args"]
+    out = O.clahe(g["unit"].astype(np.float64), float(clip), int(bins), (int(gh), int(gw)))
+    assert np.abs(out - g[name]).max() < 1e-5
+
+
+def test_standard_clean_oracle_matches_reference(golden):
+    g = golden("preprocess")
+    assert np.abs(O.standard_clean(g["pats"].astype(np.float64)) - g["standard_clean"]).max() < 1e-5
+
+
+@pytest.mark.parametrize("name", ["nlpar_a", "nlpar_b"])
+def test_nlpar_oracle_matches_reference(golden, name):
+    """nlpar (nlpar.py:19-192) on a 7 x 9 scan of 16 x 12 patterns with
+    k_rad 1 / coeff 0.375 and k_rad 3 / coeff 0.5."""
+    g = golden("preprocess")
+    k, c = g[name + "_args"]
+    out = O.nlpar(g["nlpar_in"].astype(np.float64), int(k), float(c))
+    assert _rel(out, g[name]) < 1e-6
+
+
+def test_nlpar_offsets_order():
+    """Offsets sorted by L1 norm: 0 is the point itself, 1..4 its axial
+    neighbours, 5..8 four of the L1-norm-2 offsets (diagonals or axial at
+    distance 2, as torch.argsort breaks the ties), which feed the noise
+    estimate and the coefficient fit."""
+    for k in (1, 3, 5, 7):
+        off = O.nlpar_offsets(k)
+        l1 = np.abs(off).sum(1)
+        assert off.shape == ((2 * k + 1) ** 2, 2)
+        assert l1[0] == 0 and (l1[1:5] == 1).all() and (l1[5:9] == 2).all()
+        assert (l1[:-1] <= l1[1:]).all()
+        assert len({tuple(o) for o in off}) == off.shape[0]
