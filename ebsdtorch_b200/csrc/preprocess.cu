@@ -54,41 +54,92 @@ __global__ void k_sub_vector(float* __restrict__ X, int64_t n, int n_cols, int64
 
 constexpr int kNormThreads = 256;
 
+__device__ __forceinline__ void cp_async4(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float* dst, const float* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // mode 0 min-max: (x - min) / ((1e-4 + max) - min); 1 zero mean; 2 zero mean
-// and unit unbiased standard deviation (torch.std). One CTA per pattern.
+// and unit unbiased standard deviation (torch.std). One CTA per pattern; with
+// PER > 0 a row of up to PER * 256 values is held in registers (one read, one
+// write), otherwise it is re-read from global memory (L2) per pass.
+template <int PER>
 __global__ void __launch_bounds__(kNormThreads) k_normalize(float* __restrict__ X, int64_t n, int n_cols,
                                                            int64_t ld, int mode) {
   __shared__ float fred[32];
   __shared__ double dred[32];
+  constexpr int R = PER > 0 ? PER : 1;
+  float v[R];
   for (int64_t r = blockIdx.x; r < n; r += gridDim.x) {
     float* row = X + r * ld;
+    auto at = [&](int k, int c) -> float {
+      if constexpr (PER > 0) {
+        return v[k];
+      } else {
+        return row[c];
+      }
+    };
+    if constexpr (PER > 0) {
+#pragma unroll
+      for (int k = 0; k < PER; ++k) {
+        const int c = threadIdx.x + k * kNormThreads;
+        v[k] = c < n_cols ? row[c] : 0.f;
+      }
+    }
     if (mode == 0) {
       float mn = INFINITY, mx = -INFINITY;
-      for (int c = threadIdx.x; c < n_cols; c += blockDim.x) {
-        mn = fminf(mn, row[c]);
-        mx = fmaxf(mx, row[c]);
-      }
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        for (int c = threadIdx.x + k * kNormThreads; c < n_cols; c += R * kNormThreads) {
+          const float x = at(k, c);
+          mn = fminf(mn, x);
+          mx = fmaxf(mx, x);
+          if constexpr (PER > 0) break;
+        }
       mx = block_max(mx, fred);
       mn = -block_max(-mn, fred);
       const float den = (1e-4f + mx) - mn;
-      for (int c = threadIdx.x; c < n_cols; c += blockDim.x) row[c] = (row[c] - mn) / den;
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        for (int c = threadIdx.x + k * kNormThreads; c < n_cols; c += R * kNormThreads) {
+          row[c] = (at(k, c) - mn) / den;
+          if constexpr (PER > 0) break;
+        }
     } else {
       double s = 0.0;
-      for (int c = threadIdx.x; c < n_cols; c += blockDim.x) s += row[c];
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        for (int c = threadIdx.x + k * kNormThreads; c < n_cols; c += R * kNormThreads) {
+          s += at(k, c);
+          if constexpr (PER > 0) break;
+        }
       const float mean = (float)(block_sum(s, dred) / n_cols);
       float sd = 1.0f;
       if (mode == 2) {
         double ss = 0.0;
-        for (int c = threadIdx.x; c < n_cols; c += blockDim.x) {
-          const double d = (double)(row[c] - mean);
-          ss += d * d;
-        }
+#pragma unroll
+        for (int k = 0; k < R; ++k)
+          for (int c = threadIdx.x + k * kNormThreads; c < n_cols; c += R * kNormThreads) {
+            const double d = (double)(at(k, c) - mean);
+            ss += d * d;
+            if constexpr (PER > 0) break;
+          }
         sd = (float)sqrt(block_sum(ss, dred) / (double)(n_cols - 1));
       }
-      for (int c = threadIdx.x; c < n_cols; c += blockDim.x) {
-        const float v = row[c] - mean;
-        row[c] = mode == 2 ? v / sd : v;
-      }
+#pragma unroll
+      for (int k = 0; k < R; ++k)
+        for (int c = threadIdx.x + k * kNormThreads; c < n_cols; c += R * kNormThreads) {
+          const float x = at(k, c) - mean;
+          row[c] = mode == 2 ? x / sd : x;
+          if constexpr (PER > 0) break;
+        }
     }
     __syncthreads();
   }
@@ -97,8 +148,10 @@ __global__ void __launch_bounds__(kNormThreads) k_normalize(float* __restrict__ 
 // --------------------------------------------------------------------- CLAHE
 
 constexpr int kClaheThreads = 256;
-// dynamic shared memory of one CTA: the CDF and histogram tables, plus the
-// image when it fits (then global memory is read once and written once)
+// dynamic shared memory of one CTA: the CDF and histogram tables, the
+// coordinate tables, plus two image buffers when they fit (then each image
+// is read once, prefetched while the previous one is equalised, and written
+// once)
 constexpr size_t kClaheSmemCap = 220 * 1024;
 
 __device__ __forceinline__ int reflect_index(int i, int n) { return i < n ? i : 2 * (n - 1) - i; }
@@ -118,8 +171,41 @@ struct ClaheArgs {
   int minmax_in, minmax_out;
   float limit;
   int clip, nb, gh, gw;
+  int vec16;  // rows 16-byte aligned with H * W % 4 == 0: 16-byte async copies
   float* out;
   int64_t ld_out;
+};
+
+// Shared-memory layout of k_clahe (bytes), shared with the host.
+struct ClaheLayout {
+  size_t cdf, hist, colsrc, coltile, rowsrc, rowtile, colx, colw, rowy, roww, img, total_tables;
+  __host__ __device__ ClaheLayout(int H, int W, int gh, int gw, int nb) {
+    const int th = (H + gh - 1) / gh, tw = (W + gw - 1) / gw;
+    const int hp = gh * th, wp = gw * tw;
+    size_t o = 0;
+    cdf = o;
+    o += (size_t)gh * gw * nb * 4;
+    hist = o;
+    o += (size_t)gh * gw * nb * 4;
+    colsrc = o;
+    o += (size_t)wp * 4;
+    coltile = o;
+    o += (size_t)wp * 4;
+    rowsrc = o;
+    o += (size_t)hp * 4;
+    rowtile = o;
+    o += (size_t)hp * 4;
+    colx = o;
+    o += (size_t)W * 4;
+    colw = o;
+    o += (size_t)W * 4;
+    rowy = o;
+    o += (size_t)H * 4;
+    roww = o;
+    o += (size_t)H * 4;
+    img = (o + 15) / 16 * 16;
+    total_tables = img;
+  }
 };
 
 // One CTA per image. Optional pre-pass (x - sub, then min-max); tile
@@ -128,28 +214,84 @@ struct ClaheArgs {
 // the remainder one count to each of the first bins, cumulate into a CDF;
 // then each pixel reads the (tile-y, tile-x, bin) CDF volume by trilinear
 // interpolation with grid_sample's align_corners=False / border rules;
-// optional post min-max. STAGED keeps the image in shared memory so global
-// memory is read once and written once.
+// optional post min-max. STAGED keeps the image in shared memory, the next
+// image arriving by cp.async while this one is processed; otherwise every
+// pass reads global memory (L2).
 template <bool STAGED>
 __global__ void __launch_bounds__(kClaheThreads) k_clahe(const ClaheArgs a) {
-  extern __shared__ __align__(16) float sm[];
+  extern __shared__ __align__(16) uint8_t smraw[];
   __shared__ float red[32];
   const int n_tiles = a.gh * a.gw, nb = a.nb, H = a.H, W = a.W, P = H * W;
-  float* cdf = sm;                                               // n_tiles * nb
-  int* hist = reinterpret_cast<int*>(cdf + n_tiles * nb);        // n_tiles * nb
-  float* img_s = reinterpret_cast<float*>(hist + n_tiles * nb);  // P (STAGED)
+  const ClaheLayout L(H, W, a.gh, a.gw, nb);
+  float* cdf = reinterpret_cast<float*>(smraw + L.cdf);
+  int* hist = reinterpret_cast<int*>(smraw + L.hist);
+  int* colsrc = reinterpret_cast<int*>(smraw + L.colsrc);
+  int* coltile = reinterpret_cast<int*>(smraw + L.coltile);
+  int* rowsrc = reinterpret_cast<int*>(smraw + L.rowsrc);
+  int* rowtile = reinterpret_cast<int*>(smraw + L.rowtile);
+  int* colx = reinterpret_cast<int*>(smraw + L.colx);
+  float* colw = reinterpret_cast<float*>(smraw + L.colw);
+  int* rowy = reinterpret_cast<int*>(smraw + L.rowy);
+  float* roww = reinterpret_cast<float*>(smraw + L.roww);
+  float* img_s = reinterpret_cast<float*>(smraw + L.img);  // 2 x P (STAGED)
   const int th = (H + a.gh - 1) / a.gh, tw = (W + a.gw - 1) / a.gw;
-  const int vpt = th * tw;
+  const int hp = a.gh * th, wp = a.gw * tw, vpt = th * tw;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
-  for (int64_t r = blockIdx.x; r < a.n; r += gridDim.x) {
+
+  // coordinate tables: padded pixel -> source pixel and tile; output pixel
+  // -> lower CDF cell and weight (torch.linspace(-1, 1, n) grids unnormalised
+  // with align_corners=False, clamped at the border)
+  for (int x = threadIdx.x; x < wp; x += blockDim.x) {
+    colsrc[x] = reflect_index(x, W);
+    coltile[x] = x / tw;
+  }
+  for (int y = threadIdx.x; y < hp; y += blockDim.x) {
+    rowsrc[y] = reflect_index(y, H) * W;
+    rowtile[y] = (y / th) * a.gw;
+  }
+  for (int x = threadIdx.x; x < W; x += blockDim.x) {
+    const float c = -1.0f + 2.0f * (float)x / (float)(W - 1);
+    const float f = fminf(fmaxf(((c + 1.0f) * a.gw - 1.0f) / 2.0f, 0.0f), (float)(a.gw - 1));
+    colx[x] = (int)f;
+    colw[x] = f - (int)f;
+  }
+  for (int y = threadIdx.x; y < H; y += blockDim.x) {
+    const float c = -1.0f + 2.0f * (float)y / (float)(H - 1);
+    const float f = fminf(fmaxf(((c + 1.0f) * a.gh - 1.0f) / 2.0f, 0.0f), (float)(a.gh - 1));
+    rowy[y] = (int)f;
+    roww[y] = f - (int)f;
+  }
+
+  auto prefetch = [&](int64_t r, float* buf) {
+    const float* src = a.X + r * a.ld;
+    if (a.vec16) {
+      for (int t = threadIdx.x; t < P / 4; t += blockDim.x) cp_async16(buf + 4 * t, src + 4 * t);
+    } else {
+      for (int t = threadIdx.x; t < P; t += blockDim.x) cp_async4(buf + t, src + t);
+    }
+  };
+  if constexpr (STAGED) {
+    if (blockIdx.x < a.n) prefetch(blockIdx.x, img_s);
+    cp_async_commit();
+  }
+  int it = 0;
+  for (int64_t r = blockIdx.x; r < a.n; r += gridDim.x, ++it) {
     const float* img = a.X + r * a.ld;
     float* dst = a.out + r * a.ld_out;
-    // pre-pass: x - sub, min / max
+    float* buf = img_s + (it & 1) * P;
+    if constexpr (STAGED) {
+      if (r + gridDim.x < a.n) prefetch(r + gridDim.x, img_s + ((it + 1) & 1) * P);
+      cp_async_commit();
+      cp_async_wait<1>();
+    }
+    for (int t = threadIdx.x; t < n_tiles * nb; t += blockDim.x) hist[t] = 0;
+    __syncthreads();
+    // pre-pass: x - sub, min / max (in place in shared memory when staged)
     float mn = INFINITY, mx = -INFINITY;
     for (int t = threadIdx.x; t < P; t += blockDim.x) {
-      float v = img[t];
+      float v = STAGED ? buf[t] : img[t];
       if (a.sub) v -= __ldg(a.sub + t);
-      if constexpr (STAGED) img_s[t] = v;
+      if constexpr (STAGED) buf[t] = v;
       mn = fminf(mn, v);
       mx = fmaxf(mx, v);
     }
@@ -158,26 +300,27 @@ __global__ void __launch_bounds__(kClaheThreads) k_clahe(const ClaheArgs a) {
       const float2 m = block_minmax(mn, mx, red);
       in_mn = m.x;
       in_den = (1e-4f + m.y) - m.x;
+      if constexpr (STAGED)
+        for (int t = threadIdx.x; t < P; t += blockDim.x) buf[t] = (buf[t] - in_mn) / in_den;
     }
+    __syncthreads();
     // the value CLAHE sees at pixel t
     auto value = [&](int t) -> float {
-      float v;
       if constexpr (STAGED) {
-        v = img_s[t];
+        return buf[t];
       } else {
-        v = img[t];
+        float v = img[t];
         if (a.sub) v -= __ldg(a.sub + t);
+        return a.minmax_in ? (v - in_mn) / in_den : v;
       }
-      return a.minmax_in ? (v - in_mn) / in_den : v;
     };
-    for (int t = threadIdx.x; t < n_tiles * nb; t += blockDim.x) hist[t] = 0;
-    __syncthreads();
-    const int hp = a.gh * th, wp = a.gw * tw;
-    for (int t = threadIdx.x; t < hp * wp; t += blockDim.x) {
-      const int y = t / wp, x = t - y * wp;
-      const float v = value(reflect_index(y, H) * W + reflect_index(x, W));
-      const int b = min(max((int)(v * (float)(nb - 1)), 0), nb - 1);
-      atomicAdd(&hist[((y / th) * a.gw + x / tw) * nb + b], 1);
+    for (int y = wid; y < hp; y += n_warps) {
+      const int src = rowsrc[y], tile_row = rowtile[y];
+      for (int x = lane; x < wp; x += 32) {
+        const float v = value(src + colsrc[x]);
+        const int b = min(max((int)(v * (float)(nb - 1)), 0), nb - 1);
+        atomicAdd(&hist[(tile_row + coltile[x]) * nb + b], 1);
+      }
     }
     __syncthreads();
     for (int tile = wid; tile < n_tiles; tile += n_warps) {
@@ -220,56 +363,44 @@ __global__ void __launch_bounds__(kClaheThreads) k_clahe(const ClaheArgs a) {
     __syncthreads();
     mn = INFINITY;
     mx = -INFINITY;
-    for (int t = threadIdx.x; t < P; t += blockDim.x) {
-      const int y = t / W, x = t - y * W;
-      const float v = value(t);
-      // grid_sample coordinates: value -> bins, image x -> tile columns,
-      // image y -> tile rows (torch.linspace(-1, 1, n) grids)
-      const float cx = -1.0f + 2.0f * (float)x / (float)(W - 1);
-      const float cy = -1.0f + 2.0f * (float)y / (float)(H - 1);
-      float fb = ((v * 2.0f - 1.0f + 1.0f) * nb - 1.0f) / 2.0f;
-      float fx = ((cx + 1.0f) * a.gw - 1.0f) / 2.0f;
-      float fy = ((cy + 1.0f) * a.gh - 1.0f) / 2.0f;
-      fb = fminf(fmaxf(fb, 0.0f), (float)(nb - 1));
-      fx = fminf(fmaxf(fx, 0.0f), (float)(a.gw - 1));
-      fy = fminf(fmaxf(fy, 0.0f), (float)(a.gh - 1));
-      const int b0 = (int)fb, x0 = (int)fx, y0 = (int)fy;
-      const int b1 = min(b0 + 1, nb - 1), x1 = min(x0 + 1, a.gw - 1), y1 = min(y0 + 1, a.gh - 1);
-      const float wb = fb - b0, wx = fx - x0, wy = fy - y0;
-      const float* c00 = cdf + (y0 * a.gw + x0) * nb;
-      const float* c01 = cdf + (y0 * a.gw + x1) * nb;
-      const float* c10 = cdf + (y1 * a.gw + x0) * nb;
-      const float* c11 = cdf + (y1 * a.gw + x1) * nb;
-      const float v00 = c00[b0] * (1.f - wb) + c00[b1] * wb;
-      const float v01 = c01[b0] * (1.f - wb) + c01[b1] * wb;
-      const float v10 = c10[b0] * (1.f - wb) + c10[b1] * wb;
-      const float v11 = c11[b0] * (1.f - wb) + c11[b1] * wb;
-      const float o = (v00 * (1.f - wx) + v01 * wx) * (1.f - wy) + (v10 * (1.f - wx) + v11 * wx) * wy;
-      mn = fminf(mn, o);
-      mx = fmaxf(mx, o);
-      if constexpr (STAGED) {
-        if (a.minmax_out) {
-          img_s[t] = o;  // pixel t is read and written by this thread only
-          continue;
+    for (int y = wid; y < H; y += n_warps) {
+      const int y0 = rowy[y], y1 = min(y0 + 1, a.gh - 1);
+      const float wy = roww[y];
+      for (int x = lane; x < W; x += 32) {
+        const int t = y * W + x;
+        const float v = value(t);
+        // value coordinate: ((2 v - 1) + 1) n_bins - 1) / 2, as grid_sample
+        // unnormalises the reference's v * 2 - 1
+        const float fb = fminf(fmaxf(((v * 2.0f - 1.0f + 1.0f) * nb - 1.0f) / 2.0f, 0.0f), (float)(nb - 1));
+        const int b0 = (int)fb, b1 = min(b0 + 1, nb - 1);
+        const int x0 = colx[x], x1 = min(x0 + 1, a.gw - 1);
+        const float wb = fb - b0, wx = colw[x];
+        const float* c00 = cdf + (y0 * a.gw + x0) * nb;
+        const float* c01 = cdf + (y0 * a.gw + x1) * nb;
+        const float* c10 = cdf + (y1 * a.gw + x0) * nb;
+        const float* c11 = cdf + (y1 * a.gw + x1) * nb;
+        const float v00 = c00[b0] * (1.f - wb) + c00[b1] * wb;
+        const float v01 = c01[b0] * (1.f - wb) + c01[b1] * wb;
+        const float v10 = c10[b0] * (1.f - wb) + c10[b1] * wb;
+        const float v11 = c11[b0] * (1.f - wb) + c11[b1] * wb;
+        const float o = (v00 * (1.f - wx) + v01 * wx) * (1.f - wy) + (v10 * (1.f - wx) + v11 * wx) * wy;
+        mn = fminf(mn, o);
+        mx = fmaxf(mx, o);
+        if (STAGED && a.minmax_out) {
+          buf[t] = o;  // pixel t is read and written by this thread only
+        } else {
+          dst[t] = o;
         }
       }
-      dst[t] = o;
     }
     if (a.minmax_out) {
       const float2 m = block_minmax(mn, mx, red);  // synchronises the block
       const float den = (1e-4f + m.y) - m.x;
-      for (int t = threadIdx.x; t < P; t += blockDim.x) {
-        float o;
-        if constexpr (STAGED) {
-          o = img_s[t];
-        } else {
-          o = dst[t];
-        }
-        dst[t] = (o - m.x) / den;
-      }
+      for (int t = threadIdx.x; t < P; t += blockDim.x) dst[t] = ((STAGED ? buf[t] : dst[t]) - m.x) / den;
     }
     __syncthreads();
   }
+  if constexpr (STAGED) cp_async_wait<0>();
 }
 
 // --------------------------------------------------------------------- NLPAR
@@ -285,69 +416,81 @@ constexpr int kNlPairs = kNlMaxOffsets / (kNlThreads / (kNlTile * kNlTile));  //
 // Words per staged pixel plane: odd, so the 32 pixels a warp stores land in
 // distinct banks; with the pitch of 24 the 4 x 8 scan points a warp reads at
 // one offset land in distinct banks as well.
-__host__ __device__ __forceinline__ int nl_plane(int halo) { return (kNlTile + 2 * halo) * kNlPitch + 1; }
+__host__ __device__ constexpr int nl_plane(int halo) { return (kNlTile + 2 * halo) * kNlPitch + 1; }
 
-// T[q * plane + yy * pitch + xx] = data[point (y0 - halo + yy, x0 - halo + xx), p0 + q];
-// zero outside the scan (the reference zero-pads the data, nlpar.py:56-61)
+// T[q * plane + yy * pitch + xx] = data[point (y0 - halo + yy, x0 - halo + xx), p0 + q]
+// by 4-byte cp.async; zero outside the scan (the reference zero-pads the
+// data, nlpar.py:56-61) and beyond the last pixel. Completes before return.
+template <int HALO>
 __device__ __forceinline__ void nl_load_chunk(float* T, const float* __restrict__ data, int hs, int ws, int64_t ld,
-                                              int y0, int x0, int halo, int p0, int np) {
-  const int side = kNlTile + 2 * halo, plane = nl_plane(halo);
+                                              int y0, int x0, int p0, int np) {
+  constexpr int side = kNlTile + 2 * HALO, plane = nl_plane(HALO);
   for (int t = threadIdx.x; t < side * side * kNlChunk; t += blockDim.x) {
     const int row = t / kNlChunk, q = t - row * kNlChunk;
     const int yy = row / side, xx = row - yy * side;
-    const int y = y0 - halo + yy, x = x0 - halo + xx;
-    float v = 0.f;
-    if (q < np && y >= 0 && y < hs && x >= 0 && x < ws) v = __ldg(data + ((int64_t)y * ws + x) * ld + p0 + q);
-    T[q * plane + yy * kNlPitch + xx] = v;
+    const int y = y0 - HALO + yy, x = x0 - HALO + xx;
+    float* dst = T + q * plane + yy * kNlPitch + xx;
+    if (q < np && y >= 0 && y < hs && x >= 0 && x < ws)
+      cp_async4(dst, data + ((int64_t)y * ws + x) * ld + p0 + q);
+    else
+      *dst = 0.f;
   }
+  cp_async_commit();
+  cp_async_wait<0>();
 }
 
 // Offsets of one launch as shared-memory displacements; an offset outside
-// [-halo, halo]^2 is marked INT_MIN and yields NaN.
-__device__ __forceinline__ void nl_load_offsets(int* off_s, const int* __restrict__ offsets, int o0, int n_off,
-                                                int halo) {
+// [-halo, halo]^2 reads the point itself and is flagged (its results are NaN).
+__device__ __forceinline__ void nl_load_offsets(int* off_s, unsigned char* bad_s, const int* __restrict__ offsets,
+                                                int o0, int n_off, int halo) {
   for (int o = threadIdx.x; o < n_off; o += blockDim.x) {
     const int di = offsets[2 * (o0 + o)], dj = offsets[2 * (o0 + o) + 1];
     const bool ok = di >= -halo && di <= halo && dj >= -halo && dj <= halo;
-    off_s[o] = ok ? di * kNlPitch + dj : INT_MIN;
+    off_s[o] = ok ? di * kNlPitch + dj : 0;
+    bad_s[o] = ok ? 0 : 1;
   }
 }
 
 // dists[pt, o0 + o] = sum_p (x[pt + off[o]] - x[pt])^2. Thread: one scan
-// point (tid % 64) and the offsets o = tid / 64 + 4 j; a warp shares o.
+// point (tid % 64) and the offsets o = tid / 64 + 4 j (a warp shares o); per
+// chunk the point's own 32 values sit in registers and each offset costs one
+// shared-memory load (immediate offset) per pixel.
+template <int HALO>
 __global__ void __launch_bounds__(kNlThreads) k_nlpar_dists(const float* __restrict__ data, int hs, int ws,
-                                                           int n_pix, int64_t ld, int halo,
-                                                           const int* __restrict__ offsets, int o0, int n_off,
-                                                           int n_off_total, float* __restrict__ dists) {
+                                                           int n_pix, int64_t ld, const int* __restrict__ offsets,
+                                                           int o0, int n_off, int n_off_total,
+                                                           float* __restrict__ dists) {
+  constexpr int plane = nl_plane(HALO);
   extern __shared__ __align__(16) float T[];
   __shared__ int off_s[kNlMaxOffsets];
-  const int plane = nl_plane(halo);
+  __shared__ unsigned char bad_s[kNlMaxOffsets];
   const int tiles_x = (ws + kNlTile - 1) / kNlTile;
   const int y0 = (blockIdx.x / tiles_x) * kNlTile, x0 = (blockIdx.x % tiles_x) * kNlTile;
   const int pt = threadIdx.x % (kNlTile * kNlTile), ob = threadIdx.x / (kNlTile * kNlTile);
-  const int self = (pt / kNlTile + halo) * kNlPitch + pt % kNlTile + halo;
-  nl_load_offsets(off_s, offsets, o0, n_off, halo);
+  const int self = (pt / kNlTile + HALO) * kNlPitch + pt % kNlTile + HALO;
+  const int nj = (n_off - ob + 3) / 4;  // offsets of this thread
+  nl_load_offsets(off_s, bad_s, offsets, o0, n_off, HALO);
   float acc[kNlPairs];
 #pragma unroll
   for (int j = 0; j < kNlPairs; ++j) acc[j] = 0.f;
   for (int p0 = 0; p0 < n_pix; p0 += kNlChunk) {
-    const int np = min(kNlChunk, n_pix - p0);
     __syncthreads();
-    nl_load_chunk(T, data, hs, ws, ld, y0, x0, halo, p0, np);
+    nl_load_chunk<HALO>(T, data, hs, ws, ld, y0, x0, p0, min(kNlChunk, n_pix - p0));
     __syncthreads();
-    for (int q = 0; q < np; ++q) {
-      const float* Tq = T + q * plane + self;
-      const float s = Tq[0];
+    float sv[kNlChunk];
 #pragma unroll
-      for (int j = 0; j < kNlPairs; ++j) {
-        const int o = ob + 4 * j;
-        if (o < n_off) {
-          const int d = off_s[o];
-          if (d != INT_MIN) {
-            const float e = Tq[d] - s;
-            acc[j] = fmaf(e, e, acc[j]);
-          }
+    for (int q = 0; q < kNlChunk; ++q) sv[q] = T[q * plane + self];
+#pragma unroll
+    for (int j = 0; j < kNlPairs; ++j) {
+      if (j < nj) {
+        const float* b = T + self + off_s[ob + 4 * j];
+        float a = acc[j];
+#pragma unroll
+        for (int q = 0; q < kNlChunk; ++q) {
+          const float e = b[q * plane] - sv[q];
+          a = fmaf(e, e, a);
         }
+        acc[j] = a;
       }
     }
   }
@@ -356,52 +499,239 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_dists(const float* __restr
 #pragma unroll
   for (int j = 0; j < kNlPairs; ++j) {
     const int o = ob + 4 * j;
-    if (o < n_off) dists[((int64_t)y * ws + x) * n_off_total + o0 + o] = off_s[o] == INT_MIN ? NAN : acc[j];
+    if (o < n_off) dists[((int64_t)y * ws + x) * n_off_total + o0 + o] = bad_s[o] ? NAN : acc[j];
   }
 }
 
-// out[pt] (+)= sum_o w[pt, o0 + o] x[pt + off[o]]. Warp: 8 scan points,
-// lane = pattern pixel of the chunk; weights staged per tile.
+// out[pt] (+)= sum_o w[pt, o0 + o] x[pt + off[o]]. Warp w: the 8 scan
+// points of tile row w, lane = pattern pixel of the chunk; per offset one
+// displacement load, two float4 weight loads and 8 pattern loads at
+// immediate offsets feed 8 FMAs.
+template <int HALO>
 __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __restrict__ data, int hs, int ws,
-                                                             int n_pix, int64_t ld, int halo,
-                                                             const int* __restrict__ offsets, int o0, int n_off,
-                                                             int n_off_total, const float* __restrict__ weights,
-                                                             int accumulate, float* __restrict__ out,
-                                                             int64_t ld_out) {
+                                                             int n_pix, int64_t ld, const int* __restrict__ offsets,
+                                                             int o0, int n_off, int n_off_total,
+                                                             const float* __restrict__ weights, int accumulate,
+                                                             float* __restrict__ out, int64_t ld_out) {
+  constexpr int plane = nl_plane(HALO);
   extern __shared__ __align__(16) float T[];
   __shared__ int off_s[kNlMaxOffsets];
-  const int plane = nl_plane(halo);
-  float* w_s = T + kNlChunk * plane;  // [64][n_off]
+  __shared__ unsigned char bad_s[kNlMaxOffsets];
+  float* w_s = T + ((kNlChunk * plane + 3) & ~3);  // [o][64 points], 16-byte aligned
   const int tiles_x = (ws + kNlTile - 1) / kNlTile;
   const int y0 = (blockIdx.x / tiles_x) * kNlTile, x0 = (blockIdx.x % tiles_x) * kNlTile;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  nl_load_offsets(off_s, offsets, o0, n_off, halo);
+  nl_load_offsets(off_s, bad_s, offsets, o0, n_off, HALO);
+  __syncthreads();
   for (int t = threadIdx.x; t < kNlTile * kNlTile * n_off; t += blockDim.x) {
-    const int pt = t / n_off, o = t - pt * n_off;
+    const int pt = t % (kNlTile * kNlTile), o = t / (kNlTile * kNlTile);
     const int y = y0 + pt / kNlTile, x = x0 + pt % kNlTile;
-    w_s[t] = (y < hs && x < ws) ? weights[((int64_t)y * ws + x) * n_off_total + o0 + o] : 0.f;
+    float w = 0.f;
+    if (y < hs && x < ws) w = bad_s[o] ? NAN : weights[((int64_t)y * ws + x) * n_off_total + o0 + o];
+    w_s[t] = w;
   }
-  constexpr int kPtsPerWarp = kNlTile * kNlTile / (kNlThreads / 32);  // 8
+  const int y = y0 + wid;
+  const float4* w4 = reinterpret_cast<const float4*>(w_s) + wid * 2;
   for (int p0 = 0; p0 < n_pix; p0 += kNlChunk) {
     const int np = min(kNlChunk, n_pix - p0);
     __syncthreads();
-    nl_load_chunk(T, data, hs, ws, ld, y0, x0, halo, p0, np);
+    nl_load_chunk<HALO>(T, data, hs, ws, ld, y0, x0, p0, np);
     __syncthreads();
-    if (lane >= np) continue;
-    for (int k = 0; k < kPtsPerWarp; ++k) {
-      const int pt = wid * kPtsPerWarp + k;
-      const int y = y0 + pt / kNlTile, x = x0 + pt % kNlTile;
-      if (y >= hs || x >= ws) continue;
-      const float* Tq = T + lane * plane + (pt / kNlTile + halo) * kNlPitch + pt % kNlTile + halo;
-      const float* w = w_s + pt * n_off;
-      float s = 0.f;
-      for (int o = 0; o < n_off; ++o) {
-        const int d = off_s[o];
-        s = fmaf(w[o], d == INT_MIN ? NAN : Tq[d], s);
-      }
-      float* dp = out + ((int64_t)y * ws + x) * ld_out + p0 + lane;
-      *dp = accumulate ? *dp + s : s;
+    if (y >= hs) continue;
+    const float* base = T + lane * plane + (wid + HALO) * kNlPitch + HALO;
+    float s[kNlTile];
+#pragma unroll
+    for (int k = 0; k < kNlTile; ++k) s[k] = 0.f;
+#pragma unroll 4
+    for (int o = 0; o < n_off; ++o) {
+      const float* b = base + off_s[o];
+      const float4 wa = w4[o * (kNlTile * kNlTile / 4)], wb = w4[o * (kNlTile * kNlTile / 4) + 1];
+      s[0] = fmaf(wa.x, b[0], s[0]);
+      s[1] = fmaf(wa.y, b[1], s[1]);
+      s[2] = fmaf(wa.z, b[2], s[2]);
+      s[3] = fmaf(wa.w, b[3], s[3]);
+      s[4] = fmaf(wb.x, b[4], s[4]);
+      s[5] = fmaf(wb.y, b[5], s[5]);
+      s[6] = fmaf(wb.z, b[6], s[6]);
+      s[7] = fmaf(wb.w, b[7], s[7]);
     }
+    if (lane < np) {
+#pragma unroll
+      for (int k = 0; k < kNlTile; ++k) {
+        if (x0 + k < ws) {
+          float* dp = out + ((int64_t)y * ws + x0 + k) * ld_out + p0 + lane;
+          *dp = accumulate ? *dp + s[k] : s[k];
+        }
+      }
+    }
+  }
+}
+
+// ---- NLPAR weights (nlpar.py:122-183): noise estimate, normalised
+// distances, Newton fit of the global coefficient, masked softmax
+
+constexpr int kNlWThreads = 256;
+constexpr int kNlFitBlocks = 592;  // partial sums of one fit iteration
+
+struct NlFitState {
+  double g;       // the coefficient (the reference's guess_coeff)
+  int done;       // |obj| fell below the tolerance in an earlier iteration
+  unsigned ticket;
+};
+
+__global__ void k_nlpar_fit_init(NlFitState* st) {
+  st->g = 1.0;
+  st->done = 0;
+  st->ticket = 0u;
+}
+
+// sigma[pt] = sqrt(min(d[pt, 1..8]) / (2 P))
+__global__ void k_nlpar_sigma(const float* __restrict__ d, int64_t n_pts, int K, int n_pix,
+                              float* __restrict__ sigma) {
+  const int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (pt >= n_pts) return;
+  float m = INFINITY;
+  for (int o = 1; o < 9; ++o) m = fminf(m, d[pt * K + o]);
+  sigma[pt] = sqrtf(m / (float)(2 * n_pix));
+}
+
+// w[pt, o] = -max((d - P s2) / (sqrt(2) sqrt(P) s2), 0), s2 = sigma^2 +
+// sigma_other^2 (sigma_other = 1 outside the scan), in place over d
+__global__ void k_nlpar_logits(float* __restrict__ d, int hs, int ws, int K, int n_pix,
+                               const int* __restrict__ offsets, const float* __restrict__ sigma) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= (int64_t)hs * ws * K) return;
+  const int64_t pt = t / K;
+  const int o = (int)(t - pt * K);
+  const int y = (int)(pt / ws) + offsets[2 * o], x = (int)(pt % ws) + offsets[2 * o + 1];
+  const float so = (y >= 0 && y < hs && x >= 0 && x < ws) ? sigma[(int64_t)y * ws + x] : 1.0f;
+  const float sp = sigma[pt];
+  const float s2 = sp * sp + so * so;
+  const float scale = (float)(1.4142135623730951 * sqrt((double)n_pix));  // 2**0.5 * n_pix**0.5
+  const float v = (d[t] - (float)n_pix * s2) / (scale * s2);
+  d[t] = -fmaxf(v, 0.0f);
+}
+
+// One Newton iteration: per point e_o = exp(w_o / g^2) over offsets 0..8,
+// S = sum e_o; obj = mean(e_0 / S) - coeff, grad = mean(-2 e_0 (w_0 S -
+// sum w_o e_o) / (g^3 S^2)); the last block to finish updates g (FP64 sums).
+__global__ void __launch_bounds__(kNlWThreads) k_nlpar_fit(const float* __restrict__ w, int64_t n_pts, int K,
+                                                          double coeff, double tol, NlFitState* st,
+                                                          double2* __restrict__ partial) {
+  __shared__ double red[32];
+  __shared__ bool last;
+  if (st->done) return;  // uniform: the state is written only by the previous launch
+  const double g = st->g;
+  const float g2 = (float)(g * g), g3 = (float)(g * g * g);
+  double so = 0.0, sg = 0.0;
+  for (int64_t pt = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; pt < n_pts;
+       pt += (int64_t)gridDim.x * blockDim.x) {
+    const float* r = w + pt * K;
+    const float w0 = r[0];
+    const float e0 = expf(w0 / g2);
+    float S = e0, Swe = w0 * e0;
+    for (int o = 1; o < 9; ++o) {
+      const float wo = r[o];
+      const float e = expf(wo / g2);
+      S += e;
+      Swe += wo * e;
+    }
+    so += e0 / S;
+    sg += -2.0f * e0 * (w0 * S - Swe) / (g3 * S * S);
+  }
+  so = block_sum(so, red);
+  sg = block_sum(sg, red);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = make_double2(so, sg);
+    __threadfence();
+    last = atomicAdd(&st->ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+    const double2 v = __ldcg(partial + i);
+    a += v.x;
+    b += v.y;
+  }
+  a = block_sum(a, red);
+  b = block_sum(b, red);
+  if (threadIdx.x == 0) {
+    const double obj = a / (double)n_pts - coeff, grad = b / (double)n_pts;
+    st->g = g - obj / grad;
+    st->done = fabs(obj) < tol ? 1 : 0;
+    st->ticket = 0;
+  }
+}
+
+// weights[pt, :] = softmax over o of (w / g^2, + bias at o = 0; -inf for
+// neighbours outside the scan), in place. One warp per point.
+__global__ void k_nlpar_softmax(float* __restrict__ w, int hs, int ws, int K, const int* __restrict__ offsets,
+                                const NlFitState* st, float bias) {
+  const int64_t pt = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (pt >= (int64_t)hs * ws) return;
+  const float g2 = (float)(st->g * st->g);
+  const int py = (int)(pt / ws), px = (int)(pt % ws);
+  float* r = w + pt * K;
+  float mx = -INFINITY;
+  for (int o = lane; o < K; o += 32) {
+    const int y = py + offsets[2 * o], x = px + offsets[2 * o + 1];
+    float v = r[o] / g2;
+    if (o == 0 && bias > 0.0f) v += bias;
+    if (y < 0 || y >= hs || x < 0 || x >= ws) v = -INFINITY;
+    r[o] = v;
+    mx = fmaxf(mx, v);
+  }
+  mx = warp_max(mx);
+  float sum = 0.f;
+  for (int o = lane; o < K; o += 32) sum += expf(r[o] - mx);
+  sum = warp_sum(sum);
+  for (int o = lane; o < K; o += 32) r[o] = expf(r[o] - mx) / sum;
+}
+
+template <int HALO>
+static int nl_launch(bool average, const float* data, int hs, int ws, int n_pix, int64_t ld, const int* offsets,
+                     int o0, int n_off, int n_off_total, float* dists, const float* weights, int accumulate,
+                     float* out, int64_t ld_out, cudaStream_t s) {
+  const int tiles = ceil_div(hs, kNlTile) * ceil_div(ws, kNlTile);
+  const size_t chunk_bytes = (size_t)kNlChunk * nl_plane(HALO) * sizeof(float);
+  if (!average) {
+    EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_nlpar_dists<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)chunk_bytes));
+    k_nlpar_dists<HALO><<<tiles, kNlThreads, chunk_bytes, s>>>(data, hs, ws, n_pix, ld, offsets, o0, n_off,
+                                                               n_off_total, dists);
+  } else {
+    const size_t smem = ((chunk_bytes + 15) & ~(size_t)15) + (size_t)kNlTile * kNlTile * n_off * sizeof(float);
+    EBSD_CUDA_CHECK(
+        cudaFuncSetAttribute(k_nlpar_average<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_nlpar_average<HALO><<<tiles, kNlThreads, smem, s>>>(data, hs, ws, n_pix, ld, offsets, o0, n_off, n_off_total,
+                                                          weights, accumulate, out, ld_out);
+  }
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+static int nl_dispatch(bool average, const float* data, int hs, int ws, int n_pix, int64_t ld, int k_rad,
+                       const int* offsets, int o0, int n_off, int n_off_total, float* dists, const float* weights,
+                       int accumulate, float* out, int64_t ld_out, cudaStream_t s) {
+  switch (k_rad) {
+#define EBSD_NL_CASE(R)                                                                                          \
+  case R:                                                                                                        \
+    return nl_launch<R>(average, data, hs, ws, n_pix, ld, offsets, o0, n_off, n_off_total, dists, weights,      \
+                        accumulate, out, ld_out, s);
+    EBSD_NL_CASE(0)
+    EBSD_NL_CASE(1)
+    EBSD_NL_CASE(2)
+    EBSD_NL_CASE(3)
+    EBSD_NL_CASE(4)
+    EBSD_NL_CASE(5)
+    EBSD_NL_CASE(6)
+    EBSD_NL_CASE(7)
+#undef EBSD_NL_CASE
+    default:
+      EBSD_ARG_CHECK(false, "NLPAR: kernel radius must be in [0, %d]", kNlMaxRad);
   }
 }
 
@@ -437,7 +767,15 @@ extern "C" int ebsd_normalize_patterns(float* patterns, int64_t n, int n_pix, in
   EBSD_ARG_CHECK(mode >= 0 && mode <= 2, "mode must be 0 (minmax), 1 (zeromean) or 2 (standard)");
   if (n == 0) return 0;
   const int blocks = (int)std::min<int64_t>(n, (int64_t)device_sm_count() * 8);
-  k_normalize<<<blocks, kNormThreads, 0, as_stream(stream)>>>(patterns, n, n_pix, ld, mode);
+  cudaStream_t s = as_stream(stream);
+  if (n_pix <= 4 * kNormThreads)
+    k_normalize<4><<<blocks, kNormThreads, 0, s>>>(patterns, n, n_pix, ld, mode);
+  else if (n_pix <= 8 * kNormThreads)
+    k_normalize<8><<<blocks, kNormThreads, 0, s>>>(patterns, n, n_pix, ld, mode);
+  else if (n_pix <= 16 * kNormThreads)
+    k_normalize<16><<<blocks, kNormThreads, 0, s>>>(patterns, n, n_pix, ld, mode);
+  else
+    k_normalize<0><<<blocks, kNormThreads, 0, s>>>(patterns, n, n_pix, ld, mode);
   EBSD_LAUNCH_CHECK();
   return 0;
 }
@@ -453,8 +791,8 @@ extern "C" int ebsd_clahe(const float* images, int64_t n, int height, int width,
   const int th = (height + grid_h - 1) / grid_h, tw = (width + grid_w - 1) / grid_w;
   // reflect padding needs the pad to be smaller than the image
   EBSD_ARG_CHECK(grid_h * th - height < height && grid_w * tw - width < width, "ebsd_clahe: padding too large");
-  const size_t tables = (size_t)grid_h * grid_w * n_bins * (sizeof(float) + sizeof(int));
-  EBSD_ARG_CHECK(tables <= kClaheSmemCap, "ebsd_clahe: grid x bins too large for shared memory");
+  const ClaheLayout lay(height, width, grid_h, grid_w, n_bins);
+  EBSD_ARG_CHECK(lay.total_tables <= kClaheSmemCap, "ebsd_clahe: grid x bins too large for shared memory");
   EBSD_ARG_CHECK(images != out || ld == ld_out, "ebsd_clahe: in place needs ld == ld_out");
   if (n == 0) return 0;
   ClaheArgs a;
@@ -472,11 +810,13 @@ extern "C" int ebsd_clahe(const float* images, int64_t n, int height, int width,
   a.nb = n_bins;
   a.gh = grid_h;
   a.gw = grid_w;
+  const int n_pix = height * width;
+  a.vec16 = (reinterpret_cast<uintptr_t>(images) % 16 == 0 && ld % 4 == 0 && n_pix % 4 == 0) ? 1 : 0;
   a.out = out;
   a.ld_out = ld_out;
-  const int n_pix = height * width;
-  const bool staged = tables + (size_t)n_pix * sizeof(float) <= kClaheSmemCap;
-  const size_t smem = tables + (staged ? (size_t)n_pix * sizeof(float) : 0);
+  const size_t staged_smem = lay.total_tables + 2 * (size_t)n_pix * sizeof(float);
+  const bool staged = staged_smem <= kClaheSmemCap;
+  const size_t smem = staged ? staged_smem : lay.total_tables;
   cudaStream_t s = as_stream(stream);
   if (staged) {
     EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_clahe<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -486,7 +826,9 @@ extern "C" int ebsd_clahe(const float* images, int64_t n, int height, int width,
     k_clahe<true><<<blocks, kClaheThreads, smem, s>>>(a);
   } else {
     EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_clahe<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int blocks = (int)std::min<int64_t>(n, (int64_t)device_sm_count() * 4);
+    int per_sm = 0;
+    EBSD_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_clahe<false>, kClaheThreads, smem));
+    const int blocks = (int)std::min<int64_t>(n, (int64_t)device_sm_count() * std::max(per_sm, 1));
     k_clahe<false><<<blocks, kClaheThreads, smem, s>>>(a);
   }
   EBSD_LAUNCH_CHECK();
@@ -508,13 +850,8 @@ extern "C" int ebsd_nlpar_dists(const float* data, int scan_h, int scan_w, int n
                                 const int* offsets, int o0, int n_off, int n_off_total, float* dists, void* stream) {
   if (int rc = nl_check(data, scan_h, scan_w, n_pix, ld, k_rad, offsets, o0, n_off, n_off_total)) return rc;
   EBSD_ARG_CHECK(dists != nullptr, "NLPAR: null output");
-  const size_t smem = (size_t)kNlChunk * nl_plane(k_rad) * sizeof(float);
-  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_nlpar_dists, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int tiles = ceil_div(scan_h, kNlTile) * ceil_div(scan_w, kNlTile);
-  k_nlpar_dists<<<tiles, kNlThreads, smem, as_stream(stream)>>>(data, scan_h, scan_w, n_pix, ld, k_rad, offsets, o0,
-                                                              n_off, n_off_total, dists);
-  EBSD_LAUNCH_CHECK();
-  return 0;
+  return nl_dispatch(false, data, scan_h, scan_w, n_pix, ld, k_rad, offsets, o0, n_off, n_off_total, dists, nullptr,
+                     0, nullptr, 0, as_stream(stream));
 }
 
 extern "C" int ebsd_nlpar_average(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
@@ -523,12 +860,42 @@ extern "C" int ebsd_nlpar_average(const float* data, int scan_h, int scan_w, int
   if (int rc = nl_check(data, scan_h, scan_w, n_pix, ld, k_rad, offsets, o0, n_off, n_off_total)) return rc;
   EBSD_ARG_CHECK(weights && out && ld_out >= n_pix, "NLPAR: bad output");
   EBSD_ARG_CHECK(out != data, "NLPAR: the average cannot be written in place");
-  const size_t smem = ((size_t)kNlChunk * nl_plane(k_rad) + (size_t)kNlTile * kNlTile * n_off) * sizeof(float);
-  EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_nlpar_average, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const int tiles = ceil_div(scan_h, kNlTile) * ceil_div(scan_w, kNlTile);
-  k_nlpar_average<<<tiles, kNlThreads, smem, as_stream(stream)>>>(data, scan_h, scan_w, n_pix, ld, k_rad, offsets,
-                                                                o0, n_off, n_off_total, weights, accumulate, out,
-                                                                ld_out);
+  return nl_dispatch(true, data, scan_h, scan_w, n_pix, ld, k_rad, offsets, o0, n_off, n_off_total, nullptr, weights,
+                     accumulate, out, ld_out, as_stream(stream));
+}
+
+extern "C" size_t ebsd_nlpar_workspace_bytes(int scan_h, int scan_w) {
+  return 64 + (size_t)kNlFitBlocks * sizeof(double2) + (size_t)scan_h * scan_w * sizeof(float);
+}
+
+extern "C" int ebsd_nlpar_weights(float* dists, int scan_h, int scan_w, int n_pix, const int* offsets, int n_off,
+                                  float coeff, float coeff_fit_tol, float center_logit_bias, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  EBSD_ARG_CHECK(dists && offsets && workspace, "ebsd_nlpar_weights: null pointer");
+  EBSD_ARG_CHECK(scan_h >= 1 && scan_w >= 1 && n_pix >= 1, "ebsd_nlpar_weights: bad sizes");
+  EBSD_ARG_CHECK(n_off >= 9, "ebsd_nlpar_weights: the window needs at least 9 offsets (k_rad >= 1)");
+  EBSD_ARG_CHECK(workspace_bytes >= ebsd_nlpar_workspace_bytes(scan_h, scan_w),
+                 "ebsd_nlpar_weights: workspace too small");
+  EBSD_ARG_CHECK(reinterpret_cast<uintptr_t>(workspace) % 16 == 0, "ebsd_nlpar_weights: workspace not 16-byte aligned");
+  cudaStream_t s = as_stream(stream);
+  auto* st = reinterpret_cast<NlFitState*>(workspace);
+  auto* partial = reinterpret_cast<double2*>(static_cast<uint8_t*>(workspace) + 64);
+  float* sigma = reinterpret_cast<float*>(partial + kNlFitBlocks);
+  const int64_t n_pts = (int64_t)scan_h * scan_w;
+  k_nlpar_fit_init<<<1, 1, 0, s>>>(st);
+  EBSD_LAUNCH_CHECK();
+  k_nlpar_sigma<<<ceil_div(n_pts, 256), 256, 0, s>>>(dists, n_pts, n_off, n_pix, sigma);
+  EBSD_LAUNCH_CHECK();
+  k_nlpar_logits<<<ceil_div(n_pts * n_off, 256), 256, 0, s>>>(dists, scan_h, scan_w, n_off, n_pix, offsets, sigma);
+  EBSD_LAUNCH_CHECK();
+  const int fit_blocks = (int)std::min<int64_t>(kNlFitBlocks, ceil_div(n_pts, kNlWThreads));
+  for (int i = 0; i < 10; ++i) {
+    k_nlpar_fit<<<fit_blocks, kNlWThreads, 0, s>>>(dists, n_pts, n_off, (double)coeff, (double)coeff_fit_tol, st,
+                                                   partial);
+    EBSD_LAUNCH_CHECK();
+  }
+  k_nlpar_softmax<<<ceil_div(n_pts * 32, 256), 256, 0, s>>>(dists, scan_h, scan_w, n_off, offsets, st,
+                                                            center_logit_bias);
   EBSD_LAUNCH_CHECK();
   return 0;
 }

@@ -321,6 +321,21 @@ int ebsd_nlpar_dists(const float* data, int scan_h, int scan_w, int n_pix, int64
 int ebsd_nlpar_average(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
                        const int* offsets, int o0, int n_off, int n_off_total, const float* weights, int accumulate,
                        float* out, int64_t ld_out, void* stream);
+/* The NLPAR weights between the two passes (nlpar.py:122-183), in place over
+ * dists (scan_h * scan_w x n_off, offsets as above, n_off >= 9): noise
+ * estimate sigma = sqrt(min(dists[:, 1..8]) / (2 n_pix)), normalised
+ * distances (dists - n_pix s2) / (sqrt(2 n_pix) s2) with s2 = sigma^2 +
+ * sigma_neighbour^2 (1 outside the scan), clamped and negated; 10 Newton
+ * iterations (stopping once |obj| < coeff_fit_tol) fitting the coefficient g
+ * so that the mean softmax weight of offset 0 over offsets 0..8 equals coeff;
+ * then softmax over the window of w / g^2 (+ center_logit_bias at offset 0 when
+ * > 0; neighbours outside the scan get weight 0). workspace: device memory of
+ * ebsd_nlpar_workspace_bytes(scan_h, scan_w) bytes, 16-byte aligned. Launches
+ * 14 kernels; nothing synchronises with the host. */
+size_t ebsd_nlpar_workspace_bytes(int scan_h, int scan_w);
+int ebsd_nlpar_weights(float* dists, int scan_h, int scan_w, int n_pix, const int* offsets, int n_off, float coeff,
+                       float coeff_fit_tol, float center_logit_bias, void* workspace, size_t workspace_bytes,
+                       void* stream);
 
 /* ---- local dictionary search around orientation proposals --------------------
  * No counterpart in the reference (search step of the learned-proposal path).
