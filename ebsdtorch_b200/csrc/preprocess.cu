@@ -456,7 +456,7 @@ __device__ __forceinline__ void nl_load_offsets(int* off_s, unsigned char* bad_s
 // chunk the point's own 32 values sit in registers and each offset costs one
 // shared-memory load (immediate offset) per pixel.
 template <int HALO>
-__global__ void __launch_bounds__(kNlThreads) k_nlpar_dists(const float* __restrict__ data, int hs, int ws,
+__global__ void __launch_bounds__(kNlThreads, 3) k_nlpar_dists(const float* __restrict__ data, int hs, int ws,
                                                            int n_pix, int64_t ld, const int* __restrict__ offsets,
                                                            int o0, int n_off, int n_off_total,
                                                            float* __restrict__ dists) {
@@ -477,20 +477,25 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_dists(const float* __restr
     __syncthreads();
     nl_load_chunk<HALO>(T, data, hs, ws, ld, y0, x0, p0, min(kNlChunk, n_pix - p0));
     __syncthreads();
-    float sv[kNlChunk];
+    // two halves of 16 pixels keep 16 own values in registers (3 CTAs per SM)
+#pragma unroll 1
+    for (int h = 0; h < kNlChunk; h += kNlChunk / 2) {
+      const float* Th = T + h * plane;
+      float sv[kNlChunk / 2];
 #pragma unroll
-    for (int q = 0; q < kNlChunk; ++q) sv[q] = T[q * plane + self];
+      for (int q = 0; q < kNlChunk / 2; ++q) sv[q] = Th[q * plane + self];
 #pragma unroll
-    for (int j = 0; j < kNlPairs; ++j) {
-      if (j < nj) {
-        const float* b = T + self + off_s[ob + 4 * j];
-        float a = acc[j];
+      for (int j = 0; j < kNlPairs; ++j) {
+        if (j < nj) {
+          const float* b = Th + self + off_s[ob + 4 * j];
+          float a = acc[j];
 #pragma unroll
-        for (int q = 0; q < kNlChunk; ++q) {
-          const float e = b[q * plane] - sv[q];
-          a = fmaf(e, e, a);
+          for (int q = 0; q < kNlChunk / 2; ++q) {
+            const float e = b[q * plane] - sv[q];
+            a = fmaf(e, e, a);
+          }
+          acc[j] = a;
         }
-        acc[j] = a;
       }
     }
   }
