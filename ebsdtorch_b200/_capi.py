@@ -54,6 +54,8 @@ SIGNATURES = {
     "ebsd_nlpar_dists": (i32, [vp, i32, i32, i32, i64, i32, vp, i32, i32, i32, vp, vp]),
     "ebsd_nlpar_average": (i32, [vp, i32, i32, i32, i64, i32, vp, i32, i32, i32, vp, i32, vp, i64, vp]),
     "ebsd_nlpar_workspace_bytes": (sz, [i32, i32]),
+    "ebsd_pcfit_prep": (i32, [vp, i32, i32, i32, i32, i32, i32, i32, i32, vp, vp]),
+    "ebsd_pcfit_reduce": (i32, [vp, i32, i32, i32, i32, i64, vp, vp, vp]),
     "ebsd_nlpar_weights": (i32, [vp, i32, i32, i32, vp, i32, f32, f32, f32, vp, sz, vp]),
     "ebsd_local_search": (i32, [vp, i64, i64, vp, i32, i32, vp, vp, vp, i64, vp, i32, i64, vp, vp, i32, i64, i32,
                                 i32, f32, i32, vp, vp, vp, vp]),
@@ -88,6 +90,7 @@ LAUNCHES_PER_CALL = {
     "ebsd_cell_to_row": 2, "ebsd_local_search": 1, "ebsd_refine_grid": 1,
     "ebsd_pattern_mean": 2, "ebsd_subtract_pattern": 1, "ebsd_normalize_patterns": 1, "ebsd_clahe": 1,
     "ebsd_nlpar_dists": 1, "ebsd_nlpar_average": 1, "ebsd_nlpar_weights": 14,
+    "ebsd_pcfit_prep": 1, "ebsd_pcfit_reduce": 1,
     "ebsd_rot6d_sym_loss": 1, "ebsd_cnn_im2col": 1, "ebsd_cnn_col2im": 1, "ebsd_cnn_bias_act": 1,
     "ebsd_cnn_conv_fwd": 1, "ebsd_cnn_conv_c1": 1, "ebsd_cnn_relu_grad": 1, "ebsd_cnn_col_sum": 1,
     "ebsd_cnn_transpose": 1, "ebsd_cnn_scale_cast": 1,

@@ -337,6 +337,23 @@ int ebsd_nlpar_weights(float* dists, int scan_h, int scan_w, int n_pix, const in
                        float coeff_fit_tol, float center_logit_bias, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* ---- pattern-centre fitting (spatial FFT search) -----------------------------
+ * The kernels around the FFT cross-correlation of spatial_fft_pc_fitter
+ * (fitting.py:359-540); the dictionary on the enlarged detector comes from
+ * ebsd_project_dictionary (subtract_mean 0) and the FFTs from the caller.
+ * ebsd_pcfit_prep: n binned patterns (height x width, contiguous) ->
+ * (x - min) / max(x - min), minus the mean when zero_mean, written into
+ * out (n x padded_h x padded_w, zero elsewhere) at (pad_top, pad_left)
+ * (fitting.py:387-412). ebsd_pcfit_reduce: corr (n x n_patterns x padded_h x
+ * padded_w) holds the circular cross-correlations of n dictionary entries;
+ * for every (pattern, shift) the maximum over the n entries, read through
+ * fftshift, updates best = max(best, max) and, where the maximum equals the
+ * new best, best_index = index_base + its entry (fitting.py:498-507). */
+int ebsd_pcfit_prep(const float* patterns, int n, int height, int width, int padded_h, int padded_w, int pad_top,
+                    int pad_left, int zero_mean, float* out, void* stream);
+int ebsd_pcfit_reduce(const float* corr, int n, int n_patterns, int padded_h, int padded_w, int64_t index_base,
+                      float* best, int64_t* best_index, void* stream);
+
 /* ---- local dictionary search around orientation proposals --------------------
  * No counterpart in the reference (search step of the learned-proposal path).
  * cell_to_row (edge^3 int32): dictionary row of each cubochoric grid cell or

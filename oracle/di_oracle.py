@@ -1155,3 +1155,97 @@ def nlpar(data: np.ndarray, k_rad: int = 5, coeff: float = 0.375, coeff_fit_tol:
     for i, (di, dj) in enumerate(off):
         out += pad[k_rad + di:k_rad + di + hs, k_rad + dj:k_rad + dj + ws] * weights[:, :, i:i + 1]
     return out.reshape(data.shape)
+
+
+# --------------------------------------------------------------------------
+# Pattern-centre fitting (ebsd/fitting.py:54-540, spatial FFT fitter)
+# --------------------------------------------------------------------------
+
+
+def pixel_coords_with_periphery(detector_shape, pc_x_min, pc_x_max, pc_y_min, pc_y_max, binning=1):
+    """(Hp * Wp, 3) detector-frame pixel coordinates of the detector enlarged
+    by the pattern-centre search range, the padding (w_prior, w_after,
+    h_prior, h_after) and the enlarged shape (fitting.py:219-289): per axis
+    linspace(0.5 (b - 1) - prior, size + after - 0.5 (b - 1), n), row-major,
+    z = 0. The padding uses the reference's float expressions and int()
+    truncation."""
+    import torch
+
+    H, W = detector_shape
+    bf = float(binning)
+    wpp = int((0.5 - pc_x_min) * W / bf)
+    wpa = int((pc_x_max - 0.5) * W / bf)
+    hpp = int((0.5 - pc_y_min) * H / bf)
+    hpa = int((pc_y_max - 0.5) * H / bf)
+    shape = (H // binning + hpp + hpa, W // binning + wpp + wpa)
+    # float32 linspace as torch builds it
+    ii = torch.linspace(0.5 * (bf - 1) - hpp, H + hpa - 0.5 * (bf - 1), shape[0], dtype=torch.float32).double()
+    jj = torch.linspace(0.5 * (bf - 1) - wpp, W + wpa - 0.5 * (bf - 1), shape[1], dtype=torch.float32).double()
+    gi, gj = np.meshgrid(ii.numpy(), jj.numpy(), indexing="ij")
+    pix = np.stack((gi.reshape(-1), gj.reshape(-1), np.zeros(gi.size)), axis=1)
+    return pix, (wpp, wpa, hpp, hpa), shape
+
+
+def bruker_se3(pc, primary_tilt_deg, secondary_tilt_deg, detector_shape):
+    """Rotation and translation of the Bruker pattern-centre convention
+    (fitting.py:54-115), float64."""
+    pcx, pcy, pcz = pc
+    rows, cols = float(detector_shape[0]), float(detector_shape[1])
+    d, sx = math.radians(primary_tilt_deg), math.radians(secondary_tilt_deg)
+    sd, cd, ss, cs = math.sin(d), math.cos(d), math.sin(sx), math.cos(sx)
+    rot = np.array([[-sd, -ss * cd, cs * cd], [0.0, cs, ss], [-cd, ss * sd, -sd * cs]])
+    t = np.array([
+        pcx * cols * ss * cd + pcy * rows * sd + pcz * rows * cs * cd - ss * cd / 2 - sd / 2,
+        -cols * pcx * cs + pcz * rows * ss + cs / 2,
+        -cols * pcx * ss * sd + pcy * rows * cd - pcz * rows * sd * cs + ss * sd / 2 - cd / 2,
+    ])
+    return rot, t
+
+
+def spatial_fft_pc_fit(master_pattern, patterns, quats_dict, pc_x_min=0.0, pc_x_max=1.0, pc_y_min=0.0,
+                       pc_y_max=1.0, pc_z_min=0.3, pc_z_max=0.7, pc_z_steps=16, primary_tilt_deg=70.0,
+                       secondary_tilt_deg=0.0, batch_size=1024, virtual_binning=1, batch_local_index=False):
+    """The spatial FFT pattern-centre fitter (fitting.py:359-540), float64:
+    patterns (B, 1, H, W) binned, min-max scaled, zero-mean, zero-padded to
+    the enlarged detector; for each pc_z of linspace(min, max, steps) the
+    dictionary (quats_dict, in the fitter's order) is simulated on the
+    enlarged detector (pc_x = pc_y = 0.5, primary tilt negated) and
+    circularly cross-correlated with every pattern by FFT (fftshifted); the
+    running maximum over the dictionary starts at 0 per (pc_z, pattern,
+    shift). The fit is the argmax of the mean over patterns; pc_x / pc_y
+    follow from the shift. batch_local_index reproduces the reference's
+    orientation index, which is local to the dictionary batch that won.
+    Returns (pc (3,), orientation indices (B,), mean best dots (steps, Hp, Wp))."""
+    import torch
+
+    B, C, H, W = patterns.shape
+    b = virtual_binning
+    Hb, Wb = H // b, W // b
+    x = avg_pool(patterns[:, 0].astype(np.float64), b)
+    x = x - x.reshape(B, -1).min(axis=1)[:, None, None]
+    x = x / x.reshape(B, -1).max(axis=1)[:, None, None]
+    x = x - x.reshape(B, -1).mean(axis=1)[:, None, None]
+    pix, pad, (Hp, Wp) = pixel_coords_with_periphery((H, W), pc_x_min, pc_x_max, pc_y_min, pc_y_max, b)
+    xp = np.zeros((B, Hp, Wp))
+    xp[:, pad[2]:pad[2] + Hb, pad[0]:pad[0] + Wb] = x
+    xf = np.conj(np.fft.rfft2(xp))
+    mp = avg_pool(master_pattern.astype(np.float64), b)
+    z_vals = torch.linspace(pc_z_min, pc_z_max, pc_z_steps, dtype=torch.float32).double().numpy()
+    best = np.zeros((pc_z_steps, B, Hp, Wp))
+    best_i = np.zeros((pc_z_steps, B, Hp, Wp), dtype=np.int64)
+    for zi, z in enumerate(z_vals):
+        rot, t = bruker_se3((0.5, 0.5, z), -primary_tilt_deg, secondary_tilt_deg, (H, W))
+        rays = unit_rays(pix @ rot.T + t)
+        for j in range(0, quats_dict.shape[0], batch_size):
+            q = quats_dict[j:j + batch_size].astype(np.float64)
+            sims = project_patterns(mp, rays, q).reshape(-1, Hp, Wp)
+            corr = np.fft.irfft2(np.fft.rfft2(sims)[:, None] * xf[None], s=(Hp, Wp))
+            corr = np.fft.fftshift(corr, axes=(-2, -1))
+            vals, idx = corr.max(axis=0), corr.argmax(axis=0)
+            best[zi] = np.maximum(best[zi], vals)
+            best_i[zi] = np.where(best[zi] == vals, idx + (0 if batch_local_index else j), best_i[zi])
+    avg = best.mean(axis=1)
+    zi, yi, xi = np.unravel_index(int(avg.argmax()), avg.shape)
+    pc = np.array([0.5 + float(xi - pad[0] - (Wb + 1) // 2) / Wb, 0.5 + float(yi - pad[2] - (Hb + 1) // 2) / Hb,
+                   float(z_vals[zi])])
+    return pc, best_i[zi, :, yi, xi], avg

@@ -12,8 +12,8 @@ modified. The PCA variant is also loaded with line 355's component slice
 ``[:, -n : -n + 300]`` replaced by ``[:, -n:]`` (the "top" slice).
 
 Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
-outputs of one case (``--refinement-only`` / ``--preprocessing-only`` write
-just refine.npz / preprocess.npz). The files are small (< 1 MB each) and committed.
+outputs of one case (``--refinement-only`` / ``--preprocessing-only`` /
+``--pcfit-only`` write just refine.npz / preprocess.npz / pcfit.npz). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -167,6 +167,78 @@ def preprocessing_goldens(root: str = "/root/reference"):
         out[name] = nlpar(scan.clone(), k_rad=k, coeff=c).numpy()
         out[name + "_args"] = np.array([k, c], dtype=np.float64)
     np.savez_compressed(os.path.join(HERE, "preprocess.npz"), **out)
+
+
+def pcfit_goldens(root: str = "/root/reference"):
+    """Pattern-centre fitting (ebsd/fitting.py:359-540, spatial FFT fitter):
+    three cases (binning 1 / 2, one or several dictionary batches, tilts),
+    the enlarged pixel grid and the first simulated dictionary patterns.
+    fitting.py imports matplotlib (for a plotting helper that is commented
+    out) and, through io/read_master_pattern.py, h5py; neither is used by the
+    fitter, so empty stand-in modules are registered when they are absent."""
+    sys.path.insert(0, root)
+    for name in ("matplotlib", "matplotlib.pyplot", "h5py"):
+        try:
+            __import__(name)
+        except ImportError:
+            sys.modules[name] = types.ModuleType(name)
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    from ebsdtorch.ebsd import fitting as F
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+
+    out = {}
+    cases = [
+        dict(det=(16, 16), b=1, seed=41, pc=(0.5625, 0.4375, 0.5), x=(0.4, 0.6), y=(0.4, 0.6), z=(0.4, 0.6, 5),
+             tilt=70.0, sec=0.0, res=10.0, bs=1024, n=3),
+        dict(det=(24, 20), b=2, seed=42, pc=(0.4, 0.5833333, 0.55), x=(0.3, 0.75), y=(0.35, 0.65),
+             z=(0.45, 0.75, 4), tilt=70.0, sec=0.0, res=12.0, bs=16, n=2),
+        dict(det=(20, 20), b=1, seed=43, pc=(0.55, 0.5, 0.62), x=(0.4, 0.6), y=(0.45, 0.65), z=(0.5, 0.7, 3),
+             tilt=65.0, sec=5.0, res=12.0, bs=1024, n=2),
+    ]
+    for ci, c in enumerate(cases):
+        mp_t = smooth_master_pattern(c["seed"], 41)
+        mp = MasterPattern(mp_t.clone(), laue_group=11)
+        H, W = c["det"]
+        # patterns simulated with the fitter's own helpers at the true PC
+        torch.manual_seed(c["seed"])
+        dict_q = sample_ori_fz_laue_angle(laue_id=11, angular_resolution_deg=c["res"], device=torch.device("cpu"))
+        truth_idx = torch.randint(0, dict_q.shape[0], (c["n"],))
+        rot, tr = F.bruker_geometries_to_SE3(torch.tensor([list(c["pc"])]), torch.tensor(-c["tilt"]),
+                                             torch.tensor(c["sec"]), (H, W))
+        pix = F.get_3D_pixel_coords((H, W), torch.device("cpu"))
+        with torch.no_grad():
+            coords = F.generate_dictionary_coords(pix, dict_q[truth_idx], rot, tr)
+            pats = mp.interpolate(coords, normalize_coords=False).view(c["n"], 1, H, W)
+            pats = pats + 0.02 * torch.randn(pats.shape, generator=torch.Generator().manual_seed(c["seed"]))
+        kw = dict(pc_x_min=c["x"][0], pc_x_max=c["x"][1], pc_y_min=c["y"][0], pc_y_max=c["y"][1],
+                  pc_z_min=c["z"][0], pc_z_max=c["z"][1], pc_z_steps=c["z"][2], primary_tilt_deg=c["tilt"],
+                  secondary_tilt_deg=c["sec"], dictionary_resolution_deg=c["res"],
+                  dictionary_indexing_batch_size=c["bs"], virtual_binning=c["b"], metric="dot")
+        torch.manual_seed(1000 + ci)  # fixes the dictionary permutation inside the fitter
+        with contextlib.redirect_stdout(io.StringIO()), contextlib.redirect_stderr(io.StringIO()):
+            best_pc, best_q = F.spatial_fft_pc_fitter(MasterPattern(mp_t.clone(), laue_group=11), pats.clone(), **kw)
+        torch.manual_seed(1000 + ci)
+        fit_dict = sample_ori_fz_laue_angle(laue_id=11, angular_resolution_deg=c["res"], device=torch.device("cpu"))
+        pp, padding, shape = F.get_3D_pixel_coords_with_periphery(
+            (H, W), torch.device("cpu"), c["x"][0], c["x"][1], c["y"][0], c["y"][1], c["b"])
+        r0, t0 = F.bruker_geometries_to_SE3(torch.tensor([[0.5, 0.5, c["z"][0]]]), torch.tensor(-c["tilt"]),
+                                            torch.tensor(c["sec"]), (H, W))
+        with torch.no_grad():
+            mpb = MasterPattern(mp_t.clone(), laue_group=11)
+            sims = mpb.interpolate(F.generate_dictionary_coords(pp, fit_dict[:4], r0, t0), mode="bilinear",
+                                   align_corners=False, normalize_coords=False, virtual_binning=c["b"])
+        out[f"case{ci}_master_pattern"] = mp_t.numpy()
+        out[f"case{ci}_patterns"] = pats.numpy()
+        out[f"case{ci}_dictionary"] = fit_dict.numpy()
+        out[f"case{ci}_best_pc"] = best_pc.numpy()
+        out[f"case{ci}_best_quats"] = best_q.numpy()
+        out[f"case{ci}_pixel_coords"] = pp.numpy()
+        out[f"case{ci}_padding"] = np.array([*padding, *shape], dtype=np.int64)
+        out[f"case{ci}_sims"] = sims.reshape(4, *shape).numpy()
+        out[f"case{ci}_meta"] = np.array([H, W, c["b"], *c["x"], *c["y"], c["z"][0], c["z"][1], c["z"][2],
+                                          c["tilt"], c["sec"], c["res"], c["bs"], 1000 + ci], dtype=np.float64)
+    np.savez_compressed(os.path.join(HERE, "pcfit.npz"), **out)
 
 
 def main(root: str = "/root/reference"):
@@ -390,7 +462,10 @@ if __name__ == "__main__":
         refinement_goldens(*args[1:])
     elif args and args[0] == "--preprocessing-only":
         preprocessing_goldens(*args[1:])
+    elif args and args[0] == "--pcfit-only":
+        pcfit_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
         preprocessing_goldens(*args)
+        pcfit_goldens(*args)

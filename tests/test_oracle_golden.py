@@ -333,3 +333,49 @@ def test_nlpar_offsets_order():
         assert l1[0] == 0 and (l1[1:5] == 1).all() and (l1[5:9] == 2).all()
         assert (l1[:-1] <= l1[1:]).all()
         assert len({tuple(o) for o in off}) == off.shape[0]
+
+
+# ---- pattern-centre fitting ---------------------------------------------------
+
+
+def _pcfit_args(g, ci):
+    H, W, b, x0, x1, y0, y1, z0, z1, zs, tilt, sec, res, bs, seed = g[f"case{ci}_meta"]
+    return dict(pc_x_min=x0, pc_x_max=x1, pc_y_min=y0, pc_y_max=y1, pc_z_min=z0, pc_z_max=z1, pc_z_steps=int(zs),
+                primary_tilt_deg=tilt, secondary_tilt_deg=sec, virtual_binning=int(b)), int(bs), int(seed)
+
+
+@pytest.mark.parametrize("ci", [0, 1, 2])
+def test_pc_fit_oracle_matches_reference(golden, ci):
+    """spatial_fft_pc_fitter (fitting.py:359-540): the enlarged pixel grid,
+    the simulated dictionary on it, and the fitted pattern centre and
+    orientations (binning 1 / 2, one and two dictionary batches, secondary
+    tilt, an odd enlarged height)."""
+    g = golden("pcfit")
+    kw, bs, _ = _pcfit_args(g, ci)
+    H, W = (int(v) for v in g[f"case{ci}_meta"][:2])
+    pix, pad, shape = O.pixel_coords_with_periphery((H, W), kw["pc_x_min"], kw["pc_x_max"], kw["pc_y_min"],
+                                                    kw["pc_y_max"], kw["virtual_binning"])
+    assert np.array_equal(pix, g[f"case{ci}_pixel_coords"].astype(np.float64))
+    assert (*pad, *shape) == tuple(g[f"case{ci}_padding"])
+    rot, t = O.bruker_se3((0.5, 0.5, float(np.float32(kw["pc_z_min"]))), -kw["primary_tilt_deg"],
+                          kw["secondary_tilt_deg"], (H, W))
+    mp = O.avg_pool(g[f"case{ci}_master_pattern"].astype(np.float64), kw["virtual_binning"])
+    sims = O.project_patterns(mp, O.unit_rays(pix @ rot.T + t), g[f"case{ci}_dictionary"][:4].astype(np.float64))
+    assert np.abs(sims.reshape(g[f"case{ci}_sims"].shape) - g[f"case{ci}_sims"]).max() < 2e-4
+    pc, idx, _ = O.spatial_fft_pc_fit(g[f"case{ci}_master_pattern"], g[f"case{ci}_patterns"],
+                                      g[f"case{ci}_dictionary"], batch_size=bs, batch_local_index=True, **kw)
+    assert np.abs(pc - g[f"case{ci}_best_pc"]).max() < 1e-6
+    assert np.array_equal(g[f"case{ci}_dictionary"][idx], g[f"case{ci}_best_quats"])
+
+
+def test_bruker_se3_round_trip():
+    import torch
+
+    from ebsdtorch_b200.ebsd import fitting as F
+
+    pcs = torch.tensor([[0.45, 0.55, 0.6], [0.5, 0.4, 0.7]], dtype=torch.float64)
+    r, t = F.bruker_geometries_to_SE3(pcs, torch.tensor(70.0), torch.tensor(10.0), (60, 80))
+    back, tilt, sec = F.bruker_geometry_from_SE3(r, t, (60, 80))
+    assert torch.allclose(back, pcs, atol=1e-12)
+    assert torch.allclose(tilt, torch.full((2,), 70.0, dtype=torch.float64))
+    assert torch.allclose(sec, torch.full((2,), 10.0, dtype=torch.float64))
