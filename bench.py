@@ -770,6 +770,130 @@ def run_preprocess(args):
     print(json.dumps(line), flush=True)
 
 
+PCFIT = dict(det=(60, 60), n=16, x=(0.35, 0.65), y=(0.35, 0.65), z=(0.4, 0.7, 8), res=2.0, bs=1024, mp=257,
+             pc=(0.5, 0.5, 0.55),
+             name="16 patterns of 60 x 60, pc_x / pc_y in [0.35, 0.65] (enlarged detector 78 x 78), 8 pc_z steps, "
+                  "m-3m 2.0 deg dictionary")
+
+
+def run_pcfit(args):
+    """Pattern-centre fitting (spatial_fft_pc_fitter, fitting.py:359-540):
+    whole fits on the device, and the four stages of one dictionary chunk
+    timed apart (projection on the enlarged detector, rfft2, spectrum
+    product + irfft2, the fused fftshift / max / argmax reduction)."""
+    import numpy as np
+    import torch
+
+    from ebsdtorch_b200 import _capi, kernels, synthetic
+    from ebsdtorch_b200.ebsd import EBSDGeometry, MasterPattern, spatial_fft_pc_fitter
+    from ebsdtorch_b200.ebsd import fitting as F
+    from ebsdtorch_b200.ebsd.indexing import _master_pattern_tensor
+    from ebsdtorch_b200.kernels import RowBuffers
+    from ebsdtorch_b200.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+
+    cfg = PCFIT
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    _capi.load()
+    mp_t = synthetic.synthetic_master_pattern(cfg["mp"], seed=0, device=dev)
+    mp = MasterPattern(mp_t, laue_group=11)
+    geom = EBSDGeometry(cfg["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=cfg["pc"])
+    truth = synthetic.random_quaternions(cfg["n"], 21).to(dev)
+    pats = synthetic.synthetic_patterns(mp_t, geom, truth, mean_counts=200.0, seed=22).float()
+    pats = pats.view(cfg["n"], 1, *cfg["det"])
+    kw = dict(pc_x_min=cfg["x"][0], pc_x_max=cfg["x"][1], pc_y_min=cfg["y"][0], pc_y_max=cfg["y"][1],
+              pc_z_min=cfg["z"][0], pc_z_max=cfg["z"][1], pc_z_steps=cfg["z"][2], dictionary_resolution_deg=cfg["res"],
+              dictionary_indexing_batch_size=cfg["bs"], orientation_index="global")
+    for _ in range(args.warmup):
+        spatial_fft_pc_fitter(mp, pats, **kw)
+    torch.cuda.synchronize()
+    l0 = _capi.launch_count
+    with ClockSampler(int(dev.index or 0)) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            pc, q = spatial_fft_pc_fitter(mp, pats, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3 / args.steps
+    launches = (_capi.launch_count - l0) // args.steps
+    n_dict = sample_ori_fz_laue_angle(11, cfg["res"], dev).shape[0]
+    H, W = cfg["det"]
+    pix, pad, (hp, wp) = F.get_3D_pixel_coords_with_periphery((H, W), torch.device("cpu"), *cfg["x"], *cfg["y"], 1)
+    z_steps = cfg["z"][2]
+    evals = n_dict * z_steps * cfg["n"] * hp * wp  # (orientation, pc_z, pattern, pc_x / pc_y shift) scores
+
+    # stages of one chunk of 1024 orientations
+    rays = F._rays_soa(pix.double().numpy(), 0.55, 70.0, 0.0, (H, W), dev)
+    quats = sample_ori_fz_laue_angle(11, cfg["res"], dev)[:cfg["bs"]].float().contiguous()
+    n = quats.shape[0]
+    sims = torch.empty((n, hp * wp), device=dev)
+    padded = torch.randn((cfg["n"], hp, wp), device=dev)
+    pat_fft = torch.fft.rfft2(padded).conj()
+    mp_b = _master_pattern_tensor(mp, 1, dev)
+    best = torch.zeros((cfg["n"], hp, wp), device=dev)
+    best_i = torch.zeros((cfg["n"], hp, wp), dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    state = {}
+
+    def st_project():
+        kernels.project(mp_b, rays, quats, RowBuffers(f32=sims), subtract_mean=False)
+
+    def st_rfft():
+        state["spec"] = torch.fft.rfft2(sims.view(n, hp, wp))
+
+    def st_corr():
+        state["corr"] = torch.fft.irfft2(state["spec"][:, None] * pat_fft[None], s=(hp, wp)).contiguous()
+
+    def st_reduce():
+        _capi.call("ebsd_pcfit_reduce", state["corr"].data_ptr(), n, cfg["n"], hp, wp, 0, best.data_ptr(),
+                   best_i.data_ptr(), stream)
+
+    stages = {}
+    for name, fn in (("project", st_project), ("rfft2", st_rfft), ("product_irfft2", st_corr),
+                     ("reduce", st_reduce)):
+        fn()
+        ts = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        stages[name] = statistics.median(ts)
+    peaks, src = _peaks()
+    red_bytes = n * cfg["n"] * hp * wp * 4 + 2 * cfg["n"] * hp * wp * 12  # correlations + best / index read-write
+    red_gbs = red_bytes / (stages["reduce"] / 1e3) / 1e9
+    line = {
+        "metric": "pattern-centre fits/s (spatial FFT search)", "value": 1.0 / secs, "unit": "fits/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": cfg["name"] + " (%d orientations)" % n_dict,
+                   "l2": "correlation tensors of 0.4 GB per chunk, larger than L2"},
+        "gpu_launches": launches,
+        "scores_per_s": evals / secs,
+        "fit": {"pc": [float(v) for v in pc.cpu()], "simulated_pc": list(cfg["pc"])},
+        "chunk_stages_ms": stages,
+        "roofline": {"bound": "hbm", "kernel": "k_pcfit_reduce", "achieved": red_gbs, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": red_gbs / peaks["hbm_gbs"], "traffic": None, "peak_source": src},
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import di_oracle as O
+
+        q64 = quats[:64].double().cpu().numpy()
+        t0 = time.perf_counter()
+        O.spatial_fft_pc_fit(mp_t.double().cpu().numpy(), pats[:, :, :, :].cpu().numpy(), q64, pc_x_min=cfg["x"][0],
+                             pc_x_max=cfg["x"][1], pc_y_min=cfg["y"][0], pc_y_max=cfg["y"][1], pc_z_min=0.55,
+                             pc_z_max=0.55, pc_z_steps=1, batch_size=64)
+        t_cpu = (time.perf_counter() - t0) * (n_dict / 64) * z_steps
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "fits/s", "cores": 1, "kind": "port",
+                                "sample": "oracle (NumPy float64) on 64 orientations x 1 pc_z step, extrapolated to "
+                                          "%d orientations x %d steps" % (n_dict, z_steps)}
+    print(json.dumps(line), flush=True)
+
+
 BATCHED = dict(maps=48, q_min=1000, q_max=200000, detectors=((60, 60), (80, 80), (128, 128), (160, 160)),
                phases=((11, 0.5), (9, 0.615), (5, 0.88)), mp=1001, counts=100.0, seed=3)
 
@@ -918,6 +1042,7 @@ def main():
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (config 3) instead")
     ap.add_argument("--refine", action="store_true", help="time orientation grid refinement after DI instead")
     ap.add_argument("--preprocess", action="store_true", help="time pattern preprocessing (clean + NLPAR) instead")
+    ap.add_argument("--pcfit", action="store_true", help="time pattern-centre fitting instead")
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--max-angle", type=float, default=16.0)
     ap.add_argument("--fallback-ratio", type=float, default=0.95)
@@ -935,6 +1060,8 @@ def main():
         run_refine(args, wl)
     elif args.preprocess:
         run_preprocess(args)
+    elif args.pcfit:
+        run_pcfit(args)
     else:
         run_ours(args, wl)
 

@@ -61,8 +61,21 @@ __global__ void k_pcfit_reduce(const float* __restrict__ corr, int n, int n_pat,
   const int64_t stride = total;
   float vmax = -INFINITY;
   int arg = 0;
-  for (int d = 0; d < n; ++d) {
-    const float v = __ldg(src + d * stride);
+  // 8 independent loads in flight per thread; the first maximum wins ties
+  int d = 0;
+  for (; d + 8 <= n; d += 8) {
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __ldg(src + (int64_t)(d + k) * stride);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if (v[k] > vmax) {
+        vmax = v[k];
+        arg = d + k;
+      }
+  }
+  for (; d < n; ++d) {
+    const float v = __ldg(src + (int64_t)d * stride);
     if (v > vmax) {
       vmax = v;
       arg = d;
