@@ -29,7 +29,7 @@ import torch
 from torch import Tensor
 
 from .. import kernels
-from ..engine import Searcher, SearchConfig, default_budget
+from ..engine import Searcher, SearchConfig, default_budget, wave_query_tiles
 from ..kernels import RowBuffers, round_up
 from ..s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
 
@@ -87,16 +87,74 @@ def _pattern_source(experiment_patterns, device):
     return pats
 
 
+# match waves per query chunk when the patterns stream from pinned host memory
+HOST_CHUNK_WAVES = 4
+
+
+class _QueryFill:
+    """Query rows of patterns [q0, q1) (K2). Device patterns go straight to
+    the prep kernel. Host patterns are first copied into one of two device
+    staging buffers. When they are pinned, `prefetch(q0, q1)` (called by the
+    engine once the current chunk is filled) starts the next chunk's copy on
+    a side stream, so the host-to-device transfer runs under the current
+    chunk's match kernels."""
+
+    def __init__(self, pats: Tensor, binning: int, pix_index, n_pix: int, subtract_mean: bool, device):
+        self.pats, self.binning, self.pix_index, self.n_pix = pats, binning, pix_index, n_pix
+        self.subtract_mean, self.device = subtract_mean, device
+        self.host = pats.device.type != "cuda"
+        self.copy_stream = torch.cuda.Stream(device) if self.host and pats.is_pinned() else None
+        self.slots = [None, None]      # staging buffers
+        self.slot_free = [None, None]  # event: the last prep reading the slot is done
+        self.next_slot = 0
+        self.pending = {}              # (q0, q1) -> (slot, copy-done event)
+
+    def _stage(self, q0: int, q1: int, stream) -> tuple:
+        slot = self.next_slot
+        self.next_slot ^= 1
+        n = q1 - q0
+        buf = self.slots[slot]
+        if buf is None or buf.shape[0] < n:
+            buf = torch.empty((n,) + tuple(self.pats.shape[1:]), dtype=self.pats.dtype, device=self.device)
+            self.slots[slot] = buf
+        if self.slot_free[slot] is not None:
+            stream.wait_event(self.slot_free[slot])
+        with torch.cuda.stream(stream):
+            buf[:n].copy_(self.pats[q0:q1], non_blocking=True)
+        if stream is self.copy_stream:
+            buf.record_stream(stream)
+        done = torch.cuda.Event()
+        done.record(stream)
+        return slot, done
+
+    def prefetch(self, q0: int, q1: int) -> None:
+        if self.copy_stream is not None and (q0, q1) not in self.pending and len(self.pending) < 1:
+            self.pending[(q0, q1)] = self._stage(q0, q1, self.copy_stream)
+
+    def __call__(self, q0: int, q1: int, bufs: RowBuffers) -> None:
+        if not self.host:
+            kernels.prep_patterns(self.pats[q0:q1].contiguous(), bufs, self.binning, self.pix_index, self.n_pix,
+                                  self.subtract_mean)
+            return
+        cur = torch.cuda.current_stream(self.device)
+        if (q0, q1) in self.pending:
+            slot, done = self.pending.pop((q0, q1))
+            cur.wait_event(done)
+        else:
+            for key, (slot, done) in list(self.pending.items()):  # a prefetch that was not used
+                cur.wait_event(done)
+                self.slot_free[slot] = done
+                del self.pending[key]
+            slot, _ = self._stage(q0, q1, cur)
+        kernels.prep_patterns(self.slots[slot][:q1 - q0], bufs, self.binning, self.pix_index, self.n_pix,
+                              self.subtract_mean)
+        free = torch.cuda.Event()
+        free.record(cur)
+        self.slot_free[slot] = free
+
+
 def _query_fill(pats: Tensor, binning: int, pix_index, n_pix: int, subtract_mean: bool, device):
-    host = pats.device.type != "cuda"
-
-    def fill(q0: int, q1: int, bufs: RowBuffers):
-        chunk = pats[q0:q1]
-        if host:
-            chunk = chunk.to(device, non_blocking=chunk.is_pinned())
-        kernels.prep_patterns(chunk.contiguous(), bufs, binning, pix_index, n_pix, subtract_mean)
-
-    return fill
+    return _QueryFill(pats, binning, pix_index, n_pix, subtract_mean, device)
 
 
 def _store(experiment_patterns, phase: int, ori: Tensor, idx: Tensor, val: Tensor, out_dtype):
@@ -146,8 +204,14 @@ def dictionary_index_orientations(
     subtract = bool(subtract_exp_pat_mean) if experiment_chunk_size > n_q else True
     cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=similarity,
                        workspace_bytes=workspace_bytes)
+    pats_host = experiment_patterns.patterns
+    stream_host = pats_host.device.type != "cuda" and pats_host.is_pinned()
     for i, mp in enumerate(master_patterns):
         dev = _device(mp, device)
+        if stream_host:
+            # chunks of a few match waves, so each chunk's copy runs under the
+            # previous chunk's match and only the first copy is exposed
+            cfg.max_query_chunk = HOST_CHUNK_WAVES * wave_query_tiles(dev) * kernels.TILE_Q
         ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_degrees, dev, permute=True)
         rays = _unit_rays_soa(geometry, virtual_binning, signal_mask, dev)
         mp_t = _master_pattern_tensor(mp, virtual_binning, dev)

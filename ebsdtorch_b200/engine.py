@@ -46,6 +46,9 @@ class SearchConfig:
     workspace_bytes: Optional[int] = None
     query_chunk: Optional[int] = None
     dict_chunk: Optional[int] = None
+    # upper bound on the planned query chunk (host-resident patterns stream in
+    # several chunks so that copies overlap the matching)
+    max_query_chunk: Optional[int] = None
     # match launch shape (the batch autotuner sets these): dictionary rows per
     # CTA tile (0 = 256), dictionary ranges per query tile (0 = automatic),
     # query tiles per launch (0 = one wave), or one persistent launch per
@@ -205,6 +208,8 @@ class Searcher:
             qchunk = round_up(self.cfg.query_chunk, TILE_Q)
         else:
             qchunk = max(TILE_Q, left // qrow // TILE_Q * TILE_Q)
+            if self.cfg.max_query_chunk:
+                qchunk = min(qchunk, round_up(self.cfg.max_query_chunk, TILE_Q))
         self.query_chunk = min(qchunk, round_up(self.n_queries, TILE_Q))
         if left < self.query_chunk * qrow and not self.cfg.query_chunk:
             raise MemoryError(
@@ -263,6 +268,13 @@ class Searcher:
                 q1 = min(Q, q0 + qc)
                 nq = q1 - q0
                 fill_queries(q0, q1, q_rows.buffers(0, nq))
+                # the next chunk's host-to-device copy runs under this chunk's matching
+                prefetch = getattr(fill_queries, "prefetch", None)
+                if prefetch is not None:
+                    if q1 < Q:
+                        prefetch(q1, min(Q, q1 + qc))
+                    elif ci + 1 < n_dchunks and qc < Q:
+                        prefetch(0, min(Q, qc))
                 for s0 in range(0, nq, qm):
                     s1 = min(nq, s0 + qm)
                     ns = s1 - s0

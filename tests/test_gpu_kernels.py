@@ -347,3 +347,32 @@ def test_disorientation_matches_reference(golden, laue):
     a = disori_angle_laue(torch.from_numpy(g[f"q1_{laue}"]).to(DEV), torch.from_numpy(g[f"q2_{laue}"]).to(DEV),
                           laue, laue)
     assert np.abs(a.cpu().numpy() - g[f"ang_{laue}"]).max() < 2e-3  # fp32 acos near 1
+
+
+@pytest.mark.parametrize("dict_chunk", [None, 512])
+def test_host_patterns_prefetch_matches_device_patterns(dict_chunk):
+    """Pinned host patterns, copied a query chunk ahead on a side stream while
+    the previous chunk is matched (one and several dictionary chunks, a
+    ragged last query chunk), give exactly the results of the same patterns
+    resident on the device."""
+    from ebsdtorch_b200 import kernels
+    from ebsdtorch_b200.ebsd.indexing import _query_fill
+    from ebsdtorch_b200.engine import Searcher, SearchConfig
+
+    p, nd, nq, k = 16 * 16, 1300, 700, 4
+    d = _rows(nd, p, 15)
+    pats = (d[np.arange(nq) % nd] + 0.4 * _rows(nq, p, 16)).reshape(nq, 16, 16).astype(np.float32)
+    dt = torch.from_numpy(d).float().to(DEV)
+
+    def fill_d(d0, d1, bufs):
+        kernels.prep_patterns(dt[d0:d1].reshape(d1 - d0, 1, p), bufs, subtract_mean=True)
+
+    out = []
+    for src in (torch.from_numpy(pats).to(DEV), torch.from_numpy(pats).pin_memory()):
+        cfg = SearchConfig(rescore_k=16, dict_chunk=dict_chunk, query_chunk=256)
+        fill = _query_fill(src, 1, None, p, True, torch.device(DEV))
+        out.append(Searcher(nd, nq, p, k, cfg, DEV).run(fill_d, fill))
+        if src.device.type == "cpu":
+            assert fill.copy_stream is not None and not fill.pending
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
