@@ -9,8 +9,10 @@
 // irfft2 output, read through fftshift) and its index, folded into the
 // running best of the current pc_z: best = max(best, chunk max), index
 // replaced where the chunk's maximum equals the new best (fitting.py:498-507).
-// The correlation tensor is read once, coalesced along the detector rows.
+// The correlation tensor is read once, coalesced along the detector rows,
+// each output's dictionary chunk split over 4 threads.
 #include <algorithm>
+#include <climits>
 
 #include "common.cuh"
 
@@ -46,39 +48,61 @@ __global__ void __launch_bounds__(kFitThreads) k_pcfit_prep(const float* __restr
   }
 }
 
-__global__ void k_pcfit_reduce(const float* __restrict__ corr, int n, int n_pat, int hp, int wp, int64_t index_base,
-                               float* __restrict__ best, int64_t* __restrict__ best_index) {
+constexpr int kRedPos = 64;     // (pattern, shift) outputs per CTA
+constexpr int kRedSplits = 4;   // dictionary slices per output, one per 64 threads
+
+// Thread (slice, position): the maximum over its slice of the chunk, 8 loads
+// in flight; the 4 slices combine in shared memory (the larger value wins,
+// the smaller dictionary index on ties, so the first maximum wins).
+__global__ void __launch_bounds__(kRedPos * kRedSplits) k_pcfit_reduce(const float* __restrict__ corr, int n,
+                                                                       int n_pat, int hp, int wp,
+                                                                       int64_t index_base, float* __restrict__ best,
+                                                                       int64_t* __restrict__ best_index) {
+  __shared__ float sv[kRedSplits][kRedPos];
+  __shared__ int sa[kRedSplits][kRedPos];
   const int64_t plane = (int64_t)hp * wp;
   const int64_t total = (int64_t)n_pat * plane;
-  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= total) return;
-  const int b = (int)(t / plane);
-  const int rem = (int)(t - (int64_t)b * plane);
-  const int y = rem / wp, x = rem - y * wp;
-  // fftshift: output (y, x) holds input ((y - hp / 2) mod hp, (x - wp / 2) mod wp)
-  const int sy = (y - hp / 2 + hp) % hp, sx = (x - wp / 2 + wp) % wp;
-  const float* src = corr + (int64_t)b * plane + (int64_t)sy * wp + sx;
-  const int64_t stride = total;
+  const int pos = threadIdx.x % kRedPos, slice = threadIdx.x / kRedPos;
+  const int64_t t = blockIdx.x * (int64_t)kRedPos + pos;
   float vmax = -INFINITY;
-  int arg = 0;
-  // 8 independent loads in flight per thread; the first maximum wins ties
-  int d = 0;
-  for (; d + 8 <= n; d += 8) {
-    float v[8];
+  int arg = INT_MAX;
+  if (t < total) {
+    const int b = (int)(t / plane);
+    const int rem = (int)(t - (int64_t)b * plane);
+    const int y = rem / wp, x = rem - y * wp;
+    // fftshift: output (y, x) holds input ((y - hp / 2) mod hp, (x - wp / 2) mod wp)
+    const int sy = (y - hp / 2 + hp) % hp, sx = (x - wp / 2 + wp) % wp;
+    const float* src = corr + (int64_t)b * plane + (int64_t)sy * wp + sx;
+    const int d0 = (int)((int64_t)n * slice / kRedSplits), d1 = (int)((int64_t)n * (slice + 1) / kRedSplits);
+    int d = d0;
+    for (; d + 8 <= d1; d += 8) {
+      float v[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = __ldg(src + (int64_t)(d + k) * stride);
+      for (int k = 0; k < 8; ++k) v[k] = __ldg(src + (int64_t)(d + k) * total);
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
-      if (v[k] > vmax) {
-        vmax = v[k];
-        arg = d + k;
+      for (int k = 0; k < 8; ++k)
+        if (v[k] > vmax) {
+          vmax = v[k];
+          arg = d + k;
+        }
+    }
+    for (; d < d1; ++d) {
+      const float v = __ldg(src + (int64_t)d * total);
+      if (v > vmax) {
+        vmax = v;
+        arg = d;
       }
+    }
   }
-  for (; d < n; ++d) {
-    const float v = __ldg(src + (int64_t)d * stride);
-    if (v > vmax) {
+  sv[slice][pos] = vmax;
+  sa[slice][pos] = arg;
+  __syncthreads();
+  if (slice != 0 || t >= total) return;
+  for (int s = 1; s < kRedSplits; ++s) {
+    const float v = sv[s][pos];
+    if (v > vmax || (v == vmax && sa[s][pos] < arg)) {
       vmax = v;
-      arg = d;
+      arg = sa[s][pos];
     }
   }
   const float nb = fmaxf(best[t], vmax);
@@ -109,8 +133,8 @@ extern "C" int ebsd_pcfit_reduce(const float* corr, int n, int n_patterns, int p
   EBSD_ARG_CHECK(n >= 1 && n_patterns >= 1 && padded_h >= 1 && padded_w >= 1, "ebsd_pcfit_reduce: bad sizes");
   const int64_t total = (int64_t)n_patterns * padded_h * padded_w;
   EBSD_ARG_CHECK(total * n < ((int64_t)1 << 62), "ebsd_pcfit_reduce: too large");
-  k_pcfit_reduce<<<ceil_div(total, 256), 256, 0, as_stream(stream)>>>(corr, n, n_patterns, padded_h, padded_w,
-                                                                    index_base, best, best_index);
+  k_pcfit_reduce<<<ceil_div(total, kRedPos), kRedPos * kRedSplits, 0, as_stream(stream)>>>(
+      corr, n, n_patterns, padded_h, padded_w, index_base, best, best_index);
   EBSD_LAUNCH_CHECK();
   return 0;
 }

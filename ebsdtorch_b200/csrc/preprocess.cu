@@ -418,20 +418,36 @@ constexpr int kNlPairs = kNlMaxOffsets / (kNlThreads / (kNlTile * kNlTile));  //
 // one offset land in distinct banks as well.
 __host__ __device__ constexpr int nl_plane(int halo) { return (kNlTile + 2 * halo) * kNlPitch + 1; }
 
-// T[q * plane + yy * pitch + xx] = data[point (y0 - halo + yy, x0 - halo + xx), p0 + q]
-// by 4-byte cp.async; zero outside the scan (the reference zero-pads the
-// data, nlpar.py:56-61) and beyond the last pixel. Completes before return.
+constexpr int kNlMaxRows = (kNlTile + 2 * kNlMaxRad) * (kNlTile + 2 * kNlMaxRad);
+
+// Per CTA, once: for each row (yy, xx) of the staged tile + halo, the scan
+// point it holds (-1 outside the scan) and its shared-memory offset.
 template <int HALO>
-__device__ __forceinline__ void nl_load_chunk(float* T, const float* __restrict__ data, int hs, int ws, int64_t ld,
-                                              int y0, int x0, int p0, int np) {
-  constexpr int side = kNlTile + 2 * HALO, plane = nl_plane(HALO);
-  for (int t = threadIdx.x; t < side * side * kNlChunk; t += blockDim.x) {
-    const int row = t / kNlChunk, q = t - row * kNlChunk;
-    const int yy = row / side, xx = row - yy * side;
+__device__ __forceinline__ void nl_rows(int* src_s, int* dst_s, int hs, int ws, int y0, int x0) {
+  constexpr int side = kNlTile + 2 * HALO;
+  for (int r = threadIdx.x; r < side * side; r += blockDim.x) {
+    const int yy = r / side, xx = r - (r / side) * side;
     const int y = y0 - HALO + yy, x = x0 - HALO + xx;
-    float* dst = T + q * plane + yy * kNlPitch + xx;
-    if (q < np && y >= 0 && y < hs && x >= 0 && x < ws)
-      cp_async4(dst, data + ((int64_t)y * ws + x) * ld + p0 + q);
+    src_s[r] = (y >= 0 && y < hs && x >= 0 && x < ws) ? y * ws + x : -1;
+    dst_s[r] = yy * kNlPitch + xx;
+  }
+}
+
+// T[q * plane + yy * pitch + xx] = data[point (y0 - halo + yy, x0 - halo + xx), p0 + q]
+// by 4-byte cp.async (lane = pixel q, one row per warp and step); zero
+// outside the scan (the reference zero-pads the data, nlpar.py:56-61) and
+// beyond the last pixel. Completes before return.
+template <int HALO>
+__device__ __forceinline__ void nl_load_chunk(float* T, const float* __restrict__ data, int64_t ld,
+                                              const int* src_s, const int* dst_s, int p0, int np) {
+  constexpr int side = kNlTile + 2 * HALO, plane = nl_plane(HALO);
+  static_assert(kNlChunk == 32, "one warp lane per pixel of the chunk");
+  const int q = threadIdx.x & 31;
+  for (int row = threadIdx.x >> 5; row < side * side; row += blockDim.x >> 5) {
+    const int src = src_s[row];
+    float* dst = T + q * plane + dst_s[row];
+    if (src >= 0 && q < np)
+      cp_async4(dst, data + (int64_t)src * ld + p0 + q);
     else
       *dst = 0.f;
   }
@@ -458,24 +474,29 @@ __device__ __forceinline__ void nl_load_offsets(int* off_s, unsigned char* bad_s
 template <int HALO>
 __global__ void __launch_bounds__(kNlThreads, 3) k_nlpar_dists(const float* __restrict__ data, int hs, int ws,
                                                            int n_pix, int64_t ld, const int* __restrict__ offsets,
-                                                           int o0, int n_off, int n_off_total,
+                                                           int o0, int n_off, int per_group, int n_off_total,
                                                            float* __restrict__ dists) {
   constexpr int plane = nl_plane(HALO);
   extern __shared__ __align__(16) float T[];
   __shared__ int off_s[kNlMaxOffsets];
   __shared__ unsigned char bad_s[kNlMaxOffsets];
+  __shared__ int src_s[kNlMaxRows], dst_s[kNlMaxRows];
+  // this CTA's group of offsets (blockIdx.y) within the launch's block
+  o0 += blockIdx.y * per_group;
+  n_off = min(per_group, n_off - (int)blockIdx.y * per_group);
   const int tiles_x = (ws + kNlTile - 1) / kNlTile;
   const int y0 = (blockIdx.x / tiles_x) * kNlTile, x0 = (blockIdx.x % tiles_x) * kNlTile;
   const int pt = threadIdx.x % (kNlTile * kNlTile), ob = threadIdx.x / (kNlTile * kNlTile);
   const int self = (pt / kNlTile + HALO) * kNlPitch + pt % kNlTile + HALO;
   const int nj = (n_off - ob + 3) / 4;  // offsets of this thread
   nl_load_offsets(off_s, bad_s, offsets, o0, n_off, HALO);
+  nl_rows<HALO>(src_s, dst_s, hs, ws, y0, x0);
   float acc[kNlPairs];
 #pragma unroll
   for (int j = 0; j < kNlPairs; ++j) acc[j] = 0.f;
   for (int p0 = 0; p0 < n_pix; p0 += kNlChunk) {
     __syncthreads();
-    nl_load_chunk<HALO>(T, data, hs, ws, ld, y0, x0, p0, min(kNlChunk, n_pix - p0));
+    nl_load_chunk<HALO>(T, data, ld, src_s, dst_s, p0, min(kNlChunk, n_pix - p0));
     __syncthreads();
     // two halves of 16 pixels keep 16 own values in registers (3 CTAs per SM)
 #pragma unroll 1
@@ -514,19 +535,24 @@ __global__ void __launch_bounds__(kNlThreads, 3) k_nlpar_dists(const float* __re
 // immediate offsets feed 8 FMAs.
 template <int HALO>
 __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __restrict__ data, int hs, int ws,
-                                                             int n_pix, int64_t ld, const int* __restrict__ offsets,
-                                                             int o0, int n_off, int n_off_total,
-                                                             const float* __restrict__ weights, int accumulate,
-                                                             float* __restrict__ out, int64_t ld_out) {
+                                                             int n_pix, int pix_per_split, int64_t ld,
+                                                             const int* __restrict__ offsets, int o0, int n_off,
+                                                             int n_off_total, const float* __restrict__ weights,
+                                                             int accumulate, float* __restrict__ out,
+                                                             int64_t ld_out) {
   constexpr int plane = nl_plane(HALO);
   extern __shared__ __align__(16) float T[];
   __shared__ int off_s[kNlMaxOffsets];
   __shared__ unsigned char bad_s[kNlMaxOffsets];
+  __shared__ int src_s[kNlMaxRows], dst_s[kNlMaxRows];
   float* w_s = T + ((kNlChunk * plane + 3) & ~3);  // [o][64 points], 16-byte aligned
   const int tiles_x = (ws + kNlTile - 1) / kNlTile;
   const int y0 = (blockIdx.x / tiles_x) * kNlTile, x0 = (blockIdx.x % tiles_x) * kNlTile;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // this CTA's range of pattern pixels (blockIdx.y); outputs are disjoint
+  const int pix_begin = blockIdx.y * pix_per_split, pix_end = min(n_pix, pix_begin + pix_per_split);
   nl_load_offsets(off_s, bad_s, offsets, o0, n_off, HALO);
+  nl_rows<HALO>(src_s, dst_s, hs, ws, y0, x0);
   __syncthreads();
   for (int t = threadIdx.x; t < kNlTile * kNlTile * n_off; t += blockDim.x) {
     const int pt = t % (kNlTile * kNlTile), o = t / (kNlTile * kNlTile);
@@ -537,10 +563,10 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __res
   }
   const int y = y0 + wid;
   const float4* w4 = reinterpret_cast<const float4*>(w_s) + wid * 2;
-  for (int p0 = 0; p0 < n_pix; p0 += kNlChunk) {
-    const int np = min(kNlChunk, n_pix - p0);
+  for (int p0 = pix_begin; p0 < pix_end; p0 += kNlChunk) {
+    const int np = min(kNlChunk, pix_end - p0);
     __syncthreads();
-    nl_load_chunk<HALO>(T, data, hs, ws, ld, y0, x0, p0, np);
+    nl_load_chunk<HALO>(T, data, ld, src_s, dst_s, p0, np);
     __syncthreads();
     if (y >= hs) continue;
     const float* base = T + lane * plane + (wid + HALO) * kNlPitch + HALO;
@@ -696,6 +722,19 @@ __global__ void k_nlpar_softmax(float* __restrict__ w, int hs, int ws, int K, co
   for (int o = lane; o < K; o += 32) r[o] = expf(r[o] - mx) / sum;
 }
 
+// Second grid dimension, so that small scans still fill the GPU: offset
+// groups (distances) or pixel ranges (average), each CTA writing disjoint
+// outputs. Aim for `waves` waves at the kernel's occupancy. A distance CTA
+// reloads the whole tile for fewer offsets, so distances split only to fill
+// one wave; the average splits its pixel range, which costs nothing extra.
+static int nl_splits(const void* func, size_t smem, int tiles, int max_splits, int waves) {
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, kNlThreads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int64_t want = (int64_t)waves * device_sm_count() * per_sm;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(max_splits, (want + tiles - 1) / tiles));
+}
+
 template <int HALO>
 static int nl_launch(bool average, const float* data, int hs, int ws, int n_pix, int64_t ld, const int* offsets,
                      int o0, int n_off, int n_off_total, float* dists, const float* weights, int accumulate,
@@ -705,14 +744,24 @@ static int nl_launch(bool average, const float* data, int hs, int ws, int n_pix,
   if (!average) {
     EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_nlpar_dists<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)chunk_bytes));
-    k_nlpar_dists<HALO><<<tiles, kNlThreads, chunk_bytes, s>>>(data, hs, ws, n_pix, ld, offsets, o0, n_off,
-                                                               n_off_total, dists);
+    // groups of at least 16 offsets
+    const int groups = nl_splits((const void*)k_nlpar_dists<HALO>, chunk_bytes, tiles, std::max(1, n_off / 16), 1);
+    const int per_group = ceil_div(n_off, groups);
+    const int n_groups = ceil_div(n_off, per_group);
+    k_nlpar_dists<HALO><<<dim3(tiles, n_groups), kNlThreads, chunk_bytes, s>>>(data, hs, ws, n_pix, ld, offsets, o0,
+                                                                              n_off, per_group, n_off_total, dists);
   } else {
     const size_t smem = ((chunk_bytes + 15) & ~(size_t)15) + (size_t)kNlTile * kNlTile * n_off * sizeof(float);
     EBSD_CUDA_CHECK(
         cudaFuncSetAttribute(k_nlpar_average<HALO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_nlpar_average<HALO><<<tiles, kNlThreads, smem, s>>>(data, hs, ws, n_pix, ld, offsets, o0, n_off, n_off_total,
-                                                          weights, accumulate, out, ld_out);
+    // ranges of whole chunks, at least 4 chunks each
+    const int n_chunks = ceil_div(n_pix, kNlChunk);
+    const int splits = nl_splits((const void*)k_nlpar_average<HALO>, smem, tiles, std::max(1, n_chunks / 4), 3);
+    const int pix_per_split = ceil_div(n_chunks, splits) * kNlChunk;
+    const int n_splits = ceil_div(n_pix, pix_per_split);
+    k_nlpar_average<HALO><<<dim3(tiles, n_splits), kNlThreads, smem, s>>>(data, hs, ws, n_pix, pix_per_split, ld,
+                                                                         offsets, o0, n_off, n_off_total, weights,
+                                                                         accumulate, out, ld_out);
   }
   EBSD_LAUNCH_CHECK();
   return 0;
