@@ -493,6 +493,29 @@ def run_learned(args, wl):
         torch.cuda.synchronize()
     secs = e0.elapsed_time(e1) / 1e3 / args.steps
     learned_idx = exp.raw_indexing_indices[0][:, 0].clone()
+    # end to end: patterns in pinned host memory, orientations read back
+    e2e = None
+    if not args.no_e2e:
+        exp_h = ExperimentPatterns(pats.cpu().pin_memory())
+        ori_host = torch.empty((wl["Q"], 4), dtype=torch.float32).pin_memory()
+        torch.manual_seed(0)
+        learned_dictionary_index(mp, geom, exp_h, model, dictionary_resolution_degrees=wl["res"],
+                                 max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
+                                 fallback_ratio=args.fallback_ratio, stage_margin=args.stage_margin)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            torch.manual_seed(0)
+            learned_dictionary_index(mp, geom, exp_h, model, dictionary_resolution_degrees=wl["res"],
+                                     max_angle_deg=args.max_angle, pyramid_resolutions_deg=pyramid,
+                                     fallback_ratio=args.fallback_ratio, stage_margin=args.stage_margin)
+            ori_host.copy_(exp_h.orientations.float(), non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e = {"value": wl["Q"] / (e0.elapsed_time(e1) / 1e3 / args.steps), "unit": UNIT,
+               "h2d_bytes_per_step": int(pats.numel() * pats.element_size()),
+               "d2h_bytes_per_step": int(ori_host.numel() * 4), "host_memory": "pinned"}
+        del exp_h
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
 
     perr = torch.rad2deg(disori_angle_laue(exp.proposals.contiguous(), truth.float().contiguous(), 11, 11))
@@ -534,6 +557,7 @@ def run_learned(args, wl):
                     "stage_seconds": st.seconds, "train_seconds": t_train,
                     "final_train_loss": float(losses[-100:].mean()),
                     "plain_di_seconds_same_gpu": t_full, "speedup_vs_plain_di_bf16": t_full / secs},
+        "e2e": e2e,
         "clocks": clocks.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -123,7 +123,7 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     best n_rescore in FP32. Writes raw_indexing_results /
     orientations like dictionary_index_orientations; returns timings and
     counts."""
-    from .ebsd.indexing import _device, _master_pattern_tensor, _unit_rays_soa
+    from .ebsd.indexing import _device, _master_pattern_tensor, _query_fill, _unit_rays_soa
 
     sec = {}
     dev = _device(master_pattern, device)
@@ -153,10 +153,14 @@ def learned_dictionary_index(master_pattern, geometry, experiment_patterns, mode
     q_f32 = torch.empty((Q, P), dtype=torch.float32, device=dev)
     q_norm = torch.empty(Q, dtype=torch.float32, device=dev)
     proposals = torch.empty((Q, 4), dtype=torch.float32, device=dev)
+    # host patterns: the next batch's copy runs on a side stream under this
+    # batch's network inference
+    fill = _query_fill(pats if pats.dtype in kernels.PATTERN_DTYPES else pats.float(), 1, None, P, True, dev)
     for b0 in range(0, Q, batch):
         b1 = min(Q, b0 + batch)
-        chunk = pats[b0:b1].to(dev, non_blocking=True).float().contiguous()
-        kernels.prep_patterns(chunk, RowBuffers(f32=q_f32[b0:b1], norm=q_norm[b0:b1]))
+        fill(b0, b1, RowBuffers(f32=q_f32[b0:b1], norm=q_norm[b0:b1]))
+        if b1 < Q:
+            fill.prefetch(b1, min(Q, b1 + batch))
         nb = b1 - b0
         nb_pad = -(-nb // 128) * 128
         x = torch.zeros((nb_pad, H, W), dtype=torch.float32, device=dev)
