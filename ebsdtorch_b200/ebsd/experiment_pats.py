@@ -114,8 +114,8 @@ class ExperimentPatterns(Module):
         """Non-local pattern averaging over the 2D scan."""
         if len(self.spatial_shape) != 2:
             raise ValueError(f"NLPAR only supported for 2D EBSD scans, got {self.spatial_shape}")
-        self.patterns = nlpar(self.patterns.view(tuple(self.spatial_shape) + tuple(self.pattern_shape)), k_rad=k_rad,
-                              coeff=coeff).view(-1, *self.pattern_shape)
+        self.patterns = nlpar(self.patterns.reshape(tuple(self.spatial_shape) + tuple(self.pattern_shape)),
+                              k_rad=k_rad, coeff=coeff).reshape(-1, *self.pattern_shape)
 
     def get_patterns(self, indices: Tensor, binning: int):
         """Patterns at `indices`, b x b average pooled (experiment_pats.py:318-346)."""
