@@ -20,6 +20,7 @@
 namespace ebsd {
 
 constexpr int kRowThreads = 512;
+constexpr int kProjIlp = 2;  // independent pixels per projector thread and step
 constexpr int kMaxRowPix = 57344;  // 224 KiB of fp32 in shared memory
 
 struct RowOut {
@@ -100,7 +101,7 @@ __device__ void finalize_row(const float* row, int n, int subtract_mean, float p
   }
 }
 
-__global__ void __launch_bounds__(kRowThreads) k_project(
+__global__ void __launch_bounds__(kRowThreads, 2) k_project(
     const float* __restrict__ mp, int mp_h, int mp_w2, const float* __restrict__ rays, int n_pix,
     const float4* __restrict__ quats, int64_t n_rows, int subtract_mean, RowOut o) {
   extern __shared__ float row[];
@@ -112,12 +113,35 @@ __global__ void __launch_bounds__(kRowThreads) k_project(
   for (int64_t r = blockIdx.x; r < n_rows; r += gridDim.x) {
     const float4 q = quats[r];
     float part = 0.0f;
-    for (int p = threadIdx.x; p < n_pix; p += blockDim.x) {
-      const float3 v = rotate(q, __ldg(rx + p), __ldg(ry + p), __ldg(rz + p));
-      const float2 uv = lambert_side_by_side(v.x, v.y, v.z);
-      const float val = sample_border(mp, mp_h, mp_w2, uv.x, uv.y);
-      row[p] = val;
-      part += val;
+    // kProjIlp pixels per thread and step, their master-pattern gathers
+    // issued together: the projector is bound by the gather latency through
+    // L2, and independent gathers in flight hide it
+    for (int p0 = threadIdx.x; p0 < n_pix; p0 += kProjIlp * blockDim.x) {
+      BorderTaps t[kProjIlp];
+#pragma unroll
+      for (int k = 0; k < kProjIlp; ++k) {
+        const int p = min(p0 + k * (int)blockDim.x, n_pix - 1);
+        const float3 v = rotate(q, __ldg(rx + p), __ldg(ry + p), __ldg(rz + p));
+        const float2 uv = lambert_side_by_side(v.x, v.y, v.z);
+        t[k] = border_taps(mp_h, mp_w2, uv.x, uv.y);
+      }
+      float g[kProjIlp][4];
+#pragma unroll
+      for (int k = 0; k < kProjIlp; ++k) {
+        g[k][0] = __ldg(mp + t[k].i00);
+        g[k][1] = __ldg(mp + t[k].i01);
+        g[k][2] = __ldg(mp + t[k].i10);
+        g[k][3] = __ldg(mp + t[k].i11);
+      }
+#pragma unroll
+      for (int k = 0; k < kProjIlp; ++k) {
+        const int p = p0 + k * (int)blockDim.x;
+        if (p < n_pix) {
+          const float val = g[k][0] * t[k].w00 + g[k][1] * t[k].w01 + g[k][2] * t[k].w10 + g[k][3] * t[k].w11;
+          row[p] = val;
+          part += val;
+        }
+      }
     }
     __syncthreads();
     finalize_row(row, n_pix, subtract_mean, part, r, o, fred, dred);

@@ -51,6 +51,33 @@ __device__ __forceinline__ float sample_border(const float* __restrict__ img, in
   return __ldg(r0 + x0) * wnw + __ldg(r0 + x1) * wne + __ldg(r1 + x0) * wsw + __ldg(r1 + x1) * wse;
 }
 
+// The four taps of sample_border<false> (same arithmetic), split from their
+// loads so that a caller can issue the gathers of several samples together.
+struct BorderTaps {
+  int i00, i01, i10, i11;
+  float w00, w01, w10, w11;
+};
+
+__device__ __forceinline__ BorderTaps border_taps(int h, int w, float u, float v) {
+  float ix = ((u + 1.0f) * (float)w - 1.0f) / 2.0f;
+  float iy = ((v + 1.0f) * (float)h - 1.0f) / 2.0f;
+  ix = fminf(fmaxf(ix, 0.0f), (float)(w - 1));
+  iy = fminf(fmaxf(iy, 0.0f), (float)(h - 1));
+  const float fx0 = floorf(ix), fy0 = floorf(iy);
+  const int x0 = (int)fx0, y0 = (int)fy0;
+  const int x1 = min(x0 + 1, w - 1), y1 = min(y0 + 1, h - 1);
+  BorderTaps t;
+  t.w00 = (fx0 + 1.0f - ix) * (fy0 + 1.0f - iy);
+  t.w01 = (ix - fx0) * (fy0 + 1.0f - iy);
+  t.w10 = (fx0 + 1.0f - ix) * (iy - fy0);
+  t.w11 = (ix - fx0) * (iy - fy0);
+  t.i00 = y0 * w + x0;
+  t.i01 = y0 * w + x1;
+  t.i10 = y1 * w + x0;
+  t.i11 = y1 * w + x1;
+  return t;
+}
+
 // Rotate v by unit quaternion q = (w, x, y, z): v + w t + q_vec x t,
 // t = 2 q_vec x v (equal to q (0, v) q* for unit q).
 __device__ __forceinline__ float3 rotate(float4 q, float vx, float vy, float vz) {
