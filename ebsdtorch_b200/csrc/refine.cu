@@ -32,6 +32,7 @@ namespace ebsd {
 
 constexpr int kRefThreads = 512;
 constexpr int kRefGroup = 16;      // candidates scored per pass over the pixels
+constexpr int kRefIlp = 4;         // candidates whose gathers are issued together
 constexpr int kMaxRefGrid = 343;   // (2 * 3 + 1)^3
 constexpr int kMaxRefPix = 40960;  // FP32 pattern row in shared memory (160 KiB)
 
@@ -126,14 +127,34 @@ __global__ void __launch_bounds__(kRefThreads) k_refine(
             vz /= nr;
           }
           const float e = erow[p];
+          // kRefIlp candidates at a time: taps first, then their gathers
+          // together (the loop is bound by the gather latency through L2)
 #pragma unroll
-          for (int c = 0; c < kRefGroup; ++c) {
-            if (c < ng) {
-              const float3 r = rotate(cand[g0 + c], vx, vy, vz);
+          for (int c0 = 0; c0 < kRefGroup; c0 += kRefIlp) {
+            BorderTaps t[kRefIlp];
+#pragma unroll
+            for (int k = 0; k < kRefIlp; ++k) {
+              const float3 r = rotate(cand[g0 + min(c0 + k, ng - 1)], vx, vy, vz);
               const float2 uv = lambert_side_by_side(r.x, r.y, r.z);
-              const float val = sample_border<true>(mp, mp_h, mp_w2, uv.x, uv.y);
-              ad[c] = fmaf(val, e, ad[c]);
-              as[c] += val;
+              t[k] = border_taps<true>(mp_h, mp_w2, uv.x, uv.y);
+            }
+            float gv[kRefIlp][4];
+#pragma unroll
+            for (int k = 0; k < kRefIlp; ++k) {
+              gv[k][0] = __ldg(mp + t[k].i00);
+              gv[k][1] = __ldg(mp + t[k].i01);
+              gv[k][2] = __ldg(mp + t[k].i10);
+              gv[k][3] = __ldg(mp + t[k].i11);
+            }
+#pragma unroll
+            for (int k = 0; k < kRefIlp; ++k) {
+              const int c = c0 + k;
+              if (c < ng) {
+                const float val = gv[k][0] * t[k].w00 + gv[k][1] * t[k].w01 + gv[k][2] * t[k].w10 +
+                                  gv[k][3] * t[k].w11;
+                ad[c] = fmaf(val, e, ad[c]);
+                as[c] += val;
+              }
             }
           }
         }

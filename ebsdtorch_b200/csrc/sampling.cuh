@@ -51,16 +51,23 @@ __device__ __forceinline__ float sample_border(const float* __restrict__ img, in
   return __ldg(r0 + x0) * wnw + __ldg(r0 + x1) * wne + __ldg(r1 + x0) * wsw + __ldg(r1 + x1) * wse;
 }
 
-// The four taps of sample_border<false> (same arithmetic), split from their
+// The four taps of sample_border<AC> (same arithmetic), split from their
 // loads so that a caller can issue the gathers of several samples together.
 struct BorderTaps {
   int i00, i01, i10, i11;
   float w00, w01, w10, w11;
 };
 
+template <bool AC = false>
 __device__ __forceinline__ BorderTaps border_taps(int h, int w, float u, float v) {
-  float ix = ((u + 1.0f) * (float)w - 1.0f) / 2.0f;
-  float iy = ((v + 1.0f) * (float)h - 1.0f) / 2.0f;
+  float ix, iy;
+  if constexpr (AC) {
+    ix = (u + 1.0f) / 2.0f * (float)(w - 1);
+    iy = (v + 1.0f) / 2.0f * (float)(h - 1);
+  } else {
+    ix = ((u + 1.0f) * (float)w - 1.0f) / 2.0f;
+    iy = ((v + 1.0f) * (float)h - 1.0f) / 2.0f;
+  }
   ix = fminf(fmaxf(ix, 0.0f), (float)(w - 1));
   iy = fminf(fmaxf(iy, 0.0f), (float)(h - 1));
   const float fx0 = floorf(ix), fy0 = floorf(iy);
