@@ -42,6 +42,7 @@ from ..kernels import RowBuffers
 from ..s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
 from .geometry import bruker_geometry_to_SE3
 from .indexing import _device, _master_pattern_tensor
+from .._device import on_data_device
 
 MAX_PRODUCT_BYTES = 4 << 30  # spectrum product of one correlation launch
 
@@ -129,6 +130,7 @@ def _rays_soa(pix64: np.ndarray, pc_z: float, primary_tilt_deg: float, secondary
     return torch.from_numpy(c.T.copy()).float().to(device).contiguous()
 
 
+@on_data_device
 def spatial_fft_pc_fitter(
     mp,
     patterns: Tensor,

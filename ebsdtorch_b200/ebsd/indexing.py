@@ -208,23 +208,24 @@ def dictionary_index_orientations(
     stream_host = pats_host.device.type != "cuda" and pats_host.is_pinned()
     for i, mp in enumerate(master_patterns):
         dev = _device(mp, device)
-        if stream_host:
-            # chunks of a few match waves, so each chunk's copy runs under the
-            # previous chunk's match and only the first copy is exposed
-            cfg.max_query_chunk = HOST_CHUNK_WAVES * wave_query_tiles(dev) * kernels.TILE_Q
-        ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_degrees, dev, permute=True)
-        rays = _unit_rays_soa(geometry, virtual_binning, signal_mask, dev)
-        mp_t = _master_pattern_tensor(mp, virtual_binning, dev)
-        pix_index = _pix_index(signal_mask, dev)
-        n_pix = rays.shape[1]
-        pats = _pattern_source(experiment_patterns, dev)
+        with torch.cuda.device(dev):  # kernels launch on the device that holds the data
+            if stream_host:
+                # chunks of a few match waves, so each chunk's copy runs under the
+                # previous chunk's match and only the first copy is exposed
+                cfg.max_query_chunk = HOST_CHUNK_WAVES * wave_query_tiles(dev) * kernels.TILE_Q
+            ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_degrees, dev, permute=True)
+            rays = _unit_rays_soa(geometry, virtual_binning, signal_mask, dev)
+            mp_t = _master_pattern_tensor(mp, virtual_binning, dev)
+            pix_index = _pix_index(signal_mask, dev)
+            n_pix = rays.shape[1]
+            pats = _pattern_source(experiment_patterns, dev)
 
-        def fill_dict(d0, d1, bufs, mp_t=mp_t, rays=rays, ori=ori):
-            kernels.project(mp_t, rays, ori[d0:d1], bufs, subtract_mean=True)
+            def fill_dict(d0, d1, bufs, mp_t=mp_t, rays=rays, ori=ori):
+                kernels.project(mp_t, rays, ori[d0:d1], bufs, subtract_mean=True)
 
-        searcher = Searcher(ori.shape[0], n_q, n_pix, int(top_k_matches), cfg, dev)
-        idx, val = searcher.run(fill_dict, _query_fill(pats, virtual_binning, pix_index, n_pix, subtract, dev))
-        _store(experiment_patterns, i, ori, idx, val, _metric_dtype(match_dtype))
+            searcher = Searcher(ori.shape[0], n_q, n_pix, int(top_k_matches), cfg, dev)
+            idx, val = searcher.run(fill_dict, _query_fill(pats, virtual_binning, pix_index, n_pix, subtract, dev))
+            _store(experiment_patterns, i, ori, idx, val, _metric_dtype(match_dtype))
     experiment_patterns.combine_indexing_results(higher_is_better=(distance_metric == "angular"))
 
 
@@ -331,48 +332,49 @@ def pca_dictionary_index_orientations(
     subtract = bool(subtract_exp_pat_mean) if experiment_chunk_size > n_q else True
     for i, mp in enumerate(master_patterns):
         dev = _device(mp, device)
-        rays = _unit_rays_soa(geometry, virtual_binning, signal_mask, dev)
-        mp_t = _master_pattern_tensor(mp, virtual_binning, dev)
-        pix_index = _pix_index(signal_mask, dev)
-        P = rays.shape[1]
-        ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_learn_deg, dev)
-        comps = fit_pca_components(mp_t, rays, ori, int(n_pca_components), component_slice)
-        if dictionary_resolution_learn_deg != dictionary_resolution_index_deg:
-            ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_index_deg, dev)
-        proj = _Projector(comps)
-        n_comp = comps.shape[0]
-        pats = _pattern_source(experiment_patterns, dev)
-        qfill_full = _query_fill(pats, virtual_binning, pix_index, P, subtract, dev)
+        with torch.cuda.device(dev):  # kernels launch on the device that holds the data
+            rays = _unit_rays_soa(geometry, virtual_binning, signal_mask, dev)
+            mp_t = _master_pattern_tensor(mp, virtual_binning, dev)
+            pix_index = _pix_index(signal_mask, dev)
+            P = rays.shape[1]
+            ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_learn_deg, dev)
+            comps = fit_pca_components(mp_t, rays, ori, int(n_pca_components), component_slice)
+            if dictionary_resolution_learn_deg != dictionary_resolution_index_deg:
+                ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_index_deg, dev)
+            proj = _Projector(comps)
+            n_comp = comps.shape[0]
+            pats = _pattern_source(experiment_patterns, dev)
+            qfill_full = _query_fill(pats, virtual_binning, pix_index, P, subtract, dev)
 
-        def fill_dict(d0, d1, bufs, mp_t=mp_t, rays=rays, ori=ori, proj=proj):
-            for s0 in range(d0, d1, sub_chunk):
-                s1 = min(d1, s0 + sub_chunk)
-                X = torch.empty((s1 - s0, P), dtype=torch.float32, device=dev)
-                kernels.project(mp_t, rays, ori[s0:s1], RowBuffers(f32=X), subtract_mean=True)
-                Y = bufs.f32[s0 - d0:s1 - d0] if bufs.f32 is not None else torch.empty(
-                    (s1 - s0, n_comp), dtype=torch.float32, device=dev)
-                proj(X, Y)
-                _finish_rows(Y, _slice(bufs, s0 - d0, s1 - d0))
+            def fill_dict(d0, d1, bufs, mp_t=mp_t, rays=rays, ori=ori, proj=proj):
+                for s0 in range(d0, d1, sub_chunk):
+                    s1 = min(d1, s0 + sub_chunk)
+                    X = torch.empty((s1 - s0, P), dtype=torch.float32, device=dev)
+                    kernels.project(mp_t, rays, ori[s0:s1], RowBuffers(f32=X), subtract_mean=True)
+                    Y = bufs.f32[s0 - d0:s1 - d0] if bufs.f32 is not None else torch.empty(
+                        (s1 - s0, n_comp), dtype=torch.float32, device=dev)
+                    proj(X, Y)
+                    _finish_rows(Y, _slice(bufs, s0 - d0, s1 - d0))
 
-        def fill_queries(q0, q1, bufs, proj=proj):
-            for s0 in range(q0, q1, sub_chunk):
-                s1 = min(q1, s0 + sub_chunk)
-                X = torch.empty((s1 - s0, P), dtype=torch.float32, device=dev)
-                qfill_full(s0, s1, RowBuffers(f32=X))
-                Y = bufs.f32[s0 - q0:s1 - q0] if bufs.f32 is not None else torch.empty(
-                    (s1 - s0, n_comp), dtype=torch.float32, device=dev)
-                proj(X, Y)
-                _finish_rows(Y, _slice(bufs, s0 - q0, s1 - q0))
+            def fill_queries(q0, q1, bufs, proj=proj):
+                for s0 in range(q0, q1, sub_chunk):
+                    s1 = min(q1, s0 + sub_chunk)
+                    X = torch.empty((s1 - s0, P), dtype=torch.float32, device=dev)
+                    qfill_full(s0, s1, RowBuffers(f32=X))
+                    Y = bufs.f32[s0 - q0:s1 - q0] if bufs.f32 is not None else torch.empty(
+                        (s1 - s0, n_comp), dtype=torch.float32, device=dev)
+                    proj(X, Y)
+                    _finish_rows(Y, _slice(bufs, s0 - q0, s1 - q0))
 
-        budget = workspace_bytes or int(default_budget(dev) * 0.7)
-        cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=similarity, workspace_bytes=budget)
-        searcher = Searcher(ori.shape[0], n_q, n_comp, int(top_k_matches), cfg, dev)
-        idx, val = searcher.run(fill_dict, fill_queries)
-        if int(proj.status.item()) != 0:
-            raise RuntimeError("PCA projection GEMM reported a device timeout")
-        _store(experiment_patterns, i, ori, idx, val, _metric_dtype(match_dtype))
-        experiment_patterns.pca_components = getattr(experiment_patterns, "pca_components", {})
-        experiment_patterns.pca_components[i] = comps
+            budget = workspace_bytes or int(default_budget(dev) * 0.7)
+            cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=similarity, workspace_bytes=budget)
+            searcher = Searcher(ori.shape[0], n_q, n_comp, int(top_k_matches), cfg, dev)
+            idx, val = searcher.run(fill_dict, fill_queries)
+            if int(proj.status.item()) != 0:
+                raise RuntimeError("PCA projection GEMM reported a device timeout")
+            _store(experiment_patterns, i, ori, idx, val, _metric_dtype(match_dtype))
+            experiment_patterns.pca_components = getattr(experiment_patterns, "pca_components", {})
+            experiment_patterns.pca_components[i] = comps
     experiment_patterns.combine_indexing_results(higher_is_better=(distance_metric == "angular"))
 
 

@@ -33,6 +33,7 @@ from .. import kernels
 from .._capi import call, ptr
 from ..kernels import RowBuffers
 from .indexing import _device, _master_pattern_tensor
+from .._device import on_data_device
 
 
 def get_local_orientation_grid(semi_edge_in_degrees: float, kernel_radius_in_steps: int,
@@ -54,6 +55,7 @@ def get_local_orientation_grid(semi_edge_in_degrees: float, kernel_radius_in_ste
     return cu
 
 
+@on_data_device
 def orientation_grid_refinement(
     master_patterns,
     geometry,

@@ -23,6 +23,7 @@ from ._capi import call, ptr
 from .engine import RowSet, Searcher, SearchConfig
 from .kernels import LP_DTYPES, TILE_D, RowBuffers
 from .s2_and_so3.laue_fz_ori import edge_length_for_resolution
+from ._device import on_data_device
 
 
 def _stream(dev) -> int:
@@ -98,6 +99,7 @@ class LearnedStats:
     stage_mean_candidates: tuple = ()
 
 
+@on_data_device
 def learned_dictionary_index(master_pattern, geometry, experiment_patterns, model, dictionary_resolution_degrees=0.5,
                              max_angle_deg: float = 16.0, pyramid_resolutions_deg=(3.0, 1.5, 0.75),
                              stage_margin: float = 1.6, fallback_ratio: float = 0.95, n_rescore: int = 8,

@@ -18,8 +18,10 @@ from torch import Tensor
 
 from .._capi import call, ptr
 from .patterns import _stream, device_rows
+from .._device import on_data_device
 
 
+@on_data_device
 def clahe_grayscale(x: Tensor, clip_limit: float = 40.0, n_bins: int = 64,
                     grid_shape: Tuple[int, int] = (4, 4)) -> Tensor:
     """CLAHE of images (..., H, W) with values in [0, 1]; returns the same

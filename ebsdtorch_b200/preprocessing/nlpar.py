@@ -20,6 +20,7 @@ from torch import Tensor
 
 from .._capi import call, load, ptr
 from .patterns import _stream, device_rows
+from .._device import on_data_device
 
 MAX_RADIUS = 7        # the kernels' halo limit
 OFFSETS_PER_CALL = 128
@@ -36,6 +37,7 @@ def nlpar_offsets(k_rad: int) -> Tensor:
     return oc[torch.argsort(torch.sum(torch.abs(oc), dim=-1))]
 
 
+@on_data_device
 def nlpar(data: Tensor, k_rad: int = 5, coeff: float = 0.375, coeff_fit_tol: float = 1e-6,
           center_logit_bias: float = 0.0) -> Tensor:
     """Denoise a (scan_h, scan_w, H, W) scan; returns the same shape on the

@@ -17,6 +17,7 @@ import torch
 from torch import Tensor
 
 from .._capi import call, ptr
+from .._device import on_data_device
 
 NORM_MODES = {"minmax": 0, "zeromean": 1, "standard": 2}
 
@@ -40,6 +41,7 @@ def _stream(t: Tensor) -> int:
     return torch.cuda.current_stream(t.device).cuda_stream
 
 
+@on_data_device
 def pattern_mean(rows: Tensor) -> Tensor:
     """Mean over the rows of a (N, P) FP32 CUDA tensor, summed in FP64."""
     n, n_pix = rows.shape
@@ -52,6 +54,7 @@ def pattern_mean(rows: Tensor) -> Tensor:
     return mean
 
 
+@on_data_device
 def subtract_overall_background(patterns: Tensor) -> Tensor:
     """patterns minus the scan's mean pattern (experiment_pats.py:223-232)."""
     h, w = patterns.shape[-2:]
@@ -63,6 +66,7 @@ def subtract_overall_background(patterns: Tensor) -> Tensor:
     return back(rows).view(patterns.shape)
 
 
+@on_data_device
 def normalize_per_pattern(patterns: Tensor, norm_type: str = "minmax") -> Tensor:
     """Per-pattern "minmax", "zeromean" or "standard" normalisation
     (experiment_pats.py:255-285)."""
@@ -78,6 +82,7 @@ def normalize_per_pattern(patterns: Tensor, norm_type: str = "minmax") -> Tensor
     return back(rows).view(patterns.shape)
 
 
+@on_data_device
 def standard_clean(patterns: Tensor, clip_limit: float = 40.0, tile_grid_size: int = 4, n_bins: int = 64) -> Tensor:
     """Background subtraction, min-max, CLAHE, min-max
     (experiment_pats.py:287-297): one mean pass and one fused CLAHE pass

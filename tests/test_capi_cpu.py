@@ -48,3 +48,24 @@ def test_argument_errors_need_no_gpu():
         _capi.call("ebsd_match_topk", 16, 100, 16, 256, 256, 64, _capi.DT_BF16, None, 8, 1, 16, 16, 1, 0, 0, 16,
                    None)
     assert _capi.load().ebsd_grid_workspace_bytes(199) > 199**3 // 1024 * 12
+
+
+def test_device_guard_passes_host_calls_through():
+    """Without CUDA data the guard runs the call unchanged (host data goes to
+    the current device inside the call)."""
+    import torch
+
+    from ebsdtorch_b200._device import _find, on_data_device
+
+    @on_data_device
+    def f(xs, scale=1.0, device=None):
+        return [x * scale for x in xs]
+
+    x = torch.arange(4.0)
+    assert torch.equal(f([x], scale=2.0)[0], x * 2.0)
+    assert torch.equal(f([x], device="cpu")[0], x)
+
+    class Holder:
+        master_pattern = torch.zeros(2)
+
+    assert _find(Holder()) is None and _find([x, (x,)]) is None
