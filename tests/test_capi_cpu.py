@@ -69,3 +69,29 @@ def test_device_guard_passes_host_calls_through():
         master_pattern = torch.zeros(2)
 
     assert _find(Holder()) is None and _find([x, (x,)]) is None
+
+
+def test_preprocessing_and_fitting_argument_errors_need_no_gpu():
+    """The preprocessing and pattern-centre-fitting entry points reject bad
+    shapes and parameters on the host, before any CUDA call."""
+    import pytest
+
+    fake = 256  # never dereferenced: every call below fails its argument check
+    with pytest.raises(ValueError, match="mode"):
+        _capi.call("ebsd_normalize_patterns", fake, 4, 16, 16, 7, None)
+    with pytest.raises(ValueError, match="n_bins"):
+        _capi.call("ebsd_clahe", fake, 2, 16, 16, 256, None, 0, 40.0, 1, 4, 4, 0, fake, 256, None)
+    with pytest.raises(ValueError, match="bad grid"):
+        _capi.call("ebsd_clahe", fake, 2, 4, 4, 16, None, 0, 40.0, 16, 5, 3, 0, fake, 16, None)
+    with pytest.raises(ValueError, match="radius"):
+        _capi.call("ebsd_nlpar_dists", fake, 8, 8, 64, 64, 8, fake, 0, 9, 9, fake, None)
+    with pytest.raises(ValueError, match="offset block"):
+        _capi.call("ebsd_nlpar_average", fake, 8, 8, 64, 64, 3, fake, 0, 129, 129, fake, 0, fake, 64, None)
+    with pytest.raises(ValueError, match="at least 9"):
+        _capi.call("ebsd_nlpar_weights", fake, 8, 8, 64, fake, 4, 0.375, 1e-6, 0.0, fake, 1 << 20, None)
+    with pytest.raises(ValueError, match="workspace too small"):
+        _capi.call("ebsd_nlpar_weights", fake, 8, 8, 64, fake, 49, 0.375, 1e-6, 0.0, fake, 16, None)
+    with pytest.raises(ValueError, match="does not fit"):
+        _capi.call("ebsd_pcfit_prep", fake, 2, 16, 16, 20, 20, 5, 0, 1, fake, None)
+    with pytest.raises(ValueError, match="bad sizes"):
+        _capi.call("ebsd_pcfit_reduce", fake, 0, 4, 8, 8, 0, fake, fake, None)
