@@ -47,6 +47,10 @@ WORKLOADS = {
     # profiling case: the full-size kernels' shapes at a few GB of device memory
     "profile": dict(name="plain DI 128x128 px, m-3m 1.0deg dictionary (36,829), 8,192 patterns, top-8",
                     mp=1001, det=(128, 128), res=1.0, Q=8192, k=8, counts=100.0),
+    # second profiling case: a larger dictionary, to see how the match kernel's
+    # DRAM traffic per launch grows with the dictionary rows
+    "profile075": dict(name="plain DI 128x128 px, m-3m 0.75deg dictionary, 8,192 patterns, top-8",
+                       mp=1001, det=(128, 128), res=0.75, Q=8192, k=8, counts=100.0),
 }
 
 
@@ -266,6 +270,18 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, retu
     return torch.gather(best_i, 1, order), t_proj, t_match
 
 
+# DRAM bytes (read + write) of one one-wave match launch (4,736 queries
+# against the whole dictionary, bf16), captured with ncu at two dictionary
+# sizes (profiles/k_tc_gemm_match_dram_traffic.md). The traffic is affine in
+# the dictionary rows; the full launch's figure is its extrapolation.
+MATCH_DRAM_BYTES = ((36829, 8432610816 + 6049792), (89312, 16465764864 + 9438208))
+
+
+def match_traffic_estimate(d_rows: int) -> float:
+    (d1, b1), (d2, b2) = MATCH_DRAM_BYTES
+    return b1 + (b2 - b1) * (d_rows - d1) / (d2 - d1)
+
+
 def run_ours(args, wl):
     import torch
 
@@ -321,6 +337,8 @@ def run_ours(args, wl):
     avg_launch_s = sum(match_ms) / len(match_ms) / 1e3
     achieved_tflops = (sum(match_flops) / len(match_flops)) / avg_launch_s / 1e12
     match_share = sum(match_ms) / 1e3 / elapsed
+    n_dict_rows = int(exp.dictionaries[0].shape[0])
+    traffic = match_traffic_estimate(n_dict_rows) if args.precision == "bf16" else None
 
     # accuracy vs the true orientations (reported, cheap)
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
@@ -432,7 +450,10 @@ def run_ours(args, wl):
         "e2e": e2e,
         "gpu_launches": int(launches * args.steps),
         "roofline": {"bound": "tensor", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved_tflops / peak, "traffic": None,
+                     "frac": achieved_tflops / peak, "traffic": traffic,
+                     "traffic_source": ("ncu DRAM bytes of one-wave launches at 36,829 and 89,312 dictionary rows, "
+                                        "extrapolated (affine in the rows) to %d rows; per one-wave launch of 4,736 "
+                                        "queries" % n_dict_rows) if traffic is not None else None,
                      "kernel": "k_tc_gemm (match + streaming top-k)",
                      "peak_source": f"{peak_kind} bf16_tflops_sustained" + (" x2 for fp8" if args.precision == "fp8"
                                                                              else ""),
