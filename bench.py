@@ -271,7 +271,7 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, retu
 
 
 # DRAM bytes (read + write) of one one-wave match launch (4,736 queries
-# against the whole dictionary, bf16), captured with ncu at two dictionary
+# against the whole dictionary, bf16 rows of 128^2 px), captured with ncu at two dictionary
 # sizes (profiles/k_tc_gemm_match_dram_traffic.md). The traffic is affine in
 # the dictionary rows; the full launch's figure is its extrapolation.
 MATCH_DRAM_BYTES = ((36829, 8432610816 + 6049792), (89312, 16465764864 + 9438208))
@@ -338,7 +338,9 @@ def run_ours(args, wl):
     achieved_tflops = (sum(match_flops) / len(match_flops)) / avg_launch_s / 1e12
     match_share = sum(match_ms) / 1e3 / elapsed
     n_dict_rows = int(exp.dictionaries[0].shape[0])
-    traffic = match_traffic_estimate(n_dict_rows) if args.precision == "bf16" else None
+    # the captures were of 128^2 bf16 rows: no figure for other row lengths
+    traffic = match_traffic_estimate(n_dict_rows) if (args.precision == "bf16" and
+                                                      tuple(wl["det"]) == (128, 128)) else None
 
     # accuracy vs the true orientations (reported, cheap)
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
