@@ -271,9 +271,10 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, retu
 
 
 # DRAM bytes (read + write) of one one-wave match launch (4,736 queries
-# against the whole dictionary, bf16 rows of 128^2 px), captured with ncu at two dictionary
-# sizes (profiles/k_tc_gemm_match_dram_traffic.md). The traffic is affine in
-# the dictionary rows; the full launch's figure is its extrapolation.
+# against the whole dictionary, bf16 rows of 128^2 px), captured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) at two dictionary sizes. The
+# traffic is affine in the dictionary rows; the full launch's figure is its
+# extrapolation.
 MATCH_DRAM_BYTES = ((36829, 8432610816 + 6049792), (89312, 16465764864 + 9438208))
 
 
@@ -961,7 +962,7 @@ BATCHED = dict(maps=48, q_min=1000, q_max=200000, detectors=((60, 60), (80, 80),
 
 
 def run_batched(args):
-    """Config 3: many scan maps of uneven size, detector shape and phase in
+    """Many scan maps of uneven size, detector shape and phase in
     one planned batch (BatchIndexer), replayed as one CUDA graph. Patterns
     are uint16 detector counts; `value` has them resident in HBM, `e2e` in
     pinned host memory (copied inside the graph every step)."""
@@ -1066,7 +1067,7 @@ def run_batched(args):
     e2e_secs = timed(b2, True)
     b2.release_graph()
     line = {
-        "metric": "patterns indexed/s, batched uneven maps (config 3)", "value": n_pat / secs, "unit": UNIT,
+        "metric": "patterns indexed/s, batched uneven maps (48 maps of 1k-200k patterns, mixed detectors and phases)", "value": n_pat / secs, "unit": UNIT,
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
         "config": {"workload": "%d maps, patterns log-uniform in [%d, %d] (%d in total), detectors %s, phases "
@@ -1101,7 +1102,7 @@ def main():
     ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
     ap.add_argument("--fp32-subset", type=int, default=4096)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
-    ap.add_argument("--batched", action="store_true", help="time batched uneven maps (config 3) instead")
+    ap.add_argument("--batched", action="store_true", help="time batched uneven maps (48 maps, mixed sizes, detectors, phases) instead")
     ap.add_argument("--refine", action="store_true", help="time orientation grid refinement after DI instead")
     ap.add_argument("--preprocess", action="store_true", help="time pattern preprocessing (clean + NLPAR) instead")
     ap.add_argument("--pcfit", action="store_true", help="time pattern-centre fitting instead")
