@@ -530,9 +530,12 @@ __global__ void __launch_bounds__(kNlThreads, 3) k_nlpar_dists(const float* __re
 }
 
 // out[pt] (+)= sum_o w[pt, o0 + o] x[pt + off[o]]. Warp w: the 8 scan
-// points of tile row w, lane = pattern pixel of the chunk; per offset one
-// displacement load, two float4 weight loads and 8 pattern loads at
-// immediate offsets feed 8 FMAs.
+// points of tile row w, lane = pattern pixel of the chunk. The offsets are
+// walked by window row (di) and column (dj): for each di the warp loads the
+// 8 + 2 halo values of that row of the staged tile once, and every dj of the
+// row reuses them (8 FMAs per offset, two float4 weight loads). Each (di, dj)
+// may appear at most once per call; an offset outside the window makes the
+// outputs NaN.
 template <int HALO>
 __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __restrict__ data, int hs, int ws,
                                                              int n_pix, int pix_per_split, int64_t ld,
@@ -541,9 +544,10 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __res
                                                              int accumulate, float* __restrict__ out,
                                                              int64_t ld_out) {
   constexpr int plane = nl_plane(HALO);
+  constexpr int side = kNlTile + 2 * HALO, w2 = 2 * HALO + 1;
   extern __shared__ __align__(16) float T[];
-  __shared__ int off_s[kNlMaxOffsets];
-  __shared__ unsigned char bad_s[kNlMaxOffsets];
+  __shared__ int orow_s[(2 * kNlMaxRad + 1) * (2 * kNlMaxRad + 1)];  // (di, dj) -> offset of this call, or -1
+  __shared__ int any_bad;
   __shared__ int src_s[kNlMaxRows], dst_s[kNlMaxRows];
   float* w_s = T + ((kNlChunk * plane + 3) & ~3);  // [o][64 points], 16-byte aligned
   const int tiles_x = (ws + kNlTile - 1) / kNlTile;
@@ -551,15 +555,21 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __res
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // this CTA's range of pattern pixels (blockIdx.y); outputs are disjoint
   const int pix_begin = blockIdx.y * pix_per_split, pix_end = min(n_pix, pix_begin + pix_per_split);
-  nl_load_offsets(off_s, bad_s, offsets, o0, n_off, HALO);
+  for (int r = threadIdx.x; r < w2 * w2; r += blockDim.x) orow_s[r] = -1;
+  if (threadIdx.x == 0) any_bad = 0;
   nl_rows<HALO>(src_s, dst_s, hs, ws, y0, x0);
   __syncthreads();
+  for (int o = threadIdx.x; o < n_off; o += blockDim.x) {
+    const int di = offsets[2 * (o0 + o)], dj = offsets[2 * (o0 + o) + 1];
+    if (di >= -HALO && di <= HALO && dj >= -HALO && dj <= HALO)
+      orow_s[(di + HALO) * w2 + dj + HALO] = o;
+    else
+      any_bad = 1;
+  }
   for (int t = threadIdx.x; t < kNlTile * kNlTile * n_off; t += blockDim.x) {
     const int pt = t % (kNlTile * kNlTile), o = t / (kNlTile * kNlTile);
     const int y = y0 + pt / kNlTile, x = x0 + pt % kNlTile;
-    float w = 0.f;
-    if (y < hs && x < ws) w = bad_s[o] ? NAN : weights[((int64_t)y * ws + x) * n_off_total + o0 + o];
-    w_s[t] = w;
+    w_s[t] = (y < hs && x < ws) ? weights[((int64_t)y * ws + x) * n_off_total + o0 + o] : 0.f;
   }
   const int y = y0 + wid;
   const float4* w4 = reinterpret_cast<const float4*>(w_s) + wid * 2;
@@ -569,29 +579,38 @@ __global__ void __launch_bounds__(kNlThreads) k_nlpar_average(const float* __res
     nl_load_chunk<HALO>(T, data, ld, src_s, dst_s, p0, np);
     __syncthreads();
     if (y >= hs) continue;
-    const float* base = T + lane * plane + (wid + HALO) * kNlPitch + HALO;
+    const float* rows = T + lane * plane + wid * kNlPitch;  // window row wid + (di + HALO)
     float s[kNlTile];
 #pragma unroll
     for (int k = 0; k < kNlTile; ++k) s[k] = 0.f;
-#pragma unroll 4
-    for (int o = 0; o < n_off; ++o) {
-      const float* b = base + off_s[o];
-      const float4 wa = w4[o * (kNlTile * kNlTile / 4)], wb = w4[o * (kNlTile * kNlTile / 4) + 1];
-      s[0] = fmaf(wa.x, b[0], s[0]);
-      s[1] = fmaf(wa.y, b[1], s[1]);
-      s[2] = fmaf(wa.z, b[2], s[2]);
-      s[3] = fmaf(wa.w, b[3], s[3]);
-      s[4] = fmaf(wb.x, b[4], s[4]);
-      s[5] = fmaf(wb.y, b[5], s[5]);
-      s[6] = fmaf(wb.z, b[6], s[6]);
-      s[7] = fmaf(wb.w, b[7], s[7]);
+#pragma unroll 1
+    for (int a = 0; a < w2; ++a) {
+      const float* r = rows + a * kNlPitch;
+      float v[side];
+#pragma unroll
+      for (int x = 0; x < side; ++x) v[x] = r[x];
+#pragma unroll
+      for (int c = 0; c < w2; ++c) {
+        const int o = orow_s[a * w2 + c];
+        if (o < 0) continue;
+        const float4 wa = w4[o * (kNlTile * kNlTile / 4)], wb = w4[o * (kNlTile * kNlTile / 4) + 1];
+        s[0] = fmaf(wa.x, v[0 + c], s[0]);
+        s[1] = fmaf(wa.y, v[1 + c], s[1]);
+        s[2] = fmaf(wa.z, v[2 + c], s[2]);
+        s[3] = fmaf(wa.w, v[3 + c], s[3]);
+        s[4] = fmaf(wb.x, v[4 + c], s[4]);
+        s[5] = fmaf(wb.y, v[5 + c], s[5]);
+        s[6] = fmaf(wb.z, v[6 + c], s[6]);
+        s[7] = fmaf(wb.w, v[7 + c], s[7]);
+      }
     }
     if (lane < np) {
 #pragma unroll
       for (int k = 0; k < kNlTile; ++k) {
         if (x0 + k < ws) {
           float* dp = out + ((int64_t)y * ws + x0 + k) * ld_out + p0 + lane;
-          *dp = accumulate ? *dp + s[k] : s[k];
+          const float val = any_bad ? NAN : s[k];
+          *dp = accumulate ? *dp + val : val;
         }
       }
     }

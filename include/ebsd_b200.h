@@ -315,7 +315,8 @@ int ebsd_clahe(const float* images, int64_t n, int height, int width, int64_t ld
  * dists[pt, o] = sum_p (x[pt + off_o, p] - x[pt, p])^2 (scan_h * scan_w x
  * n_off_total); ebsd_nlpar_average writes (accumulate 0) or adds
  * (accumulate 1) out[pt, p] = sum_o weights[pt, o] x[pt + off_o, p]. An
- * offset outside the window yields NaN. */
+ * offset outside the window yields NaN; each offset may appear at most once
+ * per call (the window's offsets, as the reference's window is). */
 int ebsd_nlpar_dists(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
                      const int* offsets, int o0, int n_off, int n_off_total, float* dists, void* stream);
 int ebsd_nlpar_average(const float* data, int scan_h, int scan_w, int n_pix, int64_t ld, int k_rad,
