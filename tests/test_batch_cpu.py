@@ -53,3 +53,26 @@ def test_synthetic_master_pattern_bands_are_closed_under_the_laue_group():
                 assert max(abs(float(m @ x)) for x in orbit) > 1 - 1e-9
     img = synthetic.synthetic_master_pattern(33, seed=4, laue_group=9)
     assert img.shape == (33, 66) and torch.isfinite(img).all()
+
+
+def test_planner_caps_query_chunks_for_streamed_patterns():
+    """With a budget that fits everything, the planner takes all queries in one
+    chunk. With max_query_chunk (set for patterns streamed from pinned host
+    memory), the chunks are capped so that each chunk's copy can run under the
+    previous chunk's match, while the dictionary stays in one chunk."""
+    from ebsdtorch_b200.engine import Searcher, SearchConfig
+
+    one = Searcher(328720, 262144, 16384, 8, SearchConfig(workspace_bytes=150 << 30), "cpu")
+    assert one.query_chunk == 262144 and one.dict_chunk >= 328720
+    capped = Searcher(328720, 262144, 16384, 8, SearchConfig(workspace_bytes=150 << 30, max_query_chunk=18944), "cpu")
+    assert capped.query_chunk == 18944 and capped.dict_chunk == one.dict_chunk
+    small = Searcher(328720, 5000, 16384, 8, SearchConfig(workspace_bytes=150 << 30, max_query_chunk=18944), "cpu")
+    assert small.query_chunk == 5120  # the whole (padded) map when it is smaller than the cap
+
+
+def test_match_traffic_model_reproduces_its_captures():
+    import bench
+
+    for rows, dram in bench.MATCH_DRAM_BYTES:
+        assert abs(bench.match_traffic_estimate(rows) - dram) < 1.0
+    assert bench.match_traffic_estimate(328720) > 4 * (328960 * 16384 * 2)  # ~5 reads per row
