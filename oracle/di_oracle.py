@@ -1249,3 +1249,22 @@ def spatial_fft_pc_fit(master_pattern, patterns, quats_dict, pc_x_min=0.0, pc_x_
     pc = np.array([0.5 + float(xi - pad[0] - (Wb + 1) // 2) / Wb, 0.5 + float(yi - pad[2] - (Hb + 1) // 2) / Hb,
                    float(z_vals[zi])])
     return pc, best_i[zi, :, yi, xi], avg
+
+
+# --------------------------------------------------------------------------
+# EMsoft master-pattern reader (io/read_master_pattern.py:7-53)
+# --------------------------------------------------------------------------
+
+
+def emsoft_master_pattern(accum_e: np.ndarray, north: np.ndarray, south: np.ndarray) -> np.ndarray:
+    """The energy-weighted hemispheres side by side, float64: weights =
+    accum_e summed over its first two axes, normalised; each hemisphere
+    (1, n_e, H, W) squeezed and summed over energies with those weights
+    (read_master_pattern.py:35-47)."""
+    w = accum_e.astype(np.float64).sum(axis=(0, 1))
+    w = w / w.sum()
+    out = []
+    for hemi in (north, south):
+        h = hemi.astype(np.float64).reshape(-1, *hemi.shape[-2:])
+        out.append((w[:, None, None] * h).sum(axis=0))
+    return np.concatenate(out, axis=-1)

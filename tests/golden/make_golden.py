@@ -13,7 +13,8 @@ modified. The PCA variant is also loaded with line 355's component slice
 
 Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
 outputs of one case (``--refinement-only`` / ``--preprocessing-only`` /
-``--pcfit-only`` write just refine.npz / preprocess.npz / pcfit.npz). The files are small (< 1 MB each) and committed.
+``--pcfit-only`` / ``--reader-only`` write just refine.npz / preprocess.npz /
+pcfit.npz / emsoft_reader.npz). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -241,6 +242,51 @@ def pcfit_goldens(root: str = "/root/reference"):
     np.savez_compressed(os.path.join(HERE, "pcfit.npz"), **out)
 
 
+def emsoft_reader_goldens(root: str = "/root/reference"):
+    """EMsoft master-pattern reader (io/read_master_pattern.py:7-53). h5py is
+    absent, so the reference's read_master_pattern runs on an in-memory
+    stand-in of h5py.File serving seeded arrays with EMsoft's dataset names
+    and layouts: accum_e (H, W, n_energies), mLPNH / mLPSH (1, n_energies, H,
+    W), SpaceGroupNumber (1,). Cases: 5 energies / m-3m (225), 1 energy
+    (the squeeze edge) / 6/mmm (194), 7 energies / mmm (62)."""
+    sys.path.insert(0, root)
+    files = {}
+
+    class _File:
+        def __init__(self, path, mode="r"):
+            self.data = files[path]
+
+        def __enter__(self):
+            return self.data
+
+        def __exit__(self, *a):
+            return False
+
+    fake = types.ModuleType("h5py")
+    fake.File = _File
+    sys.modules["h5py"] = fake
+    from ebsdtorch.io.read_master_pattern import read_master_pattern
+
+    out = {}
+    for ci, (n_e, h, sg) in enumerate(((5, 33, 225), (1, 17, 194), (7, 25, 62))):
+        g = torch.Generator().manual_seed(300 + ci)
+        arrays = {
+            "EMData/MCOpenCL/accum_e": (torch.rand((h + 8, h + 8, n_e), generator=g) * 1000).round().numpy()
+                                       .astype(np.int32),
+            "EMData/EBSDmaster/mLPNH": torch.rand((1, n_e, h, h), generator=g).numpy().astype(np.float32),
+            "EMData/EBSDmaster/mLPSH": torch.rand((1, n_e, h, h), generator=g).numpy().astype(np.float32),
+            "CrystalData/SpaceGroupNumber": np.array([sg], dtype=np.int32),
+        }
+        files[f"case{ci}.h5"] = arrays
+        mp = read_master_pattern(f"case{ci}.h5")
+        for k, v in arrays.items():
+            out[f"case{ci}/{k}"] = v
+        out[f"case{ci}_master_pattern"] = mp.master_pattern.numpy()
+        out[f"case{ci}_laue_group"] = np.array([mp.laue_group], dtype=np.int64)
+    del sys.modules["h5py"]
+    np.savez_compressed(os.path.join(HERE, "emsoft_reader.npz"), **out)
+
+
 def main(root: str = "/root/reference"):
     ref_idx, ref_idx_top = load_reference(root)
     from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
@@ -464,8 +510,11 @@ if __name__ == "__main__":
         preprocessing_goldens(*args[1:])
     elif args and args[0] == "--pcfit-only":
         pcfit_goldens(*args[1:])
+    elif args and args[0] == "--reader-only":
+        emsoft_reader_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
         preprocessing_goldens(*args)
         pcfit_goldens(*args)
+        emsoft_reader_goldens(*args)

@@ -379,3 +379,63 @@ def test_bruker_se3_round_trip():
     assert torch.allclose(back, pcs, atol=1e-12)
     assert torch.allclose(tilt, torch.full((2,), 70.0, dtype=torch.float64))
     assert torch.allclose(sec, torch.full((2,), 10.0, dtype=torch.float64))
+
+
+# ---- EMsoft master-pattern reader -------------------------------------------
+
+_EMSOFT_KEYS = ("EMData/MCOpenCL/accum_e", "EMData/EBSDmaster/mLPNH", "EMData/EBSDmaster/mLPSH",
+                "CrystalData/SpaceGroupNumber")
+
+
+def _emsoft_case(g, ci):
+    return {k: g[f"case{ci}/{k}"] for k in _EMSOFT_KEYS}
+
+
+@pytest.mark.parametrize("ci", [0, 1, 2])
+def test_emsoft_reader_oracle_and_port_match_reference(golden, ci):
+    """read_master_pattern (io/read_master_pattern.py:7-53), run by the
+    reference on the same arrays: 5 / 1 / 7 energy bins, space groups 225 /
+    194 / 62. The FP64 oracle and the reader agree with it."""
+    from ebsdtorch_b200.io import master_pattern_from_emsoft
+
+    g = golden("emsoft_reader")
+    d = _emsoft_case(g, ci)
+    ref = g[f"case{ci}_master_pattern"]
+    ora = O.emsoft_master_pattern(d[_EMSOFT_KEYS[0]], d[_EMSOFT_KEYS[1]], d[_EMSOFT_KEYS[2]])
+    assert np.abs(ora - ref).max() <= 1e-6 * np.abs(ref).max()
+    mp = master_pattern_from_emsoft(d[_EMSOFT_KEYS[0]], d[_EMSOFT_KEYS[1]], d[_EMSOFT_KEYS[2]],
+                                    int(d[_EMSOFT_KEYS[3]][0]))
+    assert str(mp.master_pattern.dtype) == "torch.float32" and tuple(mp.master_pattern.shape) == ref.shape
+    assert np.abs(mp.master_pattern.numpy() - ref).max() <= 1e-6 * np.abs(ref).max()
+    assert mp.laue_group == int(g[f"case{ci}_laue_group"][0])
+
+
+def test_read_master_pattern_through_the_file_api(golden):
+    """The reader opens the file with h5py's File API: an in-memory stand-in
+    of that API gives the reference's result; without h5py it raises."""
+    import types
+
+    from ebsdtorch_b200.io import read_master_pattern
+
+    g = golden("emsoft_reader")
+    d = _emsoft_case(g, 0)
+
+    class _File:
+        def __init__(self, path, mode):
+            assert path == "scan.h5" and mode == "r"
+
+        def __enter__(self):
+            return d
+
+        def __exit__(self, *a):
+            return False
+
+    fake = types.SimpleNamespace(File=_File)
+    mp = read_master_pattern("scan.h5", h5py_module=fake)
+    ref = g["case0_master_pattern"]
+    assert np.abs(mp.master_pattern.numpy() - ref).max() <= 1e-6 * np.abs(ref).max()
+    try:
+        import h5py  # noqa: F401
+    except ImportError:
+        with pytest.raises(ImportError, match="h5py"):
+            read_master_pattern("scan.h5")
