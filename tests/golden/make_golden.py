@@ -2,9 +2,11 @@
 
 Run in a container that holds the reference source tree:
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [REFERENCE_ROOT]
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [--<case>-only] [REFERENCE_ROOT]
 
-REFERENCE_ROOT defaults to /root/reference. The reference's
+REFERENCE_ROOT is the directory holding the reference's ``ebsdtorch/``; without
+it, $EBSD_REFERENCE_ROOT, then the copy staged by ``oracle/stage_ref.py`` in
+``oracle/_ref`` are used (``oracle/ref_loader.py``). The reference's
 ``ebsdtorch/ebsd/indexing.py`` ends in a module-level demo script that imports
 ``kikuchipy`` (absent), so the two DI functions are loaded by executing only
 the file's lines 1-477 into a fresh module; nothing in the reference tree is
@@ -14,7 +16,9 @@ modified. The PCA variant is also loaded with line 355's component slice
 Outputs ``tests/golden/*.npz``; each file holds the inputs and the reference
 outputs of one case (``--refinement-only`` / ``--preprocessing-only`` /
 ``--pcfit-only`` / ``--reader-only`` write just refine.npz / preprocess.npz /
-pcfit.npz / emsoft_reader.npz). The files are small (< 1 MB each) and committed.
+pcfit.npz / emsoft_reader.npz; ``--config0-only`` writes config0.npz, the
+reference's own plain DI at the small configuration on inputs rebuilt by
+``config0_inputs.py``). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -29,26 +33,18 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
+ROOT = os.path.dirname(os.path.dirname(HERE))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from oracle import ref_loader  # noqa: E402
 
 
-def load_reference(root: str):
-    sys.path.insert(0, root)
-    import ebsdtorch  # noqa: F401
-
-    path = os.path.join(root, "ebsdtorch", "ebsd", "indexing.py")
-    with open(path) as f:
-        lines = f.readlines()
-    src = "".join(lines[:477])
-    mod = types.ModuleType("ref_indexing")
-    mod.__file__ = path
-    exec(compile(src, path, "exec"), mod.__dict__)
-    shipped_slice = "pca_matrix = eigenvectors[:, -n_pca_components : (-n_pca_components + 300)]"
-    assert shipped_slice in src
-    mod_top = types.ModuleType("ref_indexing_top")
-    mod_top.__file__ = path
-    exec(compile(src.replace(shipped_slice, "pca_matrix = eigenvectors[:, -n_pca_components:]"), path, "exec"),
-         mod_top.__dict__)
-    return mod, mod_top
+def load_reference(root=None):
+    """(indexing module as shipped, indexing module with the "top" PCA slice)."""
+    return ref_loader.load_indexing(root), ref_loader.load_indexing(root, top_slice=True)
 
 
 def smooth_master_pattern(seed: int, n: int) -> torch.Tensor:
@@ -59,11 +55,11 @@ def smooth_master_pattern(seed: int, n: int) -> torch.Tensor:
     return mp.contiguous().float()
 
 
-def refinement_goldens(root: str = "/root/reference"):
+def refinement_goldens(root=None):
     """Orientation grid refinement (ebsd/refining.py): local grids and three
     refinement cases (kernel radius, axial grid, binning, shrink factor,
     pattern-centre mode), float32 matching."""
-    sys.path.insert(0, root)
+    ref_loader.import_reference(root)
     from ebsdtorch.ebsd.refining import get_local_orientation_grid, orientation_grid_refinement
     from ebsdtorch.s2_and_so3.sampling import so3_uniform_quat
     from ebsdtorch.s2_and_so3.quaternions import qu_prod
@@ -123,11 +119,11 @@ def refinement_goldens(root: str = "/root/reference"):
     np.savez_compressed(os.path.join(HERE, "refine.npz"), **out)
 
 
-def preprocessing_goldens(root: str = "/root/reference"):
+def preprocessing_goldens(root=None):
     """Pattern preprocessing (experiment_pats.py:223-316, preprocessing/
     clahe.py, nlpar.py): overall background, per-pattern normalisation,
     CLAHE (divisible and reflect-padded sizes), standard_clean, NLPAR."""
-    sys.path.insert(0, root)
+    ref_loader.import_reference(root)
     from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
     from ebsdtorch.preprocessing.clahe import clahe_grayscale
     from ebsdtorch.preprocessing.nlpar import nlpar
@@ -170,14 +166,14 @@ def preprocessing_goldens(root: str = "/root/reference"):
     np.savez_compressed(os.path.join(HERE, "preprocess.npz"), **out)
 
 
-def pcfit_goldens(root: str = "/root/reference"):
+def pcfit_goldens(root=None):
     """Pattern-centre fitting (ebsd/fitting.py:359-540, spatial FFT fitter):
     three cases (binning 1 / 2, one or several dictionary batches, tilts),
     the enlarged pixel grid and the first simulated dictionary patterns.
     fitting.py imports matplotlib (for a plotting helper that is commented
     out) and, through io/read_master_pattern.py, h5py; neither is used by the
     fitter, so empty stand-in modules are registered when they are absent."""
-    sys.path.insert(0, root)
+    ref_loader.import_reference(root)
     for name in ("matplotlib", "matplotlib.pyplot", "h5py"):
         try:
             __import__(name)
@@ -242,14 +238,14 @@ def pcfit_goldens(root: str = "/root/reference"):
     np.savez_compressed(os.path.join(HERE, "pcfit.npz"), **out)
 
 
-def emsoft_reader_goldens(root: str = "/root/reference"):
+def emsoft_reader_goldens(root=None):
     """EMsoft master-pattern reader (io/read_master_pattern.py:7-53). h5py is
     absent, so the reference's read_master_pattern runs on an in-memory
     stand-in of h5py.File serving seeded arrays with EMsoft's dataset names
     and layouts: accum_e (H, W, n_energies), mLPNH / mLPSH (1, n_energies, H,
     W), SpaceGroupNumber (1,). Cases: 5 energies / m-3m (225), 1 energy
     (the squeeze edge) / 6/mmm (194), 7 energies / mmm (62)."""
-    sys.path.insert(0, root)
+    ref_loader.import_reference(root)
     files = {}
 
     class _File:
@@ -287,7 +283,48 @@ def emsoft_reader_goldens(root: str = "/root/reference"):
     np.savez_compressed(os.path.join(HERE, "emsoft_reader.npz"), **out)
 
 
-def main(root: str = "/root/reference"):
+def config0_goldens(root=None):
+    """The reference's own plain DI at the small configuration (60 x 60 px,
+    m-3m 1.0 deg dictionary of 36,829 rows, 4,096 patterns, top-4, float32
+    matching, chunked over both axes) on the inputs of config0_inputs.py.
+    Commits the seeds, the inputs' checksums and the results: per pattern the
+    top-4 dictionary indices (into the permuted dictionary) and metrics."""
+    import config0_inputs as C
+
+    ref_idx, _ = load_reference(root)
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.ebsd.geometry import EBSDGeometry
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+
+    c = C.CASE
+    inp = C.make_inputs(c)
+    mp = MasterPattern(torch.from_numpy(inp["master_pattern"]).clone(), laue_group=11)
+    geom = EBSDGeometry(c["det"], tilts_degrees=c["tilts"], proj_center=c["pc"])
+    exp = ExperimentPatterns(torch.from_numpy(inp["counts"].astype(np.float32)))
+    torch.manual_seed(c["perm_seed"])
+    with ref_loader.quiet_stdout():
+        ref_idx.dictionary_index_orientations(
+            mp, geom, exp, dictionary_resolution_degrees=c["res"], top_k_matches=c["k"],
+            dictionary_chunk_size=c["dictionary_chunk_size"], experiment_chunk_size=c["experiment_chunk_size"],
+            match_dtype=torch.float32, quantized_if_x86=False)
+    quats_k, metrics_k = exp.raw_indexing_results[0]
+    torch.manual_seed(c["perm_seed"])
+    dictionary = sample_ori_fz_laue_angle(11, c["res"], torch.device("cpu"), permute=True).numpy()
+    lookup = {row.tobytes(): i for i, row in enumerate(dictionary)}
+    q = quats_k.numpy()
+    idx = np.array([[lookup[q[i, j].tobytes()] for j in range(q.shape[1])] for i in range(q.shape[0])],
+                   dtype=np.int32)
+    np.savez_compressed(
+        os.path.join(HERE, "config0.npz"),
+        indices=idx, metrics=metrics_k.numpy().astype(np.float32),
+        n_dictionary=np.array([dictionary.shape[0]]),
+        sha256_master_pattern=np.array(inp["sha256_master_pattern"]),
+        sha256_counts=np.array(inp["sha256_counts"]),
+        case=np.array(repr(sorted(c.items()))))
+
+
+def main(root=None):
     ref_idx, ref_idx_top = load_reference(root)
     from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
     from ebsdtorch.s2_and_so3.orientations import cu2qu, qu2cu
@@ -512,9 +549,12 @@ if __name__ == "__main__":
         pcfit_goldens(*args[1:])
     elif args and args[0] == "--reader-only":
         emsoft_reader_goldens(*args[1:])
+    elif args and args[0] == "--config0-only":
+        config0_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
         preprocessing_goldens(*args)
         pcfit_goldens(*args)
         emsoft_reader_goldens(*args)
+        config0_goldens(*args)

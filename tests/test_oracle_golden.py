@@ -1,6 +1,8 @@
 """Pins the CPU oracle against golden vectors produced by the reference
 ebsdtorch itself (tests/golden/make_golden.py). CPU only."""
 
+import os
+
 import numpy as np
 import pytest
 
@@ -439,3 +441,34 @@ def test_read_master_pattern_through_the_file_api(golden):
     except ImportError:
         with pytest.raises(ImportError, match="h5py"):
             read_master_pattern("scan.h5")
+
+
+def test_config0_inputs_reproduce_the_golden_checksums(golden):
+    """The config-0 inputs (tests/golden/config0_inputs.py) rebuild bit-exactly."""
+    import sys
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import config0_inputs as C
+
+    d = golden("config0")
+    inp = C.make_inputs(C.CASE)
+    assert inp["sha256_master_pattern"] == str(d["sha256_master_pattern"])
+    assert inp["sha256_counts"] == str(d["sha256_counts"])
+    # the oracle's float32 DI of the first 48 patterns agrees with the
+    # reference's top-4 over the whole 36,829-row dictionary
+    c = C.CASE
+    import torch
+
+    base = O.sample_ori_fz_laue_angle(11, c["res"])
+    assert base.shape[0] == int(d["n_dictionary"][0])
+    torch.manual_seed(c["perm_seed"])  # the reference's randperm convention
+    dictionary = base[torch.randperm(base.shape[0]).numpy()]
+    rays = O.unit_rays(O.detector_coords_sample_frame(c["det"], c["pc"], c["tilts"]))
+    rows = O.dictionary_rows(inp["master_pattern"], rays, dictionary, dtype=np.float32, chunk=1024)
+    q = O.prep_patterns(inp["counts"][:48].astype(np.float32), dtype=np.float32)
+    idx, val = O.topk_dot(q, rows, c["k"])
+    ref_i, ref_m = d["indices"][:48], d["metrics"][:48]
+    assert (idx[:, 0] == ref_i[:, 0]).all()
+    same = idx == ref_i
+    assert same.mean() >= 0.99
+    assert (np.abs(val - ref_m)[same] / np.abs(ref_m[:, :1]).repeat(4, 1)[same]).max() < 1e-4
