@@ -317,6 +317,94 @@ def match_traffic_estimate(d_rows: int) -> float:
     return b1 + (b2 - b1) * (d_rows - d1) / (d2 - d1)
 
 
+def learned_block(args, wl, mp, geom, pats, exp_plain, ref_top1, n_sub, dist, dev):
+    """Companion measurement of the learned path on the headline run's own
+    patterns: the proposal network is trained first (outside the timed
+    region), then learned proposal + coarse-to-fine local DI + plain-DI
+    fallback is timed over `args.steps` calls, patterns resident in HBM, and
+    once more end to end from pinned host memory. Agreement is measured
+    against this run's plain DI (whose top-1 is the FP32 top-1) and, on the
+    first n_sub patterns, against the reference's FP32 GPU DI."""
+    import torch
+
+    from ebsdtorch_b200.ebsd import ExperimentPatterns
+    from ebsdtorch_b200.learned import train_proposal_cnn
+    from ebsdtorch_b200.local_search import learned_dictionary_index
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+
+    t0 = time.perf_counter()
+    model, losses = train_proposal_cnn(mp.master_pattern, geom, 11, steps=args.train_steps, batch=256, lr=1e-3,
+                                       mean_counts=wl["counts"], seed=0)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    pyramid = tuple(float(v) for v in args.pyramid.split(",") if v)
+    kw = dict(dictionary_resolution_degrees=wl["res"], max_angle_deg=args.max_angle,
+              pyramid_resolutions_deg=pyramid, fallback_ratio=args.fallback_ratio, stage_margin=args.stage_margin)
+    exp = ExperimentPatterns(pats)
+
+    def step():
+        torch.manual_seed(0)
+        return learned_dictionary_index(mp, geom, exp, model, **kw)
+
+    for _ in range(max(1, min(args.warmup, 3))):
+        step()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        st = step()
+    e1.record()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    t = _max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, dev)
+    n = args.gpus
+    ours_q = exp.orientations.float().contiguous()
+    ang = disori_angle_laue(ours_q, exp_plain.orientations.float().contiguous(), 11, 11)
+    out = {"value": n * wl["Q"] * args.steps / t, "unit": UNIT, "ms_per_step": t / args.steps * 1e3,
+           "within_0.5deg_of_plain_di": float((ang < math.radians(0.5)).float().mean()),
+           "same_top1_index_as_plain_di": float((exp.raw_indexing_indices[0][:, 0] ==
+                                                 exp_plain.raw_indexing_indices[0][:, 0]).float().mean()),
+           "fallback_fraction": st.n_fallback / st.n_patterns, "stage_radii_deg": st.stage_radii_deg,
+           "stage_mean_candidates": st.stage_mean_candidates, "stage_seconds": st.seconds,
+           "train_seconds_untimed": t_train, "train_patterns": 256 * args.train_steps,
+           "final_train_loss": float(losses[-100:].mean()),
+           "how": "CNN proposal (bf16, own kernels) + local DI within %.1f deg on the %s deg dictionaries, then the "
+                  "full one, + plain-DI fallback below %.2f x the map median" % (args.max_angle, args.pyramid,
+                                                                                args.fallback_ratio)}
+    if ref_top1 is not None:
+        a = disori_angle_laue(ours_q[:n_sub].contiguous(), ref_top1, 11, 11)
+        out["within_0.5deg_of_reference_fp32_di"] = float((a < math.radians(0.5)).float().mean())
+        out["reference_subset"] = n_sub
+    if not args.no_e2e:
+        try:
+            host = torch.empty(pats.shape, dtype=pats.dtype, pin_memory=True)
+            host.copy_(pats)
+        except RuntimeError:
+            host = pats.cpu()
+        exp_h = ExperimentPatterns(host)
+        ori_host = torch.empty((wl["Q"], 4), dtype=torch.float32, pin_memory=True)
+        torch.manual_seed(0)
+        learned_dictionary_index(mp, geom, exp_h, model, **kw)
+        torch.cuda.synchronize()
+        _barrier(dist)
+        h0 = time.perf_counter()
+        e2e_steps = max(1, args.steps // 2)
+        for _ in range(e2e_steps):
+            torch.manual_seed(0)
+            learned_dictionary_index(mp, geom, exp_h, model, **kw)
+            ori_host.copy_(exp_h.orientations.float(), non_blocking=True)
+        torch.cuda.synchronize()
+        _barrier(dist)
+        th = _max_over_ranks(time.perf_counter() - h0, dist, dev)
+        out["e2e"] = {"value": n * wl["Q"] * e2e_steps / th, "unit": UNIT,
+                      "h2d_bytes_per_step": int(host.numel() * host.element_size()),
+                      "d2h_bytes_per_step": int(ori_host.numel() * 4), "host_memory": "pinned"}
+        del exp_h, host
+    del exp, model
+    return out
+
+
 def run_ours(args, wl):
     import torch
 
@@ -465,6 +553,11 @@ def run_ours(args, wl):
             fp8["speedup_vs_plain_fp32_gpu_di"] = fp8["value"] / n / fp32_cmp["plain_fp32_gpu_di_rate"]
         del exp8
 
+    # ---- the learned path on the same patterns (training untimed) ----
+    learned = None
+    if not args.no_learned and tuple(wl["det"]) == (128, 128):
+        learned = learned_block(args, wl, mp, geom, pats, exp, ref_top1, n_sub if fp32_cmp else 0, dist, dev)
+
     # ---- end to end: host (pinned) patterns, H2D + D2H inside the timed region ----
     e2e = None
     if not args.no_e2e:
@@ -523,6 +616,7 @@ def run_ours(args, wl):
         "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
         "plain_fp32_di": fp32_cmp,
         "fp8": fp8,
+        "learned": learned,
         "clocks": clk,
     }
     if rank == 0 and n == 1 and not args.no_cpu_baseline:
@@ -1019,6 +1113,150 @@ BATCHED = dict(maps=48, q_min=1000, q_max=200000, detectors=((60, 60), (80, 80),
                phases=((11, 0.5), (9, 0.615), (5, 0.88)), mp=1001, counts=100.0, seed=3)
 
 
+def run_pca(args):
+    """PCA dictionary indexing at the full size: 128 x 128 px, a basis of
+    1,024 components fitted on the m-3m 0.9 deg dictionary (51,312 rows),
+    indexing against the 0.5 deg dictionary (328,720 rows), 262,144 patterns,
+    top-8. The fit (covariance + eigendecomposition) is a one-time cost,
+    timed and reported on its own; a step is one
+    pca_dictionary_index_orientations call given that basis (dictionary
+    projection + PCA projection, query preparation + projection, match,
+    FP32 re-score in PCA space)."""
+    import torch
+
+    from ebsdtorch_b200 import _capi, engine, synthetic
+    from ebsdtorch_b200.ebsd import (EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations,
+                                     pca_dictionary_index_orientations)
+    from ebsdtorch_b200.ebsd import indexing as I
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+    from ebsdtorch_b200.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+
+    wl = WORKLOADS["full"]
+    n_comp, learn_res = 1024, 0.9
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    _capi.load()
+    mp = MasterPattern(synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev), laue_group=11)
+    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+    truth = synthetic.random_quaternions(wl["Q"], 1000).to(dev)
+    pats = synthetic.synthetic_patterns(mp.master_pattern, geom, truth, mean_counts=wl["counts"], seed=2000)
+    exp = ExperimentPatterns(pats)
+
+    # ---- one-time fit ----
+    rays = I._unit_rays_soa(geom, 1, None, dev)
+    torch.manual_seed(0)
+    ori_learn = sample_ori_fz_laue_angle(11, learn_res, dev)
+    fit = {"learn_rows": int(ori_learn.shape[0])}
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    comps = I.fit_pca_components(mp.master_pattern, rays, ori_learn, n_comp, "top", timings=fit)
+    torch.cuda.synchronize()
+    fit["total_s"] = time.perf_counter() - t0
+    del ori_learn
+    kw = dict(n_pca_components=n_comp, dictionary_resolution_learn_deg=learn_res,
+              dictionary_resolution_index_deg=wl["res"], top_k_matches=wl["k"], match_dtype=torch.float32,
+              components=comps)
+
+    def step():
+        torch.manual_seed(0)
+        pca_dictionary_index_orientations(mp, geom, exp, **kw)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    engine.MATCH_TIMERS, I.PROJ_TIMERS = [], []
+    launches0 = _capi.launch_count
+    with ClockSampler(int(dev.index or 0)) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            step()
+        e1.record()
+        torch.cuda.synchronize()
+    launches = (_capi.launch_count - launches0) // args.steps
+    t = e0.elapsed_time(e1) / 1e3
+    mt, pt = engine.MATCH_TIMERS, I.PROJ_TIMERS
+    engine.MATCH_TIMERS = I.PROJ_TIMERS = None
+    match_ms = [a.elapsed_time(b) for a, b, _ in mt]
+    match_fl = [f for _, _, f in mt]
+    proj_ms = [a.elapsed_time(b) for a, b, _ in pt]
+    proj_fl = [f for _, _, f in pt]
+    achieved = (sum(match_fl) / len(match_fl)) / (sum(match_ms) / len(match_ms) / 1e3) / 1e12
+    peaks, peak_kind = _peaks()
+    peak = peaks.get("bf16_tflops_sustained", 1400.0)
+    D = int(exp.dictionaries[0].shape[0])
+    P = rays.shape[1]
+    value = wl["Q"] * args.steps / t
+    # FP32-class accuracy of the split GEMM: a few dictionary-like rows against FP64
+    X = pats[:64].reshape(64, -1).double()
+    X = X - X.mean(dim=1, keepdim=True)
+    Y = torch.empty((64, n_comp), dtype=torch.float32, device=dev)
+    I._Projector(comps)(X.float().contiguous(), Y)
+    Y64 = X @ comps.double().t()
+    proj_err = float(((Y.double() - Y64).abs().max(dim=1).values / Y64.abs().max(dim=1).values).max())
+    # agreement with plain DI (bf16 match + FP32 re-score == FP32 top-1) on a subset
+    n_sub = min(wl["Q"], args.fp32_subset)
+    exp_p = ExperimentPatterns(pats[:n_sub])
+    torch.manual_seed(0)
+    dictionary_index_orientations(mp, geom, exp_p, dictionary_resolution_degrees=wl["res"], top_k_matches=1,
+                                  match_dtype=torch.float32)
+    a = disori_angle_laue(exp.orientations[:n_sub].float().contiguous(), exp_p.orientations.float().contiguous(),
+                          11, 11)
+    b = disori_angle_laue(exp.orientations.float().contiguous(), truth, 11, 11)
+    # end to end from pinned host patterns
+    e2e = None
+    if not args.no_e2e:
+        host = torch.empty(pats.shape, dtype=torch.float32, pin_memory=True)
+        host.copy_(pats)
+        exp_h = ExperimentPatterns(host)
+        torch.manual_seed(0)
+        pca_dictionary_index_orientations(mp, geom, exp_h, **kw)
+        torch.cuda.synchronize()
+        h0 = time.perf_counter()
+        e2e_steps = max(1, args.steps // 2)
+        for _ in range(e2e_steps):
+            torch.manual_seed(0)
+            pca_dictionary_index_orientations(mp, geom, exp_h, **kw)
+            q_out = exp_h.raw_indexing_results[0][0].cpu()
+            m_out = exp_h.raw_indexing_results[0][1].cpu()
+        torch.cuda.synchronize()
+        e2e = {"value": wl["Q"] * e2e_steps / (time.perf_counter() - h0), "unit": UNIT,
+               "h2d_bytes_per_step": int(host.numel() * 4), "d2h_bytes_per_step": int(q_out.numel() * 4 +
+                                                                                   m_out.numel() * 4),
+               "host_memory": "pinned"}
+        del exp_h, host
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": f"PCA DI 128x128 px, {n_comp} components fitted on the m-3m {learn_res} deg dictionary "
+                               f"({fit['learn_rows']:,}), indexing {D:,} rows, {wl['Q']:,} patterns, top-{wl['k']}",
+                   "precision": "PCA projections FP32-class (3-term bf16 split on tcgen05); bf16 match + FP32 "
+                                "re-score of top-32 in PCA space",
+                   "l2": "inputs larger than L2"},
+        "e2e": e2e,
+        "gpu_launches": int(launches * args.steps),
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_tc_gemm (match + streaming top-k, K=1024)",
+                     "peak_source": f"{peak_kind} bf16_tflops_sustained",
+                     "share_of_step": sum(match_ms) / 1e3 / t},
+        "projection": {"share_of_step": sum(proj_ms) / 1e3 / t,
+                       "tflops_fp32_equivalent": sum(proj_fl) / (sum(proj_ms) / 1e3) / 1e12,
+                       "max_rel_error_vs_fp64": proj_err,
+                       "how": "3-term bf16 split (x = hi + lo) of rows and components, one tcgen05 GEMM over 3K"},
+        "algorithmic_flops_per_pattern": {"match_2DK": 2.0 * D * n_comp, "query_projection_2PK": 2.0 * P * n_comp,
+                                          "dictionary_projection_amortised": 2.0 * D * P * n_comp / wl["Q"]},
+        "fit_one_time": fit,
+        "accuracy": {"within_0.5deg_of_plain_di": float((a < math.radians(0.5)).float().mean()),
+                     "same_top1_orientation_as_plain_di": float(
+                         ((exp.orientations[:n_sub].float() - exp_p.orientations.float()).abs().amax(1) < 1e-5)
+                         .float().mean()),
+                     "subset": n_sub, "within_0.5deg_of_truth": float((b < math.radians(0.5)).float().mean())},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_batched(args):
     """Many scan maps of uneven size, detector shape and phase in
     one planned batch (BatchIndexer), replayed as one CUDA graph. Patterns
@@ -1158,12 +1396,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
+    ap.add_argument("--no-learned", action="store_true", help="skip the companion learned-path measurement")
     ap.add_argument("--fp32-subset", type=int, default=8192)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (48 maps, mixed sizes, detectors, phases) instead")
     ap.add_argument("--refine", action="store_true", help="time orientation grid refinement after DI instead")
     ap.add_argument("--preprocess", action="store_true", help="time pattern preprocessing (clean + NLPAR) instead")
     ap.add_argument("--pcfit", action="store_true", help="time pattern-centre fitting instead")
+    ap.add_argument("--pca", action="store_true", help="time PCA dictionary indexing (1,024 components) instead")
     ap.add_argument("--train-steps", type=int, default=3000)
     ap.add_argument("--max-angle", type=float, default=16.0)
     ap.add_argument("--fallback-ratio", type=float, default=0.95)
@@ -1183,6 +1423,8 @@ def main():
         run_preprocess(args)
     elif args.pcfit:
         run_pcfit(args)
+    elif args.pca:
+        run_pca(args)
     else:
         run_ours(args, wl)
 

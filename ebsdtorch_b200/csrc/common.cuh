@@ -129,8 +129,11 @@ static inline int build_laue_table(int laue, LaueTable* t) {
 // Device helpers
 // ---------------------------------------------------------------------------
 
-// Upper bound on any spin-wait inside a kernel. A wait that exceeds it sets
-// the caller's status word to EBSD_DEVICE_TIMEOUT and the kernel unwinds.
+// Default upper bound on any spin-wait inside a kernel (kernels take the
+// limit as a parameter; ebsd_set_wait_limit_ns changes it). A wait that
+// exceeds it sets the caller's status word to EBSD_DEVICE_TIMEOUT and the
+// kernel unwinds. Waits for a CTA's own copies and MMAs before it exits
+// always use this default.
 constexpr uint64_t kWaitLimitNs = 4000000000ull;  // 4 s
 
 __device__ __forceinline__ uint64_t globaltimer_ns() {
@@ -241,8 +244,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait on an mbarrier phase. Returns false when the wait limit
-// expired or when *abort became non-zero (another role gave up).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+// (limit_ns, counted after a short spin) expired or when *abort became
+// non-zero (another role gave up).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                          uint64_t limit_ns = kWaitLimitNs) {
 #pragma unroll 1
   for (int i = 0; i < 256; ++i)
     if (mbar_try_wait(bar, parity)) return true;
@@ -251,14 +256,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
   }
 }
 
 // As mbar_wait, for waits expected to last many microseconds (the epilogue
 // waiting for a whole accumulator): after a short spin the thread sleeps
 // between polls instead of issuing back-to-back try_waits.
-__device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity, volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity, volatile int* abort,
+                                                uint64_t limit_ns = kWaitLimitNs) {
 #pragma unroll 1
   for (int i = 0; i < 32; ++i)
     if (mbar_try_wait(bar, parity)) return true;
@@ -267,7 +273,7 @@ __device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity, v
   while (true) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (globaltimer_ns() - t0 > kWaitLimitNs) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
     __nanosleep(500);
   }
 }

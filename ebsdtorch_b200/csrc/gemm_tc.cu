@@ -17,8 +17,11 @@
 //               registers across all dictionary tiles of its range.
 // A unit of work is (query tile, dictionary range); the epilogue of tile t
 // overlaps the MMAs of tile t+1 through the second accumulator.
-// Every wait is bounded (common.cuh); a timeout is reported in *status.
+// Every wait is bounded (p.wait_ns); a timeout is reported in *status. When
+// any role gives up, the CTA still lets every TMA copy and MMA it issued
+// complete (bounded by the default limit) before it releases TMEM and exits.
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -39,8 +42,9 @@ struct Tile {
   static constexpr int STAGES = BN_ == 256 ? 4 : 6;
   static constexpr int B_BYTES = BN_ * BKB;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 1) + 16;
-  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + BAR_BYTES;
+  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 2) + 16;
+  static constexpr int PACE_BYTES = 8 * 256;  // fetched pacing slots (kPaceSlots)
+  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + PACE_BYTES + BAR_BYTES;
   static constexpr uint32_t TMEM_COLS = 2 * BN_;  // two accumulators
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 };
@@ -68,7 +72,54 @@ struct GemmParams {
   int64_t ld_out;
   int relu;
   int* status;
+  uint64_t wait_ns;  // limit of every role's waits (kWaitLimitNs by default)
+  // Pacing of one-wave match launches (0 = off): every kPaceEvery stages a
+  // producer publishes its stage count and lets CTAs more than pace_window
+  // stages behind catch up (bounded by kPaceMaxWaitNs).
+  int pace_window;
+  uint32_t pace_epoch;
 };
+
+// Stage counts published by the producers of paced launches, one slot per
+// CTA: (epoch << 32) | stages issued. A launch only reads slots stamped with
+// its own epoch, so stale or foreign entries are ignored. 2 KB per device,
+// part of the module image.
+constexpr int kPaceSlots = 256;
+constexpr int kPaceEvery = 32;              // stages between two checkpoints
+constexpr uint64_t kPaceMaxWaitNs = 20000;  // longest wait at one checkpoint
+static __device__ __align__(16) unsigned long long g_pace[kPaceSlots];
+
+__device__ __forceinline__ void pace_publish(int slot, uint32_t epoch, uint32_t stages) {
+  const unsigned long long v = ((unsigned long long)epoch << 32) | stages;
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(g_pace + slot), "l"(v) : "memory");
+}
+
+// Untiled bulk copy of the first `bytes` of g_pace into shared memory,
+// completion signalled on `bar` (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void pace_fetch(uint32_t dst, uint32_t bytes, uint32_t bar) {
+  mbar_arrive_expect_tx(bar, bytes);
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"((uint64_t)__cvta_generic_to_global(g_pace)), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+// Largest lag behind `stages` among the fetched slots of this launch's
+// epoch, ignoring CTAs more than `far` stages behind (a CTA that started
+// late cannot catch up within a checkpoint).
+__device__ __forceinline__ uint32_t pace_lag(const unsigned long long* slots, int n, uint32_t epoch,
+                                             uint32_t stages, uint32_t far) {
+  uint32_t lag = 0;
+#pragma unroll 8
+  for (int i = 0; i < n; ++i) {
+    const unsigned long long v = slots[i];
+    if ((uint32_t)(v >> 32) != epoch) continue;
+    const uint32_t st = (uint32_t)v;
+    const uint32_t d = st < stages ? stages - st : 0u;
+    if (d <= far && d > lag) lag = d;
+  }
+  return lag;
+}
 
 template <int KIND, int BN>
 __host__ __device__ constexpr uint32_t make_idesc() {
@@ -114,14 +165,17 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
   const uint32_t sbase = smem_u32(smem);
   float* scratch = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
+  unsigned long long* pace_slots =
+      reinterpret_cast<unsigned long long*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES + T::PACE_BYTES);
   const uint32_t bar0 = smem_u32(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
   auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
   auto accf_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
   auto acce_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
   const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  const uint32_t pace_bar = bar0 + 8u * (2 * STAGES + 5);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 6);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -149,6 +203,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(acce_bar(a), EPI_THREADS);
     }
     mbar_init(drain_bar, 1);
+    mbar_init(pace_bar, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -162,22 +217,59 @@ __global__ void __launch_bounds__(THREADS, 1)
   tc_fence_after();
   const uint32_t tmem_base = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
 
+  const uint64_t wait_ns = p.wait_ns;
+  // producer progress (warp 0, lane 0) and whether any MMA was issued (warp 1,
+  // lane 0): read by the drain after the roles when a role gave up
+  uint32_t prod_stage = 0, prod_phase = 0;
+  int64_t issued = 0;
+  bool any_mma = false;
+
   if (warp == 0) {
     // ---------------- TMA producer ----------------
     if (lane == 0) {
       uint32_t stage = 0, phase = 0;
-      int64_t issued = 0;
       bool ok = true;
       const int k_iters = p.k_iters;
+      const int pace_window = PERSIST ? 0 : p.pace_window;
+      const uint32_t pace_epoch = p.pace_epoch;
+      // pacing: the slots are fetched asynchronously at one checkpoint and
+      // read at the next, so an on-time CTA never waits for the fetch
+      const int pace_n = (int)gridDim.x;
+      const uint32_t pace_bytes = (uint32_t)((pace_n + 1) / 2) * 16u;
+      const uint32_t pace_dst = smem_u32(pace_slots);
+      uint32_t pace_phase = 0;
+      bool pace_pending = false;
+      volatile int pace_never = 0;
+      auto pace_collect = [&]() -> uint32_t {
+        mbar_wait(pace_bar, pace_phase, &pace_never);
+        pace_phase ^= 1u;
+        pace_pending = false;
+        return pace_lag(pace_slots, pace_n, pace_epoch, (uint32_t)issued, 8u * (uint32_t)pace_window);
+      };
       auto produce_unit = [&](int u) {
         const int a_row = unit_tile(u) * BM;
         int n_begin, n_end;
         unit_range(u, n_begin, n_end);
         for (int n = n_begin; n < n_end && ok; ++n) {
           for (int k = 0; k < k_iters; ++k) {
-            if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag)) {
+            if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, wait_ns)) {
               ok = false;
               break;
+            }
+            if (pace_window > 0 && (issued & (kPaceEvery - 1)) == 0 && issued > 0) {
+              uint32_t lag = pace_pending ? pace_collect() : 0u;
+              if (lag > (uint32_t)pace_window) {
+                const uint64_t t0 = globaltimer_ns();
+                while (lag > (uint32_t)pace_window && globaltimer_ns() - t0 < kPaceMaxWaitNs) {
+                  __nanosleep(256);
+                  pace_fetch(pace_dst, pace_bytes, pace_bar);
+                  pace_pending = true;
+                  lag = pace_collect();
+                }
+              }
+              pace_publish(blockIdx.x, pace_epoch, (uint32_t)issued);
+              pace_fetch(pace_dst, pace_bytes, pace_bar);
+              pace_pending = true;
             }
             const uint32_t a_dst = sbase + stage * STAGE_BYTES;
             mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
@@ -199,22 +291,10 @@ __global__ void __launch_bounds__(THREADS, 1)
       } else {
         produce_unit(blockIdx.x);
       }
-      if (!ok) {
-        report_timeout(p, abort_flag);
-        // let the copies already in flight land before the CTA exits
-        const int64_t inflight = issued < STAGES ? issued : (int64_t)STAGES;
-        uint32_t s = stage, ph = phase;
-        for (int64_t i = 0; i < inflight; ++i) {
-          if (s == 0) {
-            s = STAGES - 1;
-            ph ^= 1u;
-          } else {
-            --s;
-          }
-          volatile int never = 0;
-          mbar_wait(full_bar(s), ph, &never);
-        }
-      }
+      if (!ok) report_timeout(p, abort_flag);
+      if (pace_pending) pace_collect();  // the last slot fetch lands before the CTA exits
+      prod_stage = stage;
+      prod_phase = phase;
     }
     __syncwarp();
   } else if (warp == 1) {
@@ -223,21 +303,21 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t stage = 0, phase = 0;
       int acc = 0;
       uint32_t acc_phase = 0;
-      bool ok = true, any = false;
+      bool ok = true;
       constexpr uint32_t idesc = make_idesc<KIND, BN>();
       const int k_iters = p.k_iters;
       auto mma_unit = [&](int u) {
         int n_begin, n_end;
         unit_range(u, n_begin, n_end);
         for (int n = n_begin; n < n_end && ok; ++n) {
-          if (!mbar_wait(acce_bar(acc), acc_phase ^ 1u, abort_flag)) {
+          if (!mbar_wait(acce_bar(acc), acc_phase ^ 1u, abort_flag, wait_ns)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t d_tmem = tmem_base + (uint32_t)(acc * BN);
           for (int k = 0; k < k_iters; ++k) {
-            if (!mbar_wait(full_bar(stage), phase, abort_flag)) {
+            if (!mbar_wait(full_bar(stage), phase, abort_flag, wait_ns)) {
               ok = false;
               break;
             }
@@ -249,7 +329,7 @@ __global__ void __launch_bounds__(THREADS, 1)
               tc_mma<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32),
                            idesc, (k | kk) != 0 ? 1u : 0u);
             }
-            any = true;
+            any_mma = true;
             tc_commit(empty_bar(stage));
             if (++stage == STAGES) {
               stage = 0;
@@ -269,15 +349,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       } else {
         mma_unit(blockIdx.x);
       }
-      if (!ok) {
-        report_timeout(p, abort_flag);
-        if (any) {
-          // wait for the MMAs already issued before TMEM is released
-          tc_commit(drain_bar);
-          volatile int never = 0;
-          mbar_wait(drain_bar, 0, &never);
-        }
-      }
+      if (!ok) report_timeout(p, abort_flag);
     }
     __syncwarp();
   } else {
@@ -302,7 +374,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bi[j] = -1;
       }
       for (int n = n_begin; n < n_end; ++n) {
-        bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag);
+        bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag, wait_ns);
         got = __all_sync(0xffffffffu, got);
         if (!got) {
           ok = false;
@@ -405,6 +477,31 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (!ok && lane == 0) report_timeout(p, abort_flag);
   }
 
+  // Every role has finished. If one gave up, the others may have stopped
+  // with work in flight: the producer's last copies (up to STAGES of them;
+  // earlier ones were consumed by the MMA thread) and the MMA thread's last
+  // MMAs. Wait for both, with the default limit and no abort, before shared
+  // memory and TMEM are released.
+  __syncthreads();
+  if (*abort_flag) {
+    volatile int never = 0;
+    if (warp == 0 && lane == 0) {
+      const int64_t inflight = issued < STAGES ? issued : (int64_t)STAGES;
+      uint32_t s = prod_stage, ph = prod_phase;
+      for (int64_t i = 0; i < inflight; ++i) {
+        if (s == 0) {
+          s = STAGES - 1;
+          ph ^= 1u;
+        } else {
+          --s;
+        }
+        mbar_wait(full_bar(s), ph, &never);
+      }
+    } else if (warp == 1 && lane == 0 && any_mma) {
+      tc_commit(drain_bar);
+      mbar_wait(drain_bar, 0, &never);
+    }
+  }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
@@ -421,6 +518,17 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// Wait limit handed to every tensor-core kernel launch (0 = kWaitLimitNs).
+static std::atomic<uint64_t> g_wait_limit_ns{0};
+// Pacing of one-wave match launches: on (1) by default; epoch per launch.
+static std::atomic<int> g_pacing{1};
+static std::atomic<uint32_t> g_pace_epoch{0};
+
+static uint64_t wait_limit_ns() {
+  const uint64_t v = g_wait_limit_ns.load(std::memory_order_relaxed);
+  return v ? v : kWaitLimitNs;
+}
 
 static EncodeTiledFn encode_fn() {
   static EncodeTiledFn fn = nullptr;
@@ -463,11 +571,13 @@ static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t ro
 }
 
 template <int KIND, int MODE, int KC, int BN, bool PERSIST = false>
-static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
+static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p_in, int grid,
                   cudaStream_t s) {
   auto kern = k_tc_gemm<KIND, MODE, KC, BN, PERSIST>;
   constexpr int smem = Tile<BN>::SMEM_BYTES;
   EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  GemmParams p = p_in;
+  p.wait_ns = wait_limit_ns();
   kern<<<grid, THREADS, smem, s>>>(a, b, p);
   EBSD_LAUNCH_CHECK();
   return 0;
@@ -520,6 +630,15 @@ static int check_operands(const void* A, int64_t m_pad, const void* B, int64_t n
 }  // namespace ebsd
 
 using namespace ebsd;
+
+extern "C" int64_t ebsd_set_wait_limit_ns(int64_t ns) {
+  const uint64_t prev = g_wait_limit_ns.exchange(ns > 0 ? (uint64_t)ns : 0u);
+  return prev ? (int64_t)prev : (int64_t)kWaitLimitNs;
+}
+
+extern "C" int ebsd_set_match_pacing(int on) {
+  return g_pacing.exchange(on ? 1 : 0);
+}
 
 extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
   // One wave: query tiles x dictionary ranges ~= number of SMs, so all units
@@ -575,6 +694,13 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   // loops over its units
   const bool persist = max_ctas > 0 && max_ctas < p.units;
   const int grid = persist ? max_ctas : p.units;
+  // pace one-wave launches over long rows: all CTAs are resident together
+  // and each streams many stages of shared operand tiles
+  if (!persist && g_pacing.load(std::memory_order_relaxed) && grid <= device_sm_count() && grid < kPaceSlots &&
+      p.k_iters >= 64) {
+    p.pace_window = p.k_iters / 2;
+    p.pace_epoch = g_pace_epoch.fetch_add(1, std::memory_order_relaxed) + 1;
+  }
   cudaStream_t s = as_stream(stream);
   return lp_dtype == EBSD_DT_BF16 ? launch_topk_shape<0>(n_cand, tile_n, persist, ta, tb, p, grid, s)
                                   : launch_topk_shape<1>(n_cand, tile_n, persist, ta, tb, p, grid, s);

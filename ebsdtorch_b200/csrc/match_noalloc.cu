@@ -31,7 +31,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 // Device address of g_noalloc_scratch per device. In host code the symbol is
 // only a host-side stand-in, so the address is looked up once per device,
-// with that device current, and cached.
+// with that device current, and cached. The cache is keyed by device ordinal
+// and is valid for the runtime's primary context only: a cudaDeviceReset, or
+// a caller running on another driver context, would leave a stale address.
+// The first lookup may load the module (lazy loading), which allocates the
+// array; callers make one warm-up call at set-up time.
 static void* g_scratch_addr[kMaxDevices] = {nullptr};
 static std::mutex g_scratch_mu;
 

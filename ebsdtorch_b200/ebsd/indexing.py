@@ -233,7 +233,7 @@ def dictionary_index_orientations(
 
 
 def fit_pca_components(mp_t: Tensor, rays: Tensor, ori_learn: Tensor, n_components: int,
-                       component_slice: str = "top") -> Tensor:
+                       component_slice: str = "top", timings: Optional[dict] = None) -> Tensor:
     """PCA basis of the zero-mean simulated patterns of `ori_learn`
     (indexing.py:290-355, pca_covmat.py:94-158). The covariance is an
     FP32-class product on the tensor cores (3-term bf16 split) of the
@@ -242,8 +242,12 @@ def fit_pca_components(mp_t: Tensor, rays: Tensor, ori_learn: Tensor, n_componen
 
     component_slice "top": the n leading eigenvectors. "reference": the
     reference's slice ``[:, -n : -n + 300]`` (indexing.py:355), which keeps at
-    most 300 and, for P' >= 300 and n < 300, none."""
+    most 300 and, for P' >= 300 and n < 300, none. `timings`, when given,
+    receives the seconds of the covariance and of the eigendecomposition."""
+    import time
+
     dev = mp_t.device
+    t0 = time.perf_counter()
     N, P = ori_learn.shape[0], rays.shape[1]
     if N < 2:
         raise ValueError("PCA needs at least two learning orientations")
@@ -259,8 +263,13 @@ def fit_pca_components(mp_t: Tensor, rays: Tensor, ori_learn: Tensor, n_componen
     del A3, B3
     if int(status.item()) != 0:
         raise RuntimeError("covariance GEMM reported a device timeout")
+    t1 = time.perf_counter()
     _, vecs = torch.linalg.eigh(cov)
     del cov
+    if timings is not None:
+        torch.cuda.synchronize(dev)
+        timings["covariance_s"] = t1 - t0
+        timings["eigh_s"] = time.perf_counter() - t1
     if component_slice == "reference":
         V = vecs[:, -n_components:(-n_components + 300)]
     elif component_slice == "top":
@@ -272,6 +281,11 @@ def fit_pca_components(mp_t: Tensor, rays: Tensor, ori_learn: Tensor, n_componen
             f"the reference component slice [-{n_components}:{300 - n_components}] selects no components "
             f"for {P} pixels; use component_slice='top'")
     return V.t().contiguous()
+
+
+# When set to a list, _Projector appends (start, end, flops) CUDA-event
+# triples around every projection (split + GEMM; measurement only).
+PROJ_TIMERS: Optional[list] = None
 
 
 class _Projector:
@@ -286,8 +300,15 @@ class _Projector:
 
     def __call__(self, X: Tensor, out: Tensor) -> None:
         n = X.shape[0]
+        timers = PROJ_TIMERS
+        if timers is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         A3 = kernels.split3(X, 0, False, self.seg, round_up(n, kernels.TILE_Q), 3 * self.seg)
         kernels.gemm_nt(A3, self.B3, out, m_valid=n, n_valid=self.n_comp, status=self.status)
+        if timers is not None:
+            ev[1].record()
+            timers.append((ev[0], ev[1], 2.0 * n * self.P * self.n_comp))
 
 
 def _finish_rows(Y: Tensor, bufs: RowBuffers):
@@ -322,9 +343,14 @@ def pca_dictionary_index_orientations(
     device=None,
     workspace_bytes: Optional[int] = None,
     sub_chunk: int = 16384,
+    components=None,
 ) -> None:
     """PCA dictionary indexing (indexing.py:214-476). See the module doc and
-    fit_pca_components for ``component_slice``."""
+    fit_pca_components for ``component_slice``. ``components``: optional
+    basis from an earlier call (``experiment_patterns.pca_components`` -- one
+    (n_comp, P') float32 tensor, or a list with one per master pattern) that
+    is used instead of fitting one; the learning dictionary is then not
+    built."""
     _check_common(distance_metric, average_pattern_center)
     if not isinstance(master_patterns, (list, tuple)):
         master_patterns = [master_patterns]
@@ -337,10 +363,22 @@ def pca_dictionary_index_orientations(
             mp_t = _master_pattern_tensor(mp, virtual_binning, dev)
             pix_index = _pix_index(signal_mask, dev)
             P = rays.shape[1]
-            ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_learn_deg, dev)
-            comps = fit_pca_components(mp_t, rays, ori, int(n_pca_components), component_slice)
-            if dictionary_resolution_learn_deg != dictionary_resolution_index_deg:
-                ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_index_deg, dev)
+            given = components[i] if isinstance(components, (list, tuple, dict)) else components
+            if given is None:
+                ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_learn_deg, dev)
+                comps = fit_pca_components(mp_t, rays, ori, int(n_pca_components), component_slice)
+                if dictionary_resolution_learn_deg != dictionary_resolution_index_deg:
+                    ori = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_index_deg, dev)
+            else:
+                comps = given.to(device=dev, dtype=torch.float32).contiguous()
+                if comps.dim() != 2 or comps.shape[1] != P:
+                    raise ValueError(f"components must be (n_comp, {P}) for this detector, got {tuple(comps.shape)}")
+                # the reference draws the learning dictionary's permutation
+                # first: keep the global generator in step with it
+                ori_learn = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_learn_deg, dev)
+                ori = ori_learn if dictionary_resolution_learn_deg == dictionary_resolution_index_deg else \
+                    sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_index_deg, dev)
+                del ori_learn
             proj = _Projector(comps)
             n_comp = comps.shape[0]
             pats = _pattern_source(experiment_patterns, dev)

@@ -12,7 +12,10 @@
  *
  * Conventions
  *  - All pointers are device pointers unless stated otherwise; buffers are
- *    allocated by the caller. The library allocates no device memory.
+ *    allocated by the caller. The library makes no device allocation of its
+ *    own, with one exception: the 32 MiB file-scope scratch array of
+ *    ebsd_match_topk_noalloc, which every GPU that loads the library holds
+ *    until the process exits.
  *  - Work is enqueued on `stream` (a cudaStream_t passed as void*); calls are
  *    asynchronous unless stated otherwise.
  *  - Return value: 0 success, > 0 argument error (nothing launched),
@@ -161,6 +164,26 @@ int ebsd_avg_pool(const float* in, int64_t n, int height, int width, int binning
  *   part_val/part_idx[(q * part_slots + slot_base + range) * n_cand + j].
  * part_slots >= slot_base + splits. */
 int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad);
+
+/* No counterpart in the reference (which has no device-side waits): sets the
+ * limit, in nanoseconds, of every bounded wait inside the tensor-core kernels
+ * launched after the call (ebsd_match_topk*, ebsd_gemm_nt, ebsd_cnn_conv_fwd
+ * and the allocation-free match); ns <= 0 restores the default of 4 s.
+ * Returns the previous limit. A wait that runs out stores
+ * EBSD_DEVICE_TIMEOUT in the call's status word, and the kernel returns
+ * after its own copies and MMAs have completed, leaving the context usable.
+ * Meant for tests and for callers that want a tighter watchdog. */
+int64_t ebsd_set_wait_limit_ns(int64_t ns);
+
+/* No counterpart in the reference: switches pacing of one-wave match launches
+ * on (1, the default) or off (0); returns the previous setting. With pacing,
+ * the CTAs of a launch that stream long rows (>= 64 stages per tile) publish
+ * their progress every 32 stages in a 2 KB module array and a CTA that is more
+ * than half a tile ahead of another waits (at most 20 us per checkpoint), so
+ * the CTAs that share operand tiles read them from L2 rather than DRAM.
+ * Results do not depend on it. */
+int ebsd_set_match_pacing(int on);
+
 int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
                     int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
                     const float* col_scale, int n_cand, int splits, float* part_val,
@@ -220,9 +243,15 @@ int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n
  * larger calls are rejected with EBSD_ERR_ARG. No cudaMalloc, cudaFree or
  * allocating library routine is called. The first call on each device looks
  * up the array's device address (cudaGetSymbolAddress, with that device
- * current); make that first call before any stream capture. All calls share
- * the array and it keeps the last call's contents: calls that overlap on the
- * GPU race and must be serialised by the caller. */
+ * current); make that first call before any stream capture. Under CUDA's
+ * lazy module loading (the default) that first lookup also loads the module,
+ * which allocates the array and can block or fail for lack of memory: make
+ * one warm-up call at set-up time, not from the callback that must not
+ * block. The address is cached per device ordinal for the runtime's primary
+ * context: other driver contexts and use after cudaDeviceReset are not
+ * supported. All calls share the array and it keeps the last call's
+ * contents: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
 int ebsd_match_topk_noalloc(const void* queries_lp, int64_t n_queries, int64_t n_queries_pad,
                             const void* dict_lp, int64_t n_dict_pad, int64_t n_dict_valid,
                             int64_t k_pad, int lp_dtype, const float* col_scale,

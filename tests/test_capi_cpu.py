@@ -95,3 +95,31 @@ def test_preprocessing_and_fitting_argument_errors_need_no_gpu():
         _capi.call("ebsd_pcfit_prep", fake, 2, 16, 16, 20, 20, 5, 0, 1, fake, None)
     with pytest.raises(ValueError, match="bad sizes"):
         _capi.call("ebsd_pcfit_reduce", fake, 0, 4, 8, 8, 0, fake, fake, None)
+
+
+def test_noalloc_argument_checks_need_no_gpu():
+    """ebsd_match_topk_noalloc rejects bad arguments on the host, before any
+    CUDA call: k_out outside 1..64, more queries than padded rows, null
+    outputs, and padded query counts whose candidate lists would not fit the
+    fixed 32 MiB scratch. The rejection message states the largest padded
+    query count that fits for that k (32 MiB - 256 B over 8 B per candidate
+    slot, rounded to a power-of-two candidate count)."""
+    lib = _capi.load()
+    fake = 256  # never dereferenced: every call below fails its argument check
+
+    def call(nq, nq_pad, k, out_val=fake, out_idx=fake):
+        return lib.ebsd_match_topk_noalloc(fake, nq, nq_pad, fake, 256, 256, 64, _capi.DT_BF16, None, None, k,
+                                           out_val, out_idx, None, None)
+
+    for k in (0, 65, -1):
+        assert call(128, 128, k) == 1 and "k_out" in _capi.last_error()
+    assert call(129, 128, 8) == 1 and "n_queries" in _capi.last_error()
+    assert call(0, 128, 8) == 1 and "n_queries" in _capi.last_error()
+    assert call(128, 128, 8, out_val=None) == 1 and "null output" in _capi.last_error()
+    assert call(128, 128, 8, out_idx=None) == 1 and "null output" in _capi.last_error()
+    cap = (32 << 20) - 256
+    for k, n_cand in ((1, 1), (64, 64), (5, 8)):
+        most = cap // (8 * n_cand)
+        assert call(128, most + 1, k) == 1
+        msg = _capi.last_error()
+        assert "scratch" in msg and f"at most {most} padded queries" in msg, msg

@@ -6,11 +6,11 @@ consecutive calls that reuse its fixed device scratch array.
 
 Kept in its own file, named to be collected after every other test file."""
 
-import ctypes as C
-
 import numpy as np
 import pytest
 import torch
+
+from oracle import di_oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -51,31 +51,71 @@ def _existing_path(lib, q_lp, nq, d_lp, nd, col_scale, k):
     return idx.cpu().numpy(), val.cpu().numpy()
 
 
+def _case(nq, nd, p, seed):
+    nq_pad, nd_pad, k_pad = -(-nq // 128) * 128, -(-nd // 256) * 256, -(-p // 64) * 64
+    d64, d_lp, d_norm = _rows(nd, nd_pad, k_pad, p, seed)
+    _, q_lp, _ = _rows(nq, nq_pad, k_pad, p, seed + 1, like=d64, noise=0.5)
+    col_scale = torch.zeros(nd_pad, dtype=torch.float32, device=DEV)
+    col_scale[:nd] = d_norm
+    return dict(nq=nq, nd=nd, nq_pad=nq_pad, nd_pad=nd_pad, k_pad=k_pad, q_lp=q_lp, d_lp=d_lp, col_scale=col_scale)
+
+
+def _noalloc(lib, c, k):
+    from ebsdtorch_b200 import _capi
+
+    val = torch.full((c["nq"], k), float("nan"), dtype=torch.float32, device=DEV)
+    idx = torch.full((c["nq"], k), -7, dtype=torch.int64, device=DEV)
+    st = torch.full((1,), 123, dtype=torch.int32, device=DEV)
+    rc = lib.ebsd_match_topk_noalloc(c["q_lp"].data_ptr(), c["nq"], c["nq_pad"], c["d_lp"].data_ptr(), c["nd_pad"],
+                                     c["nd"], c["k_pad"], _capi.DT_BF16, c["col_scale"].data_ptr(), None, k,
+                                     val.data_ptr(), idx.data_ptr(), st.data_ptr(),
+                                     torch.cuda.current_stream().cuda_stream)
+    assert rc == 0, _capi.last_error()
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    return idx.cpu().numpy(), val.cpu().numpy()
+
+
+def _check(got, ref):
+    (gi, gv), (ri, rv) = got, ref
+    assert (gi == ri).mean() >= 0.999
+    assert np.abs(gv - rv).max() <= 1e-5 * np.abs(rv).max()
+
+
 @pytest.mark.parametrize("nq,nd,p,k", [(1000, 5000, 300, 8), (77, 700, 64, 1)])
 def test_noalloc_matches_existing_entry_points(nq, nd, p, k):
     from ebsdtorch_b200 import _capi
 
     lib = _capi.load()
-    nq_pad, nd_pad, k_pad = -(-nq // 128) * 128, -(-nd // 256) * 256, -(-p // 64) * 64
-    d64, d_lp, d_norm = _rows(nd, nd_pad, k_pad, p, 1)
-    _, q_lp, _ = _rows(nq, nq_pad, k_pad, p, 2, like=d64, noise=0.5)
-    col_scale = torch.zeros(nd_pad, dtype=torch.float32, device=DEV)
-    col_scale[:nd] = d_norm
-    ref_i, ref_v = _existing_path(lib, q_lp, nq, d_lp, nd, col_scale, k)
-    s = torch.cuda.current_stream().cuda_stream
+    c = _case(nq, nd, p, 1)
+    ref = _existing_path(lib, c["q_lp"], nq, c["d_lp"], nd, c["col_scale"], k)
     for _ in range(2):  # two calls in a row share the fixed scratch
-        val = torch.full((nq, k), float("nan"), dtype=torch.float32, device=DEV)
-        idx = torch.full((nq, k), -7, dtype=torch.int64, device=DEV)
-        st = torch.full((1,), 123, dtype=torch.int32, device=DEV)
-        rc = lib.ebsd_match_topk_noalloc(q_lp.data_ptr(), nq, nq_pad, d_lp.data_ptr(), nd_pad, nd, k_pad,
-                                         _capi.DT_BF16, col_scale.data_ptr(), None, k, val.data_ptr(),
-                                         idx.data_ptr(), st.data_ptr(), s)
-        assert rc == 0, _capi.last_error()
-        torch.cuda.synchronize()
-        assert int(st.item()) == 0
-        got_i, got_v = idx.cpu().numpy(), val.cpu().numpy()
-        assert (got_i == ref_i).mean() >= 0.999
-        assert np.abs(got_v - ref_v).max() <= 1e-5 * np.abs(ref_v).max()
+        _check(_noalloc(lib, c, k), ref)
+    # and both agree with the oracle's exact top-k of the same bf16 rows
+    q = c["q_lp"][:nq].double().cpu().numpy()
+    d = (c["d_lp"][:nd].double() * c["col_scale"][:nd, None].double()).cpu().numpy()
+    oi, ov = O.topk_dot(q, d, k)
+    gi, gv = ref
+    assert (gi[:, 0] == oi[:, 0]).mean() >= 0.999
+    assert np.abs(gv - ov).max() <= 1e-5 * np.abs(ov).max()
+
+
+def test_noalloc_ignores_leftovers_of_larger_calls():
+    """Calls of different shapes on one stream: a large one (many padded
+    queries, a larger k, more candidate lists), a small one, the large one
+    again. Each must match the regular entry points on its own inputs, so
+    nothing a larger earlier call left in the shared scratch leaks into a
+    smaller later one."""
+    from ebsdtorch_b200 import _capi
+
+    lib = _capi.load()
+    big, small = _case(3000, 9000, 200, 11), _case(40, 600, 64, 21)
+    ref_big = _existing_path(lib, big["q_lp"], big["nq"], big["d_lp"], big["nd"], big["col_scale"], 32)
+    ref_small = _existing_path(lib, small["q_lp"], small["nq"], small["d_lp"], small["nd"], small["col_scale"], 3)
+    _check(_noalloc(lib, big, 32), ref_big)
+    _check(_noalloc(lib, small, 3), ref_small)
+    _check(_noalloc(lib, big, 32), ref_big)
+    _check(_noalloc(lib, small, 3), ref_small)
 
 
 def test_noalloc_rejects_oversized_calls():
