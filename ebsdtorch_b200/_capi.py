@@ -41,6 +41,8 @@ SIGNATURES = {
                                     vp, vp]),
     "ebsd_merge_rescore": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
                                  vp, vp, vp, vp, vp]),
+    "ebsd_merge_rescore_gated": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
+                                 vp, vp, vp, vp, f32, vp, vp]),
     "ebsd_gemm_nt": (i32, [vp, i64, vp, i64, i64, i32, f32, i32, vp, i64, i64, i64, i32, vp, vp]),
     "ebsd_col_mean": (i32, [vp, i64, i32, i64, vp, vp]),
     "ebsd_split3_bf16": (i32, [vp, i64, i32, i64, vp, i32, i32, vp, i64, i64, vp]),
@@ -87,7 +89,7 @@ LAUNCHES_PER_CALL = {
     "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
     "ebsd_prep_patterns": 1, "ebsd_prep_patterns_typed": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1,
     "ebsd_match_topk": 1, "ebsd_match_topk_tiled": 1,
-    "ebsd_merge_rescore": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
+    "ebsd_merge_rescore": 1, "ebsd_merge_rescore_gated": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
     "ebsd_disori_angle": 1, "ebsd_match_topk_noalloc": 2, "ebsd_zh_to_qu": 1, "ebsd_qu_to_zh": 1,
     "ebsd_cell_to_row": 2, "ebsd_local_search": 1, "ebsd_refine_grid": 1,
     "ebsd_pattern_mean": 2, "ebsd_subtract_pattern": 1, "ebsd_normalize_patterns": 1, "ebsd_clahe": 1,

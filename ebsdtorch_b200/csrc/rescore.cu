@@ -6,6 +6,16 @@
 // scores are the reference's metric: the FP32 dot product of the zero-mean
 // query row with the zero-mean dictionary row (knn.py:96-97).
 // One CTA per query; candidates are ordered by (score desc, index asc).
+//
+// Margin gate (gate_rel > 0): a candidate's low-precision score s' and its
+// exact score s (both per unit query norm) satisfy |s' - s| <= gate_rel * w,
+// w = |d| for the dot metric and 1 for cosine, when gate_rel bounds the
+// rounding of the unit rows and the FP32 accumulation (the caller derives it
+// from the element type and the row length). Let tau be the k_out-th largest
+// lower bound s' - gate_rel * w among the n_rescore best candidates. A
+// candidate whose upper bound s' + gate_rel * w is below tau cannot be among
+// the exact top k_out, so only the others are re-scored; the result equals
+// re-scoring all n_rescore.
 #include "common.cuh"
 
 namespace ebsd {
@@ -55,13 +65,18 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     int64_t d_base, int64_t d_rows, int n_pix, const float* __restrict__ q_norm, const float* __restrict__ d_norm,
     const float* __restrict__ q_lp_scale, int similarity, int n_rescore, int k_out,
     const float* __restrict__ run_val, const int64_t* __restrict__ run_idx, int sort_n,
-    float* __restrict__ out_val, int64_t* __restrict__ out_idx) {
+    float* __restrict__ out_val, int64_t* __restrict__ out_idx, float gate_rel,
+    unsigned long long* __restrict__ n_rescored) {
   extern __shared__ float dyn[];
   float* qrow = dyn;                                            // n_pix (re-score only)
   float* cv = dyn + (d_f32 ? ((n_pix + 3) & ~3) : 0);           // sort_n
   int64_t* ci = reinterpret_cast<int64_t*>(cv + ((sort_n + 1) & ~1));  // sort_n
   __shared__ float fin_v[kMaxRescore + kMaxKOut];
   __shared__ int64_t fin_i[kMaxRescore + kMaxKOut];
+  __shared__ float lb[kMaxRescore];
+  __shared__ int sel[kMaxRescore];
+  __shared__ float tau_s;
+  __shared__ int n_sel;
 
   const int64_t q = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
@@ -86,16 +101,52 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   // 2. exact FP32 scores of the best n_rescore (or approximate * |q|)
   const int nr = n_rescore;
   if (d_f32) {
+    // 2a. which of them can reach the exact top k_out (margin gate)
+    const bool gate = gate_rel > 0.0f && nr > k_out;
+    if (gate) {
+      float w = 0.0f;
+      if (tid < nr) {
+        const int64_t i = ci[tid];
+        const bool ok = i >= d_base && i < d_base + d_rows;
+        w = gate_rel * ((similarity == EBSD_SIM_DOT && ok) ? d_norm[i - d_base] : 1.0f);
+        lb[tid] = ok ? cv[tid] - w : -INFINITY;
+      }
+      if (tid == 0) n_sel = 0;
+      __syncthreads();
+      if (tid < nr) {
+        // tau: the k_out-th largest lower bound (rank selection, index order on ties)
+        const float v = lb[tid];
+        int rank = 0;
+        for (int o = 0; o < nr; ++o) rank += (lb[o] > v || (lb[o] == v && o < tid)) ? 1 : 0;
+        if (rank == k_out - 1) tau_s = v;
+      }
+      __syncthreads();
+      if (tid < nr) {
+        const bool keep = ci[tid] >= 0 && cv[tid] + w >= tau_s;
+        if (keep) sel[atomicAdd(&n_sel, 1)] = tid;
+        fin_v[tid] = -INFINITY;  // candidates left out stay out of the final selection
+        fin_i[tid] = -1;
+      }
+      __syncthreads();
+    } else {
+      for (int c = tid; c < nr; c += blockDim.x) sel[c] = c;
+      if (tid == 0) n_sel = nr;
+      __syncthreads();
+    }
+    const int ns = n_sel;
+    if (n_rescored && tid == 0) atomicAdd(n_rescored, (unsigned long long)ns);
     // four rows per warp at once (four 16-byte loads in flight per lane)
     constexpr int R = 4;
     const bool vec = (n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0;
-    for (int c0 = wid * R; c0 < nr; c0 += nw * R) {
+    for (int s0 = wid * R; s0 < ns; s0 += nw * R) {
       int64_t di[R];
       const float* d[R];
+      int cc[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        const int c = c0 + j;
-        di[j] = (c < nr && ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
+        cc[j] = s0 + j < ns ? sel[s0 + j] : -1;
+        const int c = cc[j];
+        di[j] = (c >= 0 && ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
         d[j] = d_f32 + (di[j] >= 0 ? di[j] - d_base : 0) * ld_d;  // a missing row re-reads row 0
       }
       float acc[R];
@@ -112,8 +163,8 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
       if (lane == 0) {
 #pragma unroll
         for (int j = 0; j < R; ++j) {
-          const int c = c0 + j;
-          if (c >= nr) break;
+          const int c = cc[j];
+          if (c < 0) break;
           float v = acc[j];
           if (similarity == EBSD_SIM_COSINE && di[j] >= 0) {
             const float den = q_norm[q] * d_norm[di[j] - d_base];
@@ -167,15 +218,15 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
 
 using namespace ebsd;
 
-extern "C" int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
-                                  int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
-                                  const float* d_f32, int64_t ld_d, int64_t d_index_base,
-                                  int64_t d_rows, int n_pix,
-                                  const float* q_norm, const float* d_norm, const float* q_lp_scale,
-                                  int similarity,
-                                  int n_rescore, int k_out, const float* run_val,
-                                  const int64_t* run_idx, float* out_val, int64_t* out_idx,
-                                  void* stream) {
+extern "C" int ebsd_merge_rescore_gated(const float* part_val, const int32_t* part_idx, int64_t n_queries,
+                                        int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
+                                        const float* d_f32, int64_t ld_d, int64_t d_index_base,
+                                        int64_t d_rows, int n_pix,
+                                        const float* q_norm, const float* d_norm, const float* q_lp_scale,
+                                        int similarity,
+                                        int n_rescore, int k_out, const float* run_val,
+                                        const int64_t* run_idx, float* out_val, int64_t* out_idx,
+                                        float gate_rel, unsigned long long* n_rescored, void* stream) {
   EBSD_ARG_CHECK(part_val && part_idx && out_val && out_idx, "ebsd_merge_rescore: null pointer");
   EBSD_ARG_CHECK(n_queries >= 0 && part_slots >= 1 && n_cand >= 1, "bad candidate-list sizes");
   const int n_list = part_slots * n_cand;
@@ -193,7 +244,10 @@ extern "C" int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx
     EBSD_ARG_CHECK(n_pix >= 1 && ld_q >= n_pix && ld_d >= n_pix, "bad re-score row length");
     EBSD_ARG_CHECK(n_pix <= 40960, "re-score row length %d exceeds 40960", n_pix);
     EBSD_ARG_CHECK(d_rows >= 1 && d_index_base >= 0, "bad dictionary row range");
+    EBSD_ARG_CHECK(!(gate_rel > 0.0f) || similarity == EBSD_SIM_COSINE || d_norm,
+                   "the margin gate of the dot metric needs d_norm");
   }
+  EBSD_ARG_CHECK(!(gate_rel < 0.0f) && gate_rel < 1.0f, "gate_rel %g outside [0, 1)", (double)gate_rel);
   if (n_queries == 0) return 0;
   int sort_n = 1;
   while (sort_n < n_list) sort_n <<= 1;
@@ -204,7 +258,21 @@ extern "C" int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx
   EBSD_ARG_CHECK(n_queries < INT32_MAX, "too many queries");
   k_merge_rescore<<<(int)n_queries, kMergeThreads, smem, as_stream(stream)>>>(
       part_val, part_idx, n_list, q_f32, ld_q, d_f32, ld_d, d_index_base, d_rows, n_pix, q_norm, d_norm, q_lp_scale,
-      similarity, n_rescore, k_out, run_val, run_idx, sort_n, out_val, out_idx);
+      similarity, n_rescore, k_out, run_val, run_idx, sort_n, out_val, out_idx, gate_rel, n_rescored);
   EBSD_LAUNCH_CHECK();
   return 0;
+}
+
+extern "C" int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
+                                  int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
+                                  const float* d_f32, int64_t ld_d, int64_t d_index_base,
+                                  int64_t d_rows, int n_pix,
+                                  const float* q_norm, const float* d_norm, const float* q_lp_scale,
+                                  int similarity,
+                                  int n_rescore, int k_out, const float* run_val,
+                                  const int64_t* run_idx, float* out_val, int64_t* out_idx,
+                                  void* stream) {
+  return ebsd_merge_rescore_gated(part_val, part_idx, n_queries, part_slots, n_cand, q_f32, ld_q, d_f32, ld_d,
+                                  d_index_base, d_rows, n_pix, q_norm, d_norm, q_lp_scale, similarity, n_rescore,
+                                  k_out, run_val, run_idx, out_val, out_idx, 0.0f, nullptr, stream);
 }

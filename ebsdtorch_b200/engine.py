@@ -30,6 +30,9 @@ MAX_MERGE_CANDIDATES = 4096  # per query, ebsd_merge_rescore's limit
 # When set to a list, Searcher.run appends (start, end, flops) CUDA-event
 # triples around every tensor-core match launch (measurement only).
 MATCH_TIMERS: Optional[list] = None
+# When set to a one-element int64 device tensor, the merge kernels add the
+# number of rows they re-score in FP32 to it (measurement only).
+RESCORE_COUNTER: Optional[torch.Tensor] = None
 
 
 @dataclass
@@ -57,6 +60,9 @@ class SearchConfig:
     splits: int = 0
     wave_tiles: int = 0
     persistent: bool = False
+    # re-score in FP32 only the candidates whose bf16 score, widened by a
+    # rigorous rounding bound, can still reach the exact top-k (same results)
+    rescore_gate: bool = True
 
     def validate(self):
         if self.precision not in LP_DTYPES:
@@ -253,6 +259,8 @@ class Searcher:
                                device=dev)
         part_idx = torch.empty(part_val.shape, dtype=torch.int32, device=dev)
         n_dchunks = (D + self.dict_chunk - 1) // self.dict_chunk
+        gate = kernels.rescore_gate(self.lp_dtype, q_rows.k_pad, self.n_pix) \
+            if (self.rescore and cfg.rescore_gate) else 0.0
         for ci, d0 in enumerate(range(0, D, self.dict_chunk)):
             d1 = min(D, d0 + self.dict_chunk)
             nd = d1 - d0
@@ -303,7 +311,7 @@ class Searcher:
                         q_rows.lp_scale[s0:] if q_rows.lp_scale is not None else None, self.sim,
                         min(self.n_rescore, splits * self.n_cand), k,
                         out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
-                        out_val[g0:g1], out_idx[g0:g1])
+                        out_val[g0:g1], out_idx[g0:g1], gate_rel=gate, n_rescored=RESCORE_COUNTER)
         if check:
             check_status(status)
         return out_idx, out_val

@@ -177,16 +177,34 @@ def match_topk(q_lp, d_lp, n_dict_valid: int, lp_dtype: int, col_scale, n_cand: 
          _stream(q_lp.device))
 
 
+def rescore_gate(lp_dtype: int, k_pad: int, n_pix: int) -> float:
+    """Bound on |s' - s| / w for unit low-precision rows (see
+    ebsd_merge_rescore_gated), or 0 (no gate) for e4m3, whose bound is too
+    wide to exclude candidates. bf16 rounding of both unit rows (unit
+    roundoff u = 2^-8): factor (1 + u)^2; FP32 accumulation of k_pad exact
+    products, counted twice to allow truncating adders: 2 k_pad 2^-24; the
+    FP32 re-score of the n_pix-term dot itself: 2 n_pix 2^-24 (so that no
+    candidate left out could have ranked in by re-score rounding); 1e-6 for
+    the FP32 normalisation of the rows."""
+    if lp_dtype != DT_BF16:
+        return 0.0
+    u, u32 = 2.0 ** -8, 2.0 ** -24
+    return (1.0 + u) ** 2 * (1.0 + 2.0 * k_pad * u32) - 1.0 + 2.0 * n_pix * u32 + 1e-6
+
+
 def merge_rescore(part_val, part_idx, n_queries: int, part_slots: int, n_cand: int, q_f32, d_f32, d_index_base: int,
                   n_pix: int, q_norm, d_norm, q_lp_scale, similarity: int, n_rescore: int, k_out: int, run_val,
-                  run_idx, out_val, out_idx) -> None:
-    call("ebsd_merge_rescore", ptr(part_val), ptr(part_idx), int(n_queries), int(part_slots), int(n_cand),
+                  run_idx, out_val, out_idx, gate_rel: float = 0.0, n_rescored=None) -> None:
+    """K4. gate_rel > 0 re-scores only the candidates that can reach the exact
+    top k_out (rescore_gate); n_rescored: optional uint64 device counter of
+    the rows re-scored."""
+    call("ebsd_merge_rescore_gated", ptr(part_val), ptr(part_idx), int(n_queries), int(part_slots), int(n_cand),
          ptr(q_f32), q_f32.stride(0) if q_f32 is not None else 0, ptr(d_f32),
          d_f32.stride(0) if d_f32 is not None else 0, int(d_index_base),
          d_f32.shape[0] if d_f32 is not None else 1, int(n_pix), ptr(q_norm), ptr(d_norm),
          ptr(q_lp_scale),
          int(similarity), int(n_rescore), int(k_out), ptr(run_val), ptr(run_idx), ptr(out_val), ptr(out_idx),
-         _stream(part_val.device))
+         float(gate_rel), ptr(n_rescored), _stream(part_val.device))
 
 
 # ------------------------------------------------------------------ A11/A12

@@ -226,6 +226,25 @@ int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n
                        int k_out, const float* run_val, const int64_t* run_idx, float* out_val,
                        int64_t* out_idx, void* stream);
 
+/* As ebsd_merge_rescore, with a margin gate on the FP32 re-score (no
+ * counterpart in the reference, which scores every candidate in its match
+ * dtype). gate_rel > 0 must bound |s' - s| / w for every candidate, where s'
+ * is the low-precision score per unit query norm, s the exact one, and w the
+ * dictionary row norm (dot metric) or 1 (cosine). Only candidates whose upper
+ * bound s' + gate_rel * w reaches the k_out-th largest lower bound among the
+ * n_rescore best are re-scored; the others cannot be in the exact top k_out,
+ * so the result equals ebsd_merge_rescore's. gate_rel = 0 re-scores all
+ * n_rescore. n_rescored (may be NULL) accumulates the number of rows
+ * re-scored. */
+int ebsd_merge_rescore_gated(const float* part_val, const int32_t* part_idx, int64_t n_queries,
+                             int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
+                             const float* d_f32, int64_t ld_d, int64_t d_index_base, int64_t d_rows,
+                             int n_pix, const float* q_norm, const float* d_norm,
+                             const float* q_lp_scale, int similarity, int n_rescore, int k_out,
+                             const float* run_val, const int64_t* run_idx, float* out_val,
+                             int64_t* out_idx, float gate_rel, unsigned long long* n_rescored,
+                             void* stream);
+
 /* ---- allocation-free match ------------------------------------------------
  * No counterpart in the reference: an extra entry point for callers that
  * cannot call cudaMalloc where they index patterns -- e.g. a detector
