@@ -317,6 +317,59 @@ def match_traffic_estimate(d_rows: int) -> float:
     return b1 + (b2 - b1) * (d_rows - d1) / (d2 - d1)
 
 
+def gemm_peak_tflops(kind: str, dev, seconds: float = 3.0, n: int = 8192) -> dict:
+    """Library GEMM throughput on this GPU, the denominator for a kernel of
+    the same element type: cuBLASLt e4m3 x e4m3 -> bf16 (torch._scaled_mm,
+    per-tensor scales) or bf16 x bf16 (torch.matmul), n^3. `burst`: 50
+    calls after warm-up; `sustained`: calls repeated for `seconds` (the power
+    cap settles), rate of the last two thirds. CUDA events throughout."""
+    import torch
+
+    g = torch.Generator(device=dev).manual_seed(0)
+    a = torch.randn((n, n), device=dev, generator=g)
+    b = torch.randn((n, n), device=dev, generator=g)
+    if kind == "e4m3":
+        a8, b8 = a.to(torch.float8_e4m3fn), b.to(torch.float8_e4m3fn).t()
+        one = torch.ones((), device=dev)
+
+        def f():
+            return torch._scaled_mm(a8, b8, scale_a=one, scale_b=one, out_dtype=torch.bfloat16)
+    else:
+        a16, b16 = a.bfloat16(), b.bfloat16()
+
+        def f():
+            return a16 @ b16
+    del a, b
+    flop = 2.0 * n ** 3
+    for _ in range(10):
+        f()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        f()
+    e1.record()
+    torch.cuda.synchronize()
+    burst = 50 * flop / (e0.elapsed_time(e1) / 1e3) / 1e12
+    marks = []
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        marks.append(ev)
+        for _ in range(100):
+            f()
+        torch.cuda.synchronize()
+    ev = torch.cuda.Event(enable_timing=True)
+    ev.record()
+    marks.append(ev)
+    torch.cuda.synchronize()
+    first = len(marks) // 3
+    sustained = (len(marks) - 1 - first) * 100 * flop / (marks[first].elapsed_time(marks[-1]) / 1e3) / 1e12
+    return {"burst": burst, "sustained": sustained, "how": f"{kind} {n}^3 cuBLASLt GEMM via torch, CUDA events, "
+                                                          f"{seconds:.0f} s loop for the sustained rate"}
+
+
 def learned_block(args, wl, mp, geom, pats, exp_plain, ref_top1, n_sub, dist, dev):
     """Companion measurement of the learned path on the headline run's own
     patterns: the proposal network is trained first (outside the timed
@@ -532,6 +585,7 @@ def run_ours(args, wl):
         step8()
         torch.cuda.synchronize()
         _barrier(dist)
+        engine.MATCH_TIMERS = []
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record()
         for _ in range(args.steps):
@@ -540,10 +594,19 @@ def run_ours(args, wl):
         torch.cuda.synchronize()
         _barrier(dist)
         t8 = _max_over_ranks(f0.elapsed_time(f1) / 1e3, dist, dev)
+        timers8, engine.MATCH_TIMERS = engine.MATCH_TIMERS, None
+        ms8 = [a.elapsed_time(b) for a, b, _ in timers8]
+        fl8 = [f for _, _, f in timers8]
+        ach8 = (sum(fl8) / len(fl8)) / (sum(ms8) / len(ms8) / 1e3) / 1e12
+        pk8 = gemm_peak_tflops("e4m3", dev)
         i8 = exp8.raw_indexing_indices[0][:, 0]
         fp8 = {"value": n * wl["Q"] * args.steps / t8, "unit": UNIT, "ms_per_step": t8 / args.steps * 1e3,
                "same_top1_index_as_bf16": float((i8 == exp.raw_indexing_indices[0][:, 0]).float().mean()),
-               "precision": "e4m3 match (per-row absmax scale) + FP32 re-score of top-32"}
+               "precision": "e4m3 match (per-row absmax scale) + FP32 re-score of top-32",
+               "roofline": {"bound": "tensor", "achieved": ach8, "peak": pk8["sustained"], "unit": "TFLOP/s",
+                            "frac": ach8 / pk8["sustained"], "kernel": "k_tc_gemm kind::f8f6f4 (match + top-k)",
+                            "peak_source": "measured here: " + pk8["how"], "peak_burst": pk8["burst"],
+                            "share_of_step": sum(ms8) / 1e3 / t8}}
         if fp32_cmp is not None:
             q8 = exp8.raw_indexing_results[0][0][:n_sub, 0].float().contiguous()
             fp8["same_top1_orientation_as_plain_fp32_di"] = float(
