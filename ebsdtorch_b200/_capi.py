@@ -37,8 +37,8 @@ SIGNATURES = {
     "ebsd_set_wait_limit_ns": (i64, [i64]),
     "ebsd_set_match_pacing": (i32, [i32]),
     "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
-    "ebsd_match_topk_tiled": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, i32, i32,
-                                    vp, vp]),
+    "ebsd_match_topk_tiled": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, vp, vp, i32, i32, i32,
+                                    i32, i32, vp, vp]),
     "ebsd_merge_rescore": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
                                  vp, vp, vp, vp, vp]),
     "ebsd_merge_rescore_gated": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
@@ -81,7 +81,7 @@ SIGNATURES = {
 }
 
 DT_F32, DT_BF16, DT_E4M3 = 0, 1, 2
-SIM_DOT, SIM_COSINE = 0, 1
+SIM_DOT, SIM_COSINE, SIM_EUCLIDEAN = 0, 1, 2
 DEVICE_TIMEOUT = 0x7001
 
 # kernels launched by one successful call of each entry point

@@ -56,6 +56,10 @@ struct GemmParams {
   int k_iters;
   int64_t n_valid;
   const float* col_scale;
+  // MODE 0, optional: score = acc * col_scale[d] + col_bias[d] * row_scale[q]
+  // (the euclidean ranking 2 |d| cos - |d|^2 / |q|)
+  const float* col_bias;
+  const float* row_scale;
   float* part_val;
   int32_t* part_idx;
   int part_slots;
@@ -373,6 +377,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         bv[j] = -INFINITY;
         bi[j] = -1;
       }
+      const float rs = (MODE == 0 && p.row_scale) ? __ldg(p.row_scale + (int64_t)m_tile * BM + row) : 0.0f;
       for (int n = n_begin; n < n_end; ++n) {
         bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag, wait_ns);
         got = __all_sync(0xffffffffu, got);
@@ -403,12 +408,24 @@ __global__ void __launch_bounds__(THREADS, 1)
                   v[4 * j4 + 3] *= s4.w;
                 }
               }
+              if (p.col_bias) {
+                const float4* cb = reinterpret_cast<const float4*>(p.col_bias + col0);
+#pragma unroll
+                for (int j4 = 0; j4 < 8; ++j4) {
+                  const float4 b4 = __ldg(cb + j4);
+                  v[4 * j4 + 0] = fmaf(b4.x, rs, v[4 * j4 + 0]);
+                  v[4 * j4 + 1] = fmaf(b4.y, rs, v[4 * j4 + 1]);
+                  v[4 * j4 + 2] = fmaf(b4.z, rs, v[4 * j4 + 2]);
+                  v[4 * j4 + 3] = fmaf(b4.w, rs, v[4 * j4 + 3]);
+                }
+              }
             } else {
 #pragma unroll
               for (int j = 0; j < 32; ++j) {
                 const bool valid = col0 + j < p.n_valid;
                 const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
-                v[j] = valid ? v[j] * sc : -INFINITY;
+                const float cb = (valid && p.col_bias) ? __ldg(p.col_bias + col0 + j) : 0.0f;
+                v[j] = valid ? fmaf(cb, rs, v[j] * sc) : -INFINITY;
               }
             }
 #pragma unroll
@@ -656,7 +673,8 @@ extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad)
 
 extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
                                      int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
-                                     const float* col_scale, int n_cand, int splits, float* part_val,
+                                     const float* col_scale, const float* col_bias, const float* row_scale,
+                                     int n_cand, int splits, float* part_val,
                                      int32_t* part_idx, int part_slots, int slot_base, int32_t index_base,
                                      int tile_n, int max_ctas, int* d_status, void* stream) {
   if (tile_n == 0) tile_n = 256;
@@ -667,6 +685,8 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   EBSD_ARG_CHECK(n_dict_valid > 0 && n_dict_valid <= n_dict_pad, "n_dict_valid out of range");
   EBSD_ARG_CHECK((int64_t)index_base + n_dict_valid <= INT32_MAX, "dictionary index overflow");
   EBSD_ARG_CHECK(!col_scale || ((uintptr_t)col_scale & 15) == 0, "col_scale must be 16-byte aligned");
+  EBSD_ARG_CHECK(!col_bias || ((uintptr_t)col_bias & 15) == 0, "col_bias must be 16-byte aligned");
+  EBSD_ARG_CHECK(!col_bias == !row_scale, "col_bias and row_scale must be given together");
   const int n_tiles = (int)(n_dict_pad / tile_n);
   if (splits <= 0) splits = ebsd_match_auto_splits(n_queries_pad, n_dict_pad);
   splits = std::min(splits, n_tiles);
@@ -684,6 +704,8 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   p.k_iters = (int)(k_pad * (lp_dtype == EBSD_DT_BF16 ? 2 : 1) / BKB);
   p.n_valid = n_dict_valid;
   p.col_scale = col_scale;
+  p.col_bias = col_bias;
+  p.row_scale = row_scale;
   p.part_val = part_val;
   p.part_idx = part_idx;
   p.part_slots = part_slots;
@@ -715,8 +737,8 @@ extern "C" int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, co
     EBSD_ARG_CHECK(splits <= n_dict_pad / 256, "splits (%d) > dictionary tiles (%lld)", splits,
                    (long long)(n_dict_pad / 256));
   return ebsd_match_topk_tiled(queries_lp, n_queries_pad, dict_lp, n_dict_pad, n_dict_valid, k_pad, lp_dtype,
-                               col_scale, n_cand, splits, part_val, part_idx, part_slots, slot_base, index_base,
-                               256, 0, d_status, stream);
+                               col_scale, nullptr, nullptr, n_cand, splits, part_val, part_idx, part_slots, slot_base,
+                               index_base, 256, 0, d_status, stream);
 }
 
 extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int64_t k_pad,

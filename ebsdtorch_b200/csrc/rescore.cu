@@ -98,11 +98,14 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   }
   bitonic_sort(cv, ci, sort_n);
 
-  // 2. exact FP32 scores of the best n_rescore (or approximate * |q|)
+  // 2. exact FP32 scores of the best n_rescore (or approximate * |q|).
+  // Euclidean scores are kept internally as the negated squared distance, so
+  // that "larger ranks first" holds for every metric.
   const int nr = n_rescore;
+  const bool euclid = similarity == EBSD_SIM_EUCLIDEAN;
   if (d_f32) {
     // 2a. which of them can reach the exact top k_out (margin gate)
-    const bool gate = gate_rel > 0.0f && nr > k_out;
+    const bool gate = gate_rel > 0.0f && nr > k_out && !euclid;
     if (gate) {
       float w = 0.0f;
       if (tid < nr) {
@@ -169,6 +172,10 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
           if (similarity == EBSD_SIM_COSINE && di[j] >= 0) {
             const float den = q_norm[q] * d_norm[di[j] - d_base];
             v = den > 0.0f ? v / den : 0.0f;
+          } else if (euclid && di[j] >= 0) {
+            // |q|^2 + |d|^2 - 2 q.d with FP32 norms of the zero-mean rows (knn.py:85-91)
+            const float qn = q_norm[q], dn = d_norm[di[j] - d_base];
+            v = -(fmaf(qn, qn, dn * dn) - 2.0f * v);
           }
           fin_v[c] = di[j] >= 0 ? v : -INFINITY;
           fin_i[c] = di[j];
@@ -177,9 +184,12 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     }
   } else {
     float qn = q_lp_scale ? q_lp_scale[q] : 1.0f;
-    if (similarity == EBSD_SIM_DOT && q_norm) qn *= q_norm[q];
+    if ((similarity == EBSD_SIM_DOT || euclid) && q_norm) qn *= q_norm[q];
+    // euclidean: cv * qn = 2 q.d - |d|^2 (see ebsd_match_topk_tiled), so the
+    // negated squared distance is cv * qn - |q|^2
+    const float qq = (euclid && q_norm) ? q_norm[q] * q_norm[q] : 0.0f;
     for (int c = tid; c < nr; c += blockDim.x) {
-      fin_v[c] = ci[c] >= 0 ? cv[c] * qn : -INFINITY;
+      fin_v[c] = ci[c] >= 0 ? cv[c] * qn - qq : -INFINITY;
       fin_i[c] = ci[c];
     }
   }
@@ -187,7 +197,8 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   int nf = nr;
   if (run_val) {
     for (int c = tid; c < k_out; c += blockDim.x) {
-      fin_v[nr + c] = run_val[q * k_out + c];
+      const float rv = run_val[q * k_out + c];
+      fin_v[nr + c] = euclid ? -rv : rv;
       fin_i[nr + c] = run_idx[q * k_out + c];
     }
     nf += k_out;
@@ -204,12 +215,12 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     for (int o = 0; o < nf; ++o)
       if (o != tid && ranks_before(fin_v[o], fin_i[o], v, i)) ++rank;
     if (rank < k_out) {
-      out_val[q * k_out + rank] = v;
+      out_val[q * k_out + rank] = euclid ? -v : v;
       out_idx[q * k_out + rank] = i;
     }
   }
   for (int r = n_valid + tid; r < k_out; r += blockDim.x) {
-    out_val[q * k_out + r] = -INFINITY;
+    out_val[q * k_out + r] = euclid ? INFINITY : -INFINITY;
     out_idx[q * k_out + r] = -1;
   }
 }
@@ -235,12 +246,13 @@ extern "C" int ebsd_merge_rescore_gated(const float* part_val, const int32_t* pa
   EBSD_ARG_CHECK(n_rescore >= 1 && n_rescore <= kMaxRescore && n_rescore <= n_list,
                  "n_rescore %d outside [1, min(%d, %d)]", n_rescore, kMaxRescore, n_list);
   EBSD_ARG_CHECK(!(run_val == nullptr) == !(run_idx == nullptr), "run_val/run_idx must be given together");
-  EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || similarity == EBSD_SIM_COSINE,
-                 "similarity must be EBSD_SIM_DOT or EBSD_SIM_COSINE");
+  EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || similarity == EBSD_SIM_COSINE || similarity == EBSD_SIM_EUCLIDEAN,
+                 "similarity must be EBSD_SIM_DOT, EBSD_SIM_COSINE or EBSD_SIM_EUCLIDEAN");
+  EBSD_ARG_CHECK(similarity != EBSD_SIM_EUCLIDEAN || q_norm, "euclidean scores need q_norm");
   if (d_f32) {
     EBSD_ARG_CHECK(q_f32 != nullptr, "q_f32 is required for re-scoring");
     EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || (q_norm && d_norm),
-                   "cosine re-scoring needs q_norm and d_norm");
+                   "cosine and euclidean re-scoring need q_norm and d_norm");
     EBSD_ARG_CHECK(n_pix >= 1 && ld_q >= n_pix && ld_d >= n_pix, "bad re-score row length");
     EBSD_ARG_CHECK(n_pix <= 40960, "re-score row length %d exceeds 40960", n_pix);
     EBSD_ARG_CHECK(d_rows >= 1 && d_index_base >= 0, "bad dictionary row range");

@@ -44,12 +44,23 @@ def _device(mp, device) -> torch.device:
 
 
 def _check_common(distance_metric: str, average_pattern_center: bool):
-    if distance_metric != "angular":
+    if distance_metric not in ("angular", "euclidean"):
         raise NotImplementedError(f"'{distance_metric}' not supported.")
     if not average_pattern_center:
         raise NotImplementedError(
             "average_pattern_center=False is not supported (the reference never initialises the per-scan-point "
             "coordinates it needs)")
+
+
+def _similarity(distance_metric: str, similarity: str) -> str:
+    """The engine's score for the reference's distance_metric: "angular" is
+    the raw dot of zero-mean rows (or its cosine when asked), "euclidean" the
+    squared euclidean distance (knn.py:85-97)."""
+    if distance_metric == "euclidean":
+        if similarity != "dot":
+            raise ValueError("similarity applies to distance_metric='angular' only")
+        return "euclidean"
+    return similarity
 
 
 def _unit_rays_soa(geometry, binning: int, signal_mask: Optional[Tensor], device) -> Tensor:
@@ -202,7 +213,7 @@ def dictionary_index_orientations(
     n_q = experiment_patterns.n_patterns
     # the reference honours subtract_exp_pat_mean only on its all-at-once path
     subtract = bool(subtract_exp_pat_mean) if experiment_chunk_size > n_q else True
-    cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=similarity,
+    cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=_similarity(distance_metric, similarity),
                        workspace_bytes=workspace_bytes)
     pats_host = experiment_patterns.patterns
     stream_host = pats_host.device.type != "cuda" and pats_host.is_pinned()
@@ -405,7 +416,8 @@ def pca_dictionary_index_orientations(
                     _finish_rows(Y, _slice(bufs, s0 - q0, s1 - q0))
 
             budget = workspace_bytes or int(default_budget(dev) * 0.7)
-            cfg = SearchConfig(precision=precision, rescore_k=rescore_k, similarity=similarity, workspace_bytes=budget)
+            cfg = SearchConfig(precision=precision, rescore_k=rescore_k,
+                               similarity=_similarity(distance_metric, similarity), workspace_bytes=budget)
             searcher = Searcher(ori.shape[0], n_q, n_comp, int(top_k_matches), cfg, dev)
             idx, val = searcher.run(fill_dict, fill_queries)
             if int(proj.status.item()) != 0:

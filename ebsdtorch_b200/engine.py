@@ -21,7 +21,7 @@ from typing import Callable, Optional
 import torch
 
 from . import kernels
-from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT
+from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT, SIM_EUCLIDEAN
 from .kernels import LP_DTYPES, LP_KMULT, LP_TORCH, TILE_D, TILE_Q, RowBuffers, round_up
 
 MAX_CAND = 64
@@ -39,8 +39,10 @@ RESCORE_COUNTER: Optional[torch.Tensor] = None
 class SearchConfig:
     """precision: element type of the tensor-core contraction ("bf16" | "fp8").
     rescore_k: candidates per query re-scored in FP32 (0 = report the
-    low-precision score). similarity: "dot" is the reference metric (raw dot of
-    zero-mean rows, knn.py:96-97); "cosine" divides it by both norms.
+    low-precision score). similarity: "dot" is the reference's angular metric
+    (raw dot of zero-mean rows, knn.py:96-97); "cosine" divides it by both
+    norms; "euclidean" is the reference's squared euclidean distance of the
+    zero-mean rows (knn.py:85-91), smallest first.
     workspace_bytes: device-memory budget (default: 90 % of free memory)."""
 
     precision: str = "bf16"
@@ -67,8 +69,8 @@ class SearchConfig:
     def validate(self):
         if self.precision not in LP_DTYPES:
             raise ValueError(f"precision must be one of {sorted(LP_DTYPES)}, got {self.precision!r}")
-        if self.similarity not in ("dot", "cosine"):
-            raise ValueError(f"similarity must be 'dot' or 'cosine', got {self.similarity!r}")
+        if self.similarity not in ("dot", "cosine", "euclidean"):
+            raise ValueError(f"similarity must be 'dot', 'cosine' or 'euclidean', got {self.similarity!r}")
         if not 0 <= self.rescore_k <= 128:
             raise ValueError("rescore_k must be in [0, 128]")
         if self.tile_n not in (0, 128, 256):
@@ -150,11 +152,27 @@ class RowSet:
 
 
 def _col_scale(rows: RowSet, similarity: str) -> Optional[torch.Tensor]:
-    """Per-dictionary-row factor of the tensor-core score: |d| (dot metric)
-    times the e4m3 dequant scale."""
+    """Per-dictionary-row factor of the tensor-core score: |d| (dot metric),
+    2 |d| (euclidean), times the e4m3 dequant scale."""
     if similarity == "dot":
         return rows.norm if rows.lp_scale is None else rows.norm * rows.lp_scale
+    if similarity == "euclidean":
+        return 2.0 * rows.norm if rows.lp_scale is None else 2.0 * rows.norm * rows.lp_scale
     return rows.lp_scale
+
+
+def _col_bias(rows: RowSet, similarity: str) -> Optional[torch.Tensor]:
+    """Per-dictionary-row term of the euclidean score, -|d|^2: with the
+    per-query factor 1 / (|q| e4m3-scale) the tensor-core score ranks like
+    2 q.d - |d|^2, i.e. by the smallest |q - d|^2."""
+    return -(rows.norm * rows.norm) if similarity == "euclidean" else None
+
+
+def _row_scale(rows: RowSet, similarity: str) -> Optional[torch.Tensor]:
+    if similarity != "euclidean":
+        return None
+    n = rows.norm if rows.lp_scale is None else rows.norm * rows.lp_scale
+    return torch.where(n > 0, 1.0 / n.clamp_min(1e-30), torch.zeros_like(n))
 
 
 def wave_query_tiles(device) -> int:
@@ -193,7 +211,7 @@ class Searcher:
         self.rescore = cfg.rescore_k > 0
         self.n_cand = min(MAX_CAND, _pow2_at_least(max(k, cfg.rescore_k)))
         self.n_rescore = max(k, cfg.rescore_k) if self.rescore else k
-        self.sim = SIM_DOT if cfg.similarity == "dot" else SIM_COSINE
+        self.sim = {"dot": SIM_DOT, "cosine": SIM_COSINE, "euclidean": SIM_EUCLIDEAN}[cfg.similarity]
         self._plan()
 
     def _plan(self):
@@ -260,7 +278,7 @@ class Searcher:
         part_idx = torch.empty(part_val.shape, dtype=torch.int32, device=dev)
         n_dchunks = (D + self.dict_chunk - 1) // self.dict_chunk
         gate = kernels.rescore_gate(self.lp_dtype, q_rows.k_pad, self.n_pix) \
-            if (self.rescore and cfg.rescore_gate) else 0.0
+            if (self.rescore and cfg.rescore_gate and cfg.similarity != "euclidean") else 0.0
         for ci, d0 in enumerate(range(0, D, self.dict_chunk)):
             d1 = min(D, d0 + self.dict_chunk)
             nd = d1 - d0
@@ -270,12 +288,14 @@ class Searcher:
                     dict_rows.norm[nd:].zero_()
                 fill_dict(d0, d1, dict_rows.buffers(0, nd))
             col_scale = _col_scale(dict_rows, self.cfg.similarity)
+            col_bias = _col_bias(dict_rows, self.cfg.similarity)
             nd_pad = round_up(nd, TILE_D)
             d_lp = dict_rows.lp[:nd_pad]
             for q0 in range(0, Q, qc):
                 q1 = min(Q, q0 + qc)
                 nq = q1 - q0
                 fill_queries(q0, q1, q_rows.buffers(0, nq))
+                row_scale = _row_scale(q_rows, self.cfg.similarity)
                 # the next chunk's host-to-device copy runs under this chunk's matching
                 prefetch = getattr(fill_queries, "prefetch", None)
                 if prefetch is not None:
@@ -297,7 +317,8 @@ class Searcher:
                         ev0.record()
                     kernels.match_topk(q_rows.lp[s0:s0 + ns_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand,
                                        splits, part_val, part_idx, splits, 0, d0, status, tile_n=cfg.tile_n,
-                                       max_ctas=max_ctas)
+                                       max_ctas=max_ctas, col_bias=col_bias,
+                                       row_scale=row_scale[s0:] if row_scale is not None else None)
                     if timers is not None:
                         ev1.record()
                         timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))

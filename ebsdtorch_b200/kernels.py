@@ -163,16 +163,18 @@ def auto_splits(n_queries_pad: int, n_dict_pad: int) -> int:
 
 def match_topk(q_lp, d_lp, n_dict_valid: int, lp_dtype: int, col_scale, n_cand: int, splits: int,
                part_val, part_idx, part_slots: int, slot_base: int, index_base: int, status, tile_n: int = 0,
-               max_ctas: int = 0) -> None:
+               max_ctas: int = 0, col_bias=None, row_scale=None) -> None:
     """K3 match; tile_n / max_ctas choose the launch shape (0, 0: 256-row
-    tiles, one CTA per work unit)."""
-    if tile_n == 0 and max_ctas == 0:
+    tiles, one CTA per work unit); col_bias / row_scale add
+    col_bias[d] * row_scale[q] to the scores (euclidean ranking)."""
+    if tile_n == 0 and max_ctas == 0 and col_bias is None:
         call("ebsd_match_topk", ptr(q_lp), q_lp.shape[0], ptr(d_lp), d_lp.shape[0], int(n_dict_valid),
              q_lp.shape[1], lp_dtype, ptr(col_scale), int(n_cand), int(splits), ptr(part_val), ptr(part_idx),
              int(part_slots), int(slot_base), int(index_base), ptr(status), _stream(q_lp.device))
         return
     call("ebsd_match_topk_tiled", ptr(q_lp), q_lp.shape[0], ptr(d_lp), d_lp.shape[0], int(n_dict_valid),
-         q_lp.shape[1], lp_dtype, ptr(col_scale), int(n_cand), int(splits), ptr(part_val), ptr(part_idx),
+         q_lp.shape[1], lp_dtype, ptr(col_scale), ptr(col_bias), ptr(row_scale), int(n_cand), int(splits),
+         ptr(part_val), ptr(part_idx),
          int(part_slots), int(slot_base), int(index_base), int(tile_n), int(max_ctas), ptr(status),
          _stream(q_lp.device))
 

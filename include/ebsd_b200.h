@@ -194,10 +194,15 @@ int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* d
  * 256; n_dict_pad must be a multiple of it), and max_ctas > 0 for a
  * persistent launch of min(units, max_ctas) CTAs that each loop over work
  * units u, u + grid, ... (0 = one CTA per unit). Splits larger than the
- * number of dictionary tiles are reduced to it. */
+ * number of dictionary tiles are reduced to it. col_bias / row_scale (both
+ * or neither; 16-byte aligned; row_scale has n_queries_pad entries) add
+ * col_bias[d] * row_scale[q] to every score: with col_scale = 2 |d|,
+ * col_bias = -|d|^2 and row_scale = 1 / |q| on unit rows the scores rank
+ * by the smallest squared euclidean distance (knn.py:85-91). */
 int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
                           int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
-                          const float* col_scale, int n_cand, int splits, float* part_val, int32_t* part_idx,
+                          const float* col_scale, const float* col_bias, const float* row_scale,
+                          int n_cand, int splits, float* part_val, int32_t* part_idx,
                           int part_slots, int slot_base, int32_t index_base, int tile_n, int max_ctas,
                           int* d_status, void* stream);
 
@@ -211,12 +216,18 @@ int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const v
  *   similarity EBSD_SIM_DOT:    exact = q_f32[q] . d_f32[idx - d_index_base]
  *                               (n_pix terms), the reference metric (knn.py:96-97)
  *   similarity EBSD_SIM_COSINE: exact = that dot / (q_norm[q] d_norm[idx - d_index_base])
+ *   similarity EBSD_SIM_EUCLIDEAN: the squared distance
+ *                               q_norm[q]^2 + d_norm[.]^2 - 2 dot (knn.py:85-91); the
+ *                               best k_out are the smallest, sorted ascending, and
+ *                               missing entries are +inf / -1; run_val holds distances
  * (candidate indices are global; d_f32/d_norm hold rows d_index_base ..
  * d_index_base + d_rows - 1; a candidate outside that range is dropped)
  * With d_f32 == NULL nothing is re-scored and the score is
- *   approx * (q_lp_scale ? q_lp_scale[q] : 1) * (DOT ? q_norm[q] : 1). */
+ *   s = approx * (q_lp_scale ? q_lp_scale[q] : 1) * (DOT or EUCLIDEAN ? q_norm[q] : 1),
+ * and the euclidean distance q_norm[q]^2 - s. */
 #define EBSD_SIM_DOT 0
 #define EBSD_SIM_COSINE 1
+#define EBSD_SIM_EUCLIDEAN 2
 int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
                        int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
                        const float* d_f32, int64_t ld_d, int64_t d_index_base, int64_t d_rows,

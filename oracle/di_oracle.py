@@ -563,6 +563,30 @@ def topk_dot(queries: np.ndarray, data: np.ndarray, k: int, chunk: int = 4096):
     return best_i, best_v
 
 
+def topk_euclidean(queries: np.ndarray, data: np.ndarray, k: int, chunk: int = 4096):
+    """Top-k by the smallest squared euclidean distance |q|^2 + |d|^2 - 2 q.d,
+    sorted ascending (knn.py:85-91 with largest=False, ChunkedKNN merge and
+    retrieve_topk :219-287). Ties resolve to the lower dictionary index.
+    Returns (indices int64 (Q, k), distances (Q, k))."""
+    Q = queries.shape[0]
+    qn = (queries.astype(np.float64) ** 2).sum(axis=1).astype(queries.dtype)
+    best_v = np.full((Q, k), np.inf, dtype=np.result_type(queries, data))
+    best_i = np.zeros((Q, k), dtype=np.int64)
+    for d0 in range(0, data.shape[0], chunk):
+        blk = data[d0 : d0 + chunk]
+        dn = (blk.astype(np.float64) ** 2).sum(axis=1).astype(blk.dtype)
+        dist = qn[:, None] + dn[None, :] - 2.0 * (queries @ blk.T)
+        kk = min(k, blk.shape[0])
+        part = np.argpartition(dist, kk - 1, axis=1)[:, :kk]
+        pv = np.take_along_axis(dist, part, axis=1)
+        allv = np.concatenate((best_v, pv), axis=1)
+        alli = np.concatenate((best_i, part + d0), axis=1)
+        o = np.lexsort((alli, allv), axis=1)[:, :k]
+        best_v = np.take_along_axis(allv, o, axis=1)
+        best_i = np.take_along_axis(alli, o, axis=1)
+    return best_i, best_v
+
+
 # --------------------------------------------------------------------------
 # End-to-end plain DI (A1-A13)
 # --------------------------------------------------------------------------
@@ -607,9 +631,12 @@ def dictionary_index(
     binning: int = 1,
     dtype=np.float64,
     dictionary: Optional[np.ndarray] = None,
+    distance_metric: str = "angular",
 ):
     """Plain DI for one phase (indexing.py:14-211). Returns
-    (orientations (Q, k, 4), metrics (Q, k), indices (Q, k), dictionary (D, 4))."""
+    (orientations (Q, k, 4), metrics (Q, k), indices (Q, k), dictionary (D, 4));
+    distance_metric "angular" (largest raw dot first) or "euclidean"
+    (smallest squared distance first, knn.py:85-91)."""
     if dictionary is None:
         dictionary = sample_ori_fz_laue_angle(laue_id, resolution_deg, permutation)
     mp = avg_pool(np.asarray(master_pattern, dtype=np.float64), binning)
@@ -617,7 +644,12 @@ def dictionary_index(
     rays = unit_rays(coords)
     d = dictionary_rows(mp, rays, dictionary, mask, dtype)
     q = prep_patterns(patterns, binning, mask, True, dtype)
-    idx, val = topk_dot(q, d, top_k)
+    if distance_metric == "euclidean":
+        idx, val = topk_euclidean(q, d, top_k)
+    elif distance_metric == "angular":
+        idx, val = topk_dot(q, d, top_k)
+    else:
+        raise NotImplementedError(f"'{distance_metric}' not supported.")
     return dictionary[idx], val, idx, dictionary
 
 

@@ -18,7 +18,8 @@ outputs of one case (``--refinement-only`` / ``--preprocessing-only`` /
 ``--pcfit-only`` / ``--reader-only`` write just refine.npz / preprocess.npz /
 pcfit.npz / emsoft_reader.npz; ``--config0-only`` writes config0.npz, the
 reference's own plain DI at the small configuration on inputs rebuilt by
-``config0_inputs.py``). The files are small (< 1 MB each) and committed.
+``config0_inputs.py``; ``--euclidean-only`` writes di_euclid.npz, plain DI with
+the euclidean distance). The files are small (< 1 MB each) and committed.
 """
 
 from __future__ import annotations
@@ -324,6 +325,58 @@ def config0_goldens(root=None):
         case=np.array(repr(sorted(c.items()))))
 
 
+def euclidean_goldens(root=None):
+    """The reference's plain DI with distance_metric="euclidean" (knn.py:85-91,
+    squared distance of the zero-mean rows, smallest first), float32 matching
+    on its chunked query path, top-3, plus a second case with a signal mask
+    and binning 2 on the all-at-once path."""
+    ref_idx, _ = load_reference(root)
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.ebsd.geometry import EBSDGeometry
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.preprocessing.radial_mask import get_radial_mask
+    from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+    from ebsdtorch.s2_and_so3.quaternions import qu_apply
+    from ebsdtorch.s2_and_so3.sampling import so3_uniform_quat
+
+    out = {}
+    for ci, c in enumerate((dict(det=(20, 20), res=8.0, Q=31, k=3, b=1, mask=False, ec=8, dcs=50, seed=91),
+                            dict(det=(24, 24), res=9.0, Q=19, k=2, b=2, mask=True, ec=4096, dcs=4096, seed=92))):
+        torch.manual_seed(c["seed"])
+        mp_t = smooth_master_pattern(c["seed"], 41)
+        mp = MasterPattern(mp_t.clone(), laue_group=11)
+        geom = EBSDGeometry(c["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+        qq = so3_uniform_quat(c["Q"], torch.device("cpu"))
+        with torch.no_grad():
+            dc = geom.get_coords_sample_frame(binning=(1, 1))
+            dc = dc / dc.norm(dim=-1, keepdim=True)
+            pats = mp.interpolate(qu_apply(qq[:, None, :], dc[None]), normalize_coords=False).reshape(
+                c["Q"], *c["det"])
+            pats = 50.0 * (pats + 0.05 * torch.randn_like(pats))
+        exp = ExperimentPatterns(pats.clone())
+        bdet = (c["det"][0] // c["b"], c["det"][1] // c["b"])
+        mask = get_radial_mask(bdet) if c["mask"] else None
+        torch.manual_seed(c["seed"] + 1000)
+        with ref_loader.quiet_stdout():
+            ref_idx.dictionary_index_orientations(
+                mp, geom, exp, signal_mask=mask, experiment_chunk_size=c["ec"],
+                dictionary_resolution_degrees=c["res"], dictionary_chunk_size=c["dcs"], virtual_binning=c["b"],
+                top_k_matches=c["k"], distance_metric="euclidean", match_dtype=torch.float32,
+                quantized_if_x86=False)
+        torch.manual_seed(c["seed"] + 1000)
+        dictionary = sample_ori_fz_laue_angle(11, c["res"], torch.device("cpu"), permute=True).numpy()
+        out[f"case{ci}_master_pattern"] = mp_t.numpy()
+        out[f"case{ci}_patterns"] = pats.numpy()
+        out[f"case{ci}_mask"] = mask.numpy() if mask is not None else np.zeros(0, bool)
+        out[f"case{ci}_meta"] = np.array([*c["det"], c["res"], c["Q"], c["k"], c["b"], c["ec"], c["dcs"],
+                                          c["seed"] + 1000], dtype=np.float64)
+        out[f"case{ci}_quats"] = exp.raw_indexing_results[0][0].numpy()
+        out[f"case{ci}_dists"] = exp.raw_indexing_results[0][1].numpy()
+        out[f"case{ci}_best"] = exp.best_metrics.numpy()
+        out[f"case{ci}_dictionary"] = dictionary
+    np.savez_compressed(os.path.join(HERE, "di_euclid.npz"), **out)
+
+
 def main(root=None):
     ref_idx, ref_idx_top = load_reference(root)
     from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
@@ -551,6 +604,8 @@ if __name__ == "__main__":
         emsoft_reader_goldens(*args[1:])
     elif args and args[0] == "--config0-only":
         config0_goldens(*args[1:])
+    elif args and args[0] == "--euclidean-only":
+        euclidean_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
@@ -558,3 +613,4 @@ if __name__ == "__main__":
         pcfit_goldens(*args)
         emsoft_reader_goldens(*args)
         config0_goldens(*args)
+        euclidean_goldens(*args)

@@ -181,3 +181,53 @@ def test_synthetic_small_config_parity_and_accuracy():
     ang = disori_angle_laue(exp.orientations.float().contiguous(), truth, 11, 11)
     # 2 deg grid on a coarse 40 x 40 detector: nearest grid point ~1-2 deg away
     assert torch.median(ang).item() < np.deg2rad(4.0)
+
+
+@pytest.mark.parametrize("case", [0, 1])
+@pytest.mark.parametrize("precision", ["bf16", "fp8"])
+def test_euclidean_distance_matches_reference(golden, case, precision):
+    """distance_metric="euclidean": the reference's squared distances
+    (knn.py:85-91), smallest first, combined with higher_is_better=False."""
+    from ebsdtorch_b200.ebsd import EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations
+
+    d = golden("di_euclid")
+    m = d[f"case{case}_meta"]
+    det, res, k, b, ec, dcs, seed = (int(m[0]), int(m[1])), m[2], int(m[4]), int(m[5]), int(m[6]), int(m[7]), \
+        int(m[8])
+    mp = MasterPattern(torch.from_numpy(d[f"case{case}_master_pattern"]), laue_group=11).to(DEV)
+    geom = EBSDGeometry(det, tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6)).to(DEV)
+    exp = ExperimentPatterns(torch.from_numpy(d[f"case{case}_patterns"]).to(DEV))
+    mask = torch.from_numpy(d[f"case{case}_mask"]) if d[f"case{case}_mask"].size else None
+    torch.manual_seed(seed)
+    dictionary_index_orientations(mp, geom, exp, signal_mask=mask, experiment_chunk_size=ec,
+                                  dictionary_resolution_degrees=res, dictionary_chunk_size=dcs, virtual_binning=b,
+                                  top_k_matches=k, distance_metric="euclidean", match_dtype=torch.float32,
+                                  precision=precision)
+    quats, dists = exp.raw_indexing_results[0]
+    ref = d[f"case{case}_dists"]
+    assert np.abs(quats.cpu().numpy() - d[f"case{case}_quats"]).max() < 1e-5
+    assert np.abs(dists.cpu().numpy() - ref).max() <= 1e-4 * np.abs(ref).max()
+    assert np.abs(exp.best_metrics.cpu().numpy() - d[f"case{case}_best"]).max() <= 1e-4 * np.abs(ref).max()
+
+
+def test_euclidean_matches_oracle_with_dictionary_chunks():
+    """The euclidean running merge across dictionary chunks (distances, not
+    scores, carried between chunks) against the FP64 oracle."""
+    from ebsdtorch_b200 import synthetic
+    from ebsdtorch_b200.ebsd import dictionary_index_orientations
+
+    mp, geom, exp, _ = synthetic.make_case(129, (32, 32), 600, seed=5, mean_counts=80.0)
+    torch.manual_seed(2)
+    dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=4.0, top_k_matches=4,
+                                  distance_metric="euclidean", match_dtype=torch.float32,
+                                  workspace_bytes=6 << 20)
+    dic = exp.dictionaries[0].cpu().numpy().astype(np.float64)
+    rays = O.unit_rays(O.detector_coords_sample_frame((32, 32), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0)))
+    rows = O.dictionary_rows(mp.master_pattern.cpu().numpy(), rays, dic)
+    q = O.prep_patterns(exp.patterns.cpu().numpy())
+    oi, ov = O.topk_euclidean(q, rows, 4)
+    gi = exp.raw_indexing_indices[0].cpu().numpy()
+    gv = exp.raw_indexing_results[0][1].cpu().numpy()
+    assert (gi[:, 0] == oi[:, 0]).mean() >= 0.99
+    same = gi == oi
+    assert np.abs(gv - ov)[same].max() <= 1e-4 * np.abs(ov).max()

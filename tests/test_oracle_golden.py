@@ -472,3 +472,20 @@ def test_config0_inputs_reproduce_the_golden_checksums(golden):
     same = idx == ref_i
     assert same.mean() >= 0.99
     assert (np.abs(val - ref_m)[same] / np.abs(ref_m[:, :1]).repeat(4, 1)[same]).max() < 1e-4
+
+
+@pytest.mark.parametrize("case", [0, 1])
+def test_euclidean_dictionary_index_matches_reference(golden, case):
+    """distance_metric="euclidean" (knn.py:85-91): squared distances of the
+    zero-mean rows, smallest first."""
+    d = golden("di_euclid")
+    m = d[f"case{case}_meta"]
+    det, res, k, b = (int(m[0]), int(m[1])), m[2], int(m[4]), int(m[5])
+    mask = d[f"case{case}_mask"] if d[f"case{case}_mask"].size else None
+    oq, ov, _, _ = O.dictionary_index(d[f"case{case}_master_pattern"], 11, d[f"case{case}_patterns"], det,
+                                      (0.5, 0.5, 0.6), (0, 70, 0), res, top_k=k, mask=mask, binning=b,
+                                      dictionary=d[f"case{case}_dictionary"].astype(np.float64),
+                                      distance_metric="euclidean")
+    assert np.abs(oq - d[f"case{case}_quats"]).max() < 1e-6
+    assert np.abs(ov - d[f"case{case}_dists"]).max() <= 1e-4 * np.abs(d[f"case{case}_dists"]).max()
+    assert (np.diff(ov, axis=1) >= 0).all()
