@@ -13,9 +13,10 @@
  * Conventions
  *  - All pointers are device pointers unless stated otherwise; buffers are
  *    allocated by the caller. The library makes no device allocation of its
- *    own, with one exception: the 32 MiB file-scope scratch array of
- *    ebsd_match_topk_noalloc, which every GPU that loads the library holds
- *    until the process exits.
+ *    own; its only device memory is part of the module image, held by every
+ *    GPU that loads the library until the process exits: the 32 MiB scratch
+ *    array of ebsd_match_topk_noalloc and the 2 KB of pacing slots of the
+ *    match kernel (see ebsd_set_match_pacing).
  *  - Work is enqueued on `stream` (a cudaStream_t passed as void*); calls are
  *    asynchronous unless stated otherwise.
  *  - Return value: 0 success, > 0 argument error (nothing launched),
