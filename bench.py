@@ -1460,6 +1460,8 @@ def main():
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the companion learned-path measurement")
+    ap.add_argument("--no-pacing", action="store_true",
+                    help="launch the match kernels without CTA pacing (ebsd_set_match_pacing(0)), for A/B runs")
     ap.add_argument("--fp32-subset", type=int, default=8192)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (48 maps, mixed sizes, detectors, phases) instead")
@@ -1474,6 +1476,10 @@ def main():
     ap.add_argument("--pyramid", default="3.0,1.5,0.75", help="intermediate dictionary resolutions (deg), coarse first")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
+    if args.no_pacing and args.impl == "ours":
+        from ebsdtorch_b200 import _capi
+
+        _capi.load().ebsd_set_match_pacing(0)
     if args.impl == "reference":
         run_reference(args, wl)
     elif args.learned:
