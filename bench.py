@@ -488,7 +488,7 @@ def run_ours(args, wl):
     torch.cuda.synchronize()
 
     # ---- timed region: patterns resident in HBM ----
-    engine.MATCH_TIMERS = []
+    engine.MATCH_TIMERS, engine.MERGE_TIMERS = [], []
     launches0 = _capi.launch_count
     with ClockSampler(local) as clocks:
         _barrier(dist)
@@ -507,7 +507,21 @@ def run_ours(args, wl):
     n = args.gpus
     value = n * wl["Q"] * args.steps / t_max
     timers = engine.MATCH_TIMERS
-    engine.MATCH_TIMERS = None
+    merge_ms = sum(a.elapsed_time(b) for a, b in engine.MERGE_TIMERS)
+    engine.MATCH_TIMERS = engine.MERGE_TIMERS = None
+    # rows the margin-gated FP32 re-score reads (one untimed call with the counter)
+    counter = torch.zeros(1, dtype=torch.int64, device=dev)
+    engine.RESCORE_COUNTER = counter
+    step()
+    torch.cuda.synchronize()
+    engine.RESCORE_COUNTER = None
+    rows_per_query = int(counter.item()) / wl["Q"]
+    n_pix = int(wl["det"][0] * wl["det"][1])
+    rescore = {"share_of_step": merge_ms / 1e3 / elapsed, "rows_rescored_per_query": rows_per_query,
+               "rows_cap": 32, "bytes_per_query": (rows_per_query + 1) * n_pix * 4,
+               "achieved_gbs": wl["Q"] * args.steps * (rows_per_query + 1) * n_pix * 4 / (merge_ms / 1e3) / 1e9,
+               "how": "merge + margin-gated FP32 re-score (k_merge_rescore); bytes = FP32 rows re-scored + the "
+                      "query row, per query"}
     match_ms = [a.elapsed_time(b) for a, b, _ in timers]
     match_flops = [f for _, _, f in timers]
     avg_launch_s = sum(match_ms) / len(match_ms) / 1e3
@@ -676,6 +690,7 @@ def run_ours(args, wl):
                      "peak_source": f"{peak_kind} bf16_tflops_sustained" + (" x2 for fp8" if args.precision == "fp8"
                                                                              else ""),
                      "share_of_step": match_share},
+        "rescore": rescore,
         "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
         "plain_fp32_di": fp32_cmp,
         "fp8": fp8,
@@ -1460,8 +1475,8 @@ def main():
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the companion learned-path measurement")
-    ap.add_argument("--no-pacing", action="store_true",
-                    help="launch the match kernels without CTA pacing (ebsd_set_match_pacing(0)), for A/B runs")
+    ap.add_argument("--pacing", action="store_true",
+                    help="launch the match kernels with CTA pacing (ebsd_set_match_pacing(1)), for A/B runs")
     ap.add_argument("--fp32-subset", type=int, default=8192)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (48 maps, mixed sizes, detectors, phases) instead")
@@ -1476,10 +1491,10 @@ def main():
     ap.add_argument("--pyramid", default="3.0,1.5,0.75", help="intermediate dictionary resolutions (deg), coarse first")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
-    if args.no_pacing and args.impl == "ours":
+    if args.pacing and args.impl == "ours":
         from ebsdtorch_b200 import _capi
 
-        _capi.load().ebsd_set_match_pacing(0)
+        _capi.load().ebsd_set_match_pacing(1)
     if args.impl == "reference":
         run_reference(args, wl)
     elif args.learned:

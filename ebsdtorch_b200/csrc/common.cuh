@@ -243,11 +243,40 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// try_wait that suspends the thread for at most about hint_ns (the
+// instruction's suspend-time hint) before it reports "not yet".
+__device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait under a limit shorter than the default (a caller-set watchdog): no
+// spin phase, and every try_wait suspends for at most 200 ns, so the limit
+// is checked at least every 200 ns whatever the hardware's own suspend time.
+static __device__ __noinline__ bool mbar_wait_short(uint32_t bar, uint32_t parity, volatile int* abort,
+                                             uint64_t limit_ns) {
+  const uint64_t t0 = globaltimer_ns();
+#pragma unroll 1
+  while (true) {
+    if (mbar_try_wait_hint(bar, parity, 200u)) return true;
+    if (*abort) return false;
+    if (globaltimer_ns() - t0 > limit_ns) return false;
+  }
+}
+
 // Bounded wait on an mbarrier phase. Returns false when the wait limit
 // (limit_ns, counted after a short spin) expired or when *abort became
 // non-zero (another role gave up).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
                                           uint64_t limit_ns = kWaitLimitNs) {
+  if (limit_ns < kWaitLimitNs) return mbar_wait_short(bar, parity, abort, limit_ns);
 #pragma unroll 1
   for (int i = 0; i < 256; ++i)
     if (mbar_try_wait(bar, parity)) return true;
@@ -265,6 +294,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 // between polls instead of issuing back-to-back try_waits.
 __device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity, volatile int* abort,
                                                 uint64_t limit_ns = kWaitLimitNs) {
+  if (limit_ns < kWaitLimitNs) return mbar_wait_short(bar, parity, abort, limit_ns);
 #pragma unroll 1
   for (int i = 0; i < 32; ++i)
     if (mbar_try_wait(bar, parity)) return true;

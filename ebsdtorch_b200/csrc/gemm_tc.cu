@@ -538,8 +538,9 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 
 // Wait limit handed to every tensor-core kernel launch (0 = kWaitLimitNs).
 static std::atomic<uint64_t> g_wait_limit_ns{0};
-// Pacing of one-wave match launches: on (1) by default; epoch per launch.
-static std::atomic<int> g_pacing{1};
+// Pacing of one-wave match launches: off (0) by default (measured slower,
+// see ebsd_set_match_pacing); epoch per launch.
+static std::atomic<int> g_pacing{0};
 static std::atomic<uint32_t> g_pace_epoch{0};
 
 static uint64_t wait_limit_ns() {

@@ -33,6 +33,9 @@ MATCH_TIMERS: Optional[list] = None
 # When set to a one-element int64 device tensor, the merge kernels add the
 # number of rows they re-score in FP32 to it (measurement only).
 RESCORE_COUNTER: Optional[torch.Tensor] = None
+# When set to a list, Searcher.run appends (start, end) CUDA-event pairs
+# around every merge + re-score launch (measurement only).
+MERGE_TIMERS: Optional[list] = None
 
 
 @dataclass
@@ -324,6 +327,11 @@ class Searcher:
                         timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))
                     run = ci > 0
                     g0, g1 = q0 + s0, q0 + s1
+                    mtimers = MERGE_TIMERS
+                    if mtimers is not None:
+                        m0 = torch.cuda.Event(enable_timing=True)
+                        m1 = torch.cuda.Event(enable_timing=True)
+                        m0.record()
                     kernels.merge_rescore(
                         part_val, part_idx, ns, splits, self.n_cand,
                         q_rows.f32[s0:s1] if self.rescore else None,
@@ -333,6 +341,9 @@ class Searcher:
                         min(self.n_rescore, splits * self.n_cand), k,
                         out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
                         out_val[g0:g1], out_idx[g0:g1], gate_rel=gate, n_rescored=RESCORE_COUNTER)
+                    if mtimers is not None:
+                        m1.record()
+                        mtimers.append((m0, m1))
         if check:
             check_status(status)
         return out_idx, out_val
