@@ -16,9 +16,22 @@ is needed between steps.
 Multi-GPU (torchrun, one rank per GPU): every rank indexes its own full map
 (replicas, weak scaling, no collective on the data path); the timed region
 is bracketed by barriers and the slowest rank's time is reported.
---impl reference times the reference algorithm's CPU implementation (the
-NumPy port in oracle/, all host threads) on a bounded sample of the same
-workload and reports the rate extrapolated to the full workload.
+
+Baselines run the reference itself (staged in oracle/_ref by oracle/stage_ref.py;
+the NumPy port in oracle/ only when it is not staged):
+  --impl reference   the reference's own CPU dictionary_index_orientations on
+                     all host threads, int8 (its default) and float32, on a
+                     bounded sample, rated for the full workload
+  plain_fp32_di      the reference's own dictionary_index_orientations with
+                     match_dtype=float32 on this GPU (chunk-size sweep)
+  cpu_baseline       the reference's default CPU path, as --impl reference
+
+Companion objects of the default line: the e4m3 path (with its roofline
+against a measured e4m3 GEMM peak), the learned-proposal path (network
+trained outside the timed region), the margin-gated FP32 re-score, and, on a
+single GPU, PCA DI, grid refinement, preprocessing and pattern-centre
+fitting. Each also has a mode of its own (--pca, --refine, --preprocess,
+--pcfit, --learned, --batched) printing its line alone.
 """
 
 from __future__ import annotations
@@ -635,6 +648,19 @@ def run_ours(args, wl):
     if not args.no_learned and tuple(wl["det"]) == (128, 128):
         learned = learned_block(args, wl, mp, geom, pats, exp, ref_top1, n_sub if fp32_cmp else 0, dist, dev)
 
+    # ---- companion measurements of the other rows (single GPU): PCA DI and
+    # grid refinement on this run's own patterns, preprocessing and pattern-
+    # centre fitting on their own small workloads ----
+    companions = None
+    if not args.no_companions and n == 1 and tuple(wl["det"]) == (128, 128):
+        di_ori = exp.orientations.clone()
+        companions = {"pca": pca_block(args, wl, mp, geom, truth, pats, dev),
+                      "refine": refine_block(args, wl, mp, geom, truth, pats, di_ori, dev, min(args.steps, 3))}
+        del di_ori
+        short = argparse.Namespace(**{**vars(args), "no_cpu_baseline": True})
+        companions["preprocess"] = run_preprocess(short)
+        companions["pcfit"] = run_pcfit(short)
+
     # ---- end to end: host (pinned) patterns, H2D + D2H inside the timed region ----
     e2e = None
     if not args.no_e2e:
@@ -695,6 +721,7 @@ def run_ours(args, wl):
         "plain_fp32_di": fp32_cmp,
         "fp8": fp8,
         "learned": learned,
+        "companions": companions,
         "clocks": clk,
     }
     if rank == 0 and n == 1 and not args.no_cpu_baseline:
@@ -821,40 +848,45 @@ def run_learned(args, wl):
 
 
 def run_refine(args, wl):
-    """Orientation grid refinement after DI on the full workload: DI (bf16 +
-    FP32 re-score) first, then the timed refinement of every pattern
-    (orientation_grid_refinement, radius 1 (27 candidates), 3 iterations,
-    semi-edge = the dictionary resolution, left FZ reduction)."""
     import torch
 
-    from ebsdtorch_b200 import _capi, synthetic
-    from ebsdtorch_b200.ebsd import (EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations,
-                                     orientation_grid_refinement)
-    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+    from ebsdtorch_b200 import _capi
+    from ebsdtorch_b200.ebsd import ExperimentPatterns, dictionary_index_orientations
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     _capi.load()
-    mp = MasterPattern(synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev), laue_group=11)
-    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
-    truth = synthetic.random_quaternions(wl["Q"], 1000).to(dev)
-    pats = synthetic.synthetic_patterns(mp.master_pattern, geom, truth, mean_counts=wl["counts"], seed=2000)
+    mp, geom, truth, pats = _full_workload_inputs(wl, dev)
     exp = ExperimentPatterns(pats)
     torch.manual_seed(0)
     dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=wl["res"], top_k_matches=1,
                                   match_dtype=torch.float32)
-    di_ori = exp.orientations.clone()
+    print(json.dumps(refine_block(args, wl, mp, geom, truth, pats, exp.orientations.clone(), dev, args.steps)),
+          flush=True)
+
+
+def refine_block(args, wl, mp, geom, truth, pats, di_ori, dev, steps) -> dict:
+    """Orientation grid refinement after DI on the full workload: the timed
+    refinement of every pattern from its DI orientation
+    (orientation_grid_refinement, radius 1 (27 candidates), 3 iterations,
+    semi-edge = the dictionary resolution, left FZ reduction)."""
+    import torch
+
+    from ebsdtorch_b200.ebsd import ExperimentPatterns, orientation_grid_refinement
+    from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
+
+    exp = ExperimentPatterns(pats)
     before = torch.rad2deg(disori_angle_laue(di_ori.float().contiguous(), truth, 11, 11))
     kw = dict(grid_semi_edge_in_degrees=wl["res"], batch_size=wl["Q"], n_iter=3, kernel_radius_in_steps=1,
               fz_reduction="left")
-    for _ in range(args.warmup):
+    for _ in range(max(1, min(args.warmup, 3))):
         exp.set_orientations(di_ori.clone())
         orientation_grid_refinement(mp, geom, exp, **kw)
     torch.cuda.synchronize()
     with ClockSampler(int(dev.index or 0)) as clocks:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         total = 0.0
-        for _ in range(args.steps):
+        for _ in range(steps):
             exp.set_orientations(di_ori.clone())
             torch.cuda.synchronize()
             e0.record()
@@ -862,13 +894,13 @@ def run_refine(args, wl):
             e1.record()
             torch.cuda.synchronize()
             total += e0.elapsed_time(e1) / 1e3
-    secs = total / args.steps
+    secs = total / steps
     after = torch.rad2deg(disori_angle_laue(exp.orientations.float().contiguous(), truth, 11, 11))
     n_pix = wl["det"][0] * wl["det"][1]
     samples = wl["Q"] * 27 * 3 * n_pix
     line = {
         "metric": "patterns refined/s (orientation grid refinement after DI)", "value": wl["Q"] / secs,
-        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
+        "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "grid refinement (radius 1 = 27 candidates, 3 iterations, semi-edge %.2f deg, "
                                "left FZ reduction) of plain-DI results; " % wl["res"] + wl["name"]},
@@ -878,7 +910,8 @@ def run_refine(args, wl):
                                         "refined_within_0.5": float((after < 0.5).float().mean())},
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    del exp
+    return line
 
 
 def _short_step_counts(args, step):
@@ -1062,7 +1095,7 @@ def run_preprocess(args):
                                 "sample": "oracle (NumPy float64) standard_clean + nlpar k_rad 3 on a 24 x 24 crop "
                                           "of 60 x 60 patterns (%.1f s)" % csecs}
     del out
-    print(json.dumps(line), flush=True)
+    return line
 
 
 PCFIT = dict(det=(60, 60), n=16, x=(0.35, 0.65), y=(0.35, 0.65), z=(0.4, 0.7, 8), res=2.0, bs=1024, mp=257,
@@ -1184,14 +1217,40 @@ def run_pcfit(args):
         line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "fits/s", "cores": 1, "kind": "port",
                                 "sample": "oracle (NumPy float64) on 64 orientations x 1 pc_z step, extrapolated to "
                                           "%d orientations x %d steps" % (n_dict, z_steps)}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 BATCHED = dict(maps=48, q_min=1000, q_max=200000, detectors=((60, 60), (80, 80), (128, 128), (160, 160)),
                phases=((11, 0.5), (9, 0.615), (5, 0.88)), mp=1001, counts=100.0, seed=3)
 
 
+def _full_workload_inputs(wl, dev, rank=0):
+    """Master pattern, geometry, true orientations and patterns of a workload
+    (seeded; rank 0 gets the same map in every mode)."""
+    from ebsdtorch_b200 import synthetic
+    from ebsdtorch_b200.ebsd import EBSDGeometry, MasterPattern
+
+    mp = MasterPattern(synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev), laue_group=11)
+    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
+    truth = synthetic.random_quaternions(wl["Q"], 1000 + rank).to(dev)
+    pats = synthetic.synthetic_patterns(mp.master_pattern, geom, truth, mean_counts=wl["counts"], seed=2000 + rank)
+    return mp, geom, truth, pats
+
+
 def run_pca(args):
+    import torch
+
+    from ebsdtorch_b200 import _capi
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    _capi.load()
+    wl = WORKLOADS["full"]
+    mp, geom, truth, pats = _full_workload_inputs(wl, dev)
+    print(json.dumps(pca_block(args, wl, mp, geom, truth, pats, dev)), flush=True)
+
+
+def pca_block(args, wl, mp, geom, truth, pats, dev) -> dict:
     """PCA dictionary indexing at the full size: 128 x 128 px, a basis of
     1,024 components fitted on the m-3m 0.9 deg dictionary (51,312 rows),
     indexing against the 0.5 deg dictionary (328,720 rows), 262,144 patterns,
@@ -1202,22 +1261,13 @@ def run_pca(args):
     FP32 re-score in PCA space)."""
     import torch
 
-    from ebsdtorch_b200 import _capi, engine, synthetic
-    from ebsdtorch_b200.ebsd import (EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations,
-                                     pca_dictionary_index_orientations)
+    from ebsdtorch_b200 import _capi, engine
+    from ebsdtorch_b200.ebsd import ExperimentPatterns, dictionary_index_orientations, pca_dictionary_index_orientations
     from ebsdtorch_b200.ebsd import indexing as I
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
     from ebsdtorch_b200.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
 
-    wl = WORKLOADS["full"]
     n_comp, learn_res = 1024, 0.9
-    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
-    torch.cuda.set_device(dev)
-    _capi.load()
-    mp = MasterPattern(synthetic.synthetic_master_pattern(wl["mp"], seed=0, device=dev), laue_group=11)
-    geom = EBSDGeometry(wl["det"], tilts_degrees=(0.0, 70.0, 0.0), proj_center=(0.5, 0.5, 0.6))
-    truth = synthetic.random_quaternions(wl["Q"], 1000).to(dev)
-    pats = synthetic.synthetic_patterns(mp.master_pattern, geom, truth, mean_counts=wl["counts"], seed=2000)
     exp = ExperimentPatterns(pats)
 
     # ---- one-time fit ----
@@ -1332,7 +1382,8 @@ def run_pca(args):
                      "subset": n_sub, "within_0.5deg_of_truth": float((b < math.radians(0.5)).float().mean())},
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line), flush=True)
+    del exp, exp_p, comps
+    return line
 
 
 def run_batched(args):
@@ -1475,6 +1526,8 @@ def main():
     ap.add_argument("--no-fp32-compare", action="store_true")
     ap.add_argument("--no-fp8", action="store_true", help="skip the companion e4m3 measurement")
     ap.add_argument("--no-learned", action="store_true", help="skip the companion learned-path measurement")
+    ap.add_argument("--no-companions", action="store_true",
+                    help="skip the companion PCA / refinement / preprocessing / pattern-centre-fit measurements")
     ap.add_argument("--pacing", action="store_true",
                     help="launch the match kernels with CTA pacing (ebsd_set_match_pacing(1)), for A/B runs")
     ap.add_argument("--fp32-subset", type=int, default=8192)
@@ -1504,9 +1557,9 @@ def main():
     elif args.refine:
         run_refine(args, wl)
     elif args.preprocess:
-        run_preprocess(args)
+        print(json.dumps(run_preprocess(args)), flush=True)
     elif args.pcfit:
-        run_pcfit(args)
+        print(json.dumps(run_pcfit(args)), flush=True)
     elif args.pca:
         run_pca(args)
     else:
