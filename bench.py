@@ -1528,8 +1528,6 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the companion learned-path measurement")
     ap.add_argument("--no-companions", action="store_true",
                     help="skip the companion PCA / refinement / preprocessing / pattern-centre-fit measurements")
-    ap.add_argument("--pacing", action="store_true",
-                    help="launch the match kernels with CTA pacing (ebsd_set_match_pacing(1)), for A/B runs")
     ap.add_argument("--fp32-subset", type=int, default=8192)
     ap.add_argument("--learned", action="store_true", help="time the learned-proposal path instead")
     ap.add_argument("--batched", action="store_true", help="time batched uneven maps (48 maps, mixed sizes, detectors, phases) instead")
@@ -1544,10 +1542,6 @@ def main():
     ap.add_argument("--pyramid", default="3.0,1.5,0.75", help="intermediate dictionary resolutions (deg), coarse first")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
-    if args.pacing and args.impl == "ours":
-        from ebsdtorch_b200 import _capi
-
-        _capi.load().ebsd_set_match_pacing(1)
     if args.impl == "reference":
         run_reference(args, wl)
     elif args.learned:

@@ -35,7 +35,6 @@ SIGNATURES = {
     "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
     "ebsd_match_auto_splits": (i32, [i64, i64]),
     "ebsd_set_wait_limit_ns": (i64, [i64]),
-    "ebsd_set_match_pacing": (i32, [i32]),
     "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
     "ebsd_match_topk_tiled": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, vp, vp, i32, i32, i32,
                                     i32, i32, vp, vp]),

@@ -260,6 +260,9 @@ __device__ __forceinline__ bool mbar_try_wait_hint(uint32_t bar, uint32_t parity
 // Wait under a limit shorter than the default (a caller-set watchdog): no
 // spin phase, and every try_wait suspends for at most 200 ns, so the limit
 // is checked at least every 200 ns whatever the hardware's own suspend time.
+// Only the epilogue's waits (mbar_wait_sleep) take this path: it gives up
+// first, and the producer and MMA threads then stop on the abort flag, so
+// their latency-critical waits keep the plain form below.
 static __device__ __noinline__ bool mbar_wait_short(uint32_t bar, uint32_t parity, volatile int* abort,
                                              uint64_t limit_ns) {
   const uint64_t t0 = globaltimer_ns();
@@ -276,7 +279,6 @@ static __device__ __noinline__ bool mbar_wait_short(uint32_t bar, uint32_t parit
 // non-zero (another role gave up).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
                                           uint64_t limit_ns = kWaitLimitNs) {
-  if (limit_ns < kWaitLimitNs) return mbar_wait_short(bar, parity, abort, limit_ns);
 #pragma unroll 1
   for (int i = 0; i < 256; ++i)
     if (mbar_try_wait(bar, parity)) return true;

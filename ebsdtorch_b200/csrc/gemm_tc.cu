@@ -42,9 +42,8 @@ struct Tile {
   static constexpr int STAGES = BN_ == 256 ? 4 : 6;
   static constexpr int B_BYTES = BN_ * BKB;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 2) + 16;
-  static constexpr int PACE_BYTES = 8 * 256;  // fetched pacing slots (kPaceSlots)
-  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + PACE_BYTES + BAR_BYTES;
+  static constexpr int BAR_BYTES = 8 * (2 * STAGES + 4 + 1) + 16;
+  static constexpr int SMEM_BYTES = 1024 + STAGES * STAGE_BYTES + SCRATCH_BYTES + BAR_BYTES;
   static constexpr uint32_t TMEM_COLS = 2 * BN_;  // two accumulators
   static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 };
@@ -77,53 +76,7 @@ struct GemmParams {
   int relu;
   int* status;
   uint64_t wait_ns;  // limit of every role's waits (kWaitLimitNs by default)
-  // Pacing of one-wave match launches (0 = off): every kPaceEvery stages a
-  // producer publishes its stage count and lets CTAs more than pace_window
-  // stages behind catch up (bounded by kPaceMaxWaitNs).
-  int pace_window;
-  uint32_t pace_epoch;
 };
-
-// Stage counts published by the producers of paced launches, one slot per
-// CTA: (epoch << 32) | stages issued. A launch only reads slots stamped with
-// its own epoch, so stale or foreign entries are ignored. 2 KB per device,
-// part of the module image.
-constexpr int kPaceSlots = 256;
-constexpr int kPaceEvery = 32;              // stages between two checkpoints
-constexpr uint64_t kPaceMaxWaitNs = 20000;  // longest wait at one checkpoint
-static __device__ __align__(16) unsigned long long g_pace[kPaceSlots];
-
-__device__ __forceinline__ void pace_publish(int slot, uint32_t epoch, uint32_t stages) {
-  const unsigned long long v = ((unsigned long long)epoch << 32) | stages;
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(g_pace + slot), "l"(v) : "memory");
-}
-
-// Untiled bulk copy of the first `bytes` of g_pace into shared memory,
-// completion signalled on `bar` (16-byte aligned, size a multiple of 16).
-__device__ __forceinline__ void pace_fetch(uint32_t dst, uint32_t bytes, uint32_t bar) {
-  mbar_arrive_expect_tx(bar, bytes);
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-      "l"((uint64_t)__cvta_generic_to_global(g_pace)), "r"(bytes), "r"(bar)
-      : "memory");
-}
-
-// Largest lag behind `stages` among the fetched slots of this launch's
-// epoch, ignoring CTAs more than `far` stages behind (a CTA that started
-// late cannot catch up within a checkpoint).
-__device__ __forceinline__ uint32_t pace_lag(const unsigned long long* slots, int n, uint32_t epoch,
-                                             uint32_t stages, uint32_t far) {
-  uint32_t lag = 0;
-#pragma unroll 8
-  for (int i = 0; i < n; ++i) {
-    const unsigned long long v = slots[i];
-    if ((uint32_t)(v >> 32) != epoch) continue;
-    const uint32_t st = (uint32_t)v;
-    const uint32_t d = st < stages ? stages - st : 0u;
-    if (d <= far && d > lag) lag = d;
-  }
-  return lag;
-}
 
 template <int KIND, int BN>
 __host__ __device__ constexpr uint32_t make_idesc() {
@@ -154,10 +107,12 @@ __device__ __forceinline__ void report_timeout(const GemmParams& p, volatile int
   atomicExch(p.status, EBSD_DEVICE_TIMEOUT);
 }
 
-// MODE 0: top-k epilogue. MODE 1: store epilogue. MODE 2: convolution
+// MODE 0: top-k epilogue (BIAS: plus col_bias[col] * row_scale[row], the
+// euclidean ranking; a separate instantiation so that the angular kernel's
+// epilogue carries none of it). MODE 1: store epilogue. MODE 2: convolution
 // epilogue, out[col, row] = act(acc[row, col] + bias[row]) stored transposed
 // in bf16 (and FP32 when asked).
-template <int KIND, int MODE, int KC, int BN, bool PERSIST>
+template <int KIND, int MODE, int KC, int BN, bool PERSIST, bool BIAS = false>
 __global__ void __launch_bounds__(THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
               const GemmParams p) {
@@ -169,17 +124,14 @@ __global__ void __launch_bounds__(THREADS, 1)
   uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
   const uint32_t sbase = smem_u32(smem);
   float* scratch = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
-  unsigned long long* pace_slots =
-      reinterpret_cast<unsigned long long*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES + T::PACE_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
   const uint32_t bar0 = smem_u32(bars);
   auto full_bar = [&](int s) { return bar0 + 8u * s; };
   auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
   auto accf_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
   auto acce_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
   const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
-  const uint32_t pace_bar = bar0 + 8u * (2 * STAGES + 5);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 6);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -207,7 +159,6 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(acce_bar(a), EPI_THREADS);
     }
     mbar_init(drain_bar, 1);
-    mbar_init(pace_bar, 1);
     *abort_flag = 0;
     fence_mbar_init();
   }
@@ -234,22 +185,6 @@ __global__ void __launch_bounds__(THREADS, 1)
       uint32_t stage = 0, phase = 0;
       bool ok = true;
       const int k_iters = p.k_iters;
-      const int pace_window = PERSIST ? 0 : p.pace_window;
-      const uint32_t pace_epoch = p.pace_epoch;
-      // pacing: the slots are fetched asynchronously at one checkpoint and
-      // read at the next, so an on-time CTA never waits for the fetch
-      const int pace_n = (int)gridDim.x;
-      const uint32_t pace_bytes = (uint32_t)((pace_n + 1) / 2) * 16u;
-      const uint32_t pace_dst = smem_u32(pace_slots);
-      uint32_t pace_phase = 0;
-      bool pace_pending = false;
-      volatile int pace_never = 0;
-      auto pace_collect = [&]() -> uint32_t {
-        mbar_wait(pace_bar, pace_phase, &pace_never);
-        pace_phase ^= 1u;
-        pace_pending = false;
-        return pace_lag(pace_slots, pace_n, pace_epoch, (uint32_t)issued, 8u * (uint32_t)pace_window);
-      };
       auto produce_unit = [&](int u) {
         const int a_row = unit_tile(u) * BM;
         int n_begin, n_end;
@@ -259,21 +194,6 @@ __global__ void __launch_bounds__(THREADS, 1)
             if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, wait_ns)) {
               ok = false;
               break;
-            }
-            if (pace_window > 0 && (issued & (kPaceEvery - 1)) == 0 && issued > 0) {
-              uint32_t lag = pace_pending ? pace_collect() : 0u;
-              if (lag > (uint32_t)pace_window) {
-                const uint64_t t0 = globaltimer_ns();
-                while (lag > (uint32_t)pace_window && globaltimer_ns() - t0 < kPaceMaxWaitNs) {
-                  __nanosleep(256);
-                  pace_fetch(pace_dst, pace_bytes, pace_bar);
-                  pace_pending = true;
-                  lag = pace_collect();
-                }
-              }
-              pace_publish(blockIdx.x, pace_epoch, (uint32_t)issued);
-              pace_fetch(pace_dst, pace_bytes, pace_bar);
-              pace_pending = true;
             }
             const uint32_t a_dst = sbase + stage * STAGE_BYTES;
             mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
@@ -296,7 +216,6 @@ __global__ void __launch_bounds__(THREADS, 1)
         produce_unit(blockIdx.x);
       }
       if (!ok) report_timeout(p, abort_flag);
-      if (pace_pending) pace_collect();  // the last slot fetch lands before the CTA exits
       prod_stage = stage;
       prod_phase = phase;
     }
@@ -377,7 +296,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         bv[j] = -INFINITY;
         bi[j] = -1;
       }
-      const float rs = (MODE == 0 && p.row_scale) ? __ldg(p.row_scale + (int64_t)m_tile * BM + row) : 0.0f;
+      float rs = 0.0f;
+      if constexpr (MODE == 0 && BIAS) rs = __ldg(p.row_scale + (int64_t)m_tile * BM + row);
       for (int n = n_begin; n < n_end; ++n) {
         bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag, wait_ns);
         got = __all_sync(0xffffffffu, got);
@@ -408,7 +328,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                   v[4 * j4 + 3] *= s4.w;
                 }
               }
-              if (p.col_bias) {
+              if constexpr (BIAS) {
                 const float4* cb = reinterpret_cast<const float4*>(p.col_bias + col0);
 #pragma unroll
                 for (int j4 = 0; j4 < 8; ++j4) {
@@ -424,8 +344,12 @@ __global__ void __launch_bounds__(THREADS, 1)
               for (int j = 0; j < 32; ++j) {
                 const bool valid = col0 + j < p.n_valid;
                 const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
-                const float cb = (valid && p.col_bias) ? __ldg(p.col_bias + col0 + j) : 0.0f;
-                v[j] = valid ? fmaf(cb, rs, v[j] * sc) : -INFINITY;
+                if constexpr (BIAS) {
+                  const float cb = valid ? __ldg(p.col_bias + col0 + j) : 0.0f;
+                  v[j] = valid ? fmaf(cb, rs, v[j] * sc) : -INFINITY;
+                } else {
+                  v[j] = valid ? v[j] * sc : -INFINITY;
+                }
               }
             }
 #pragma unroll
@@ -538,10 +462,6 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 
 // Wait limit handed to every tensor-core kernel launch (0 = kWaitLimitNs).
 static std::atomic<uint64_t> g_wait_limit_ns{0};
-// Pacing of one-wave match launches: off (0) by default (measured slower,
-// see ebsd_set_match_pacing); epoch per launch.
-static std::atomic<int> g_pacing{0};
-static std::atomic<uint32_t> g_pace_epoch{0};
 
 static uint64_t wait_limit_ns() {
   const uint64_t v = g_wait_limit_ns.load(std::memory_order_relaxed);
@@ -588,10 +508,10 @@ static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t ro
   return 0;
 }
 
-template <int KIND, int MODE, int KC, int BN, bool PERSIST = false>
+template <int KIND, int MODE, int KC, int BN, bool PERSIST = false, bool BIAS = false>
 static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p_in, int grid,
                   cudaStream_t s) {
-  auto kern = k_tc_gemm<KIND, MODE, KC, BN, PERSIST>;
+  auto kern = k_tc_gemm<KIND, MODE, KC, BN, PERSIST, BIAS>;
   constexpr int smem = Tile<BN>::SMEM_BYTES;
   EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   GemmParams p = p_in;
@@ -601,17 +521,17 @@ static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& 
   return 0;
 }
 
-template <int KIND, int BN, bool PERSIST>
+template <int KIND, int BN, bool PERSIST, bool BIAS = false>
 static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
                        int grid, cudaStream_t s) {
   switch (kc) {
-    case 1: return launch<KIND, 0, 1, BN, PERSIST>(a, b, p, grid, s);
-    case 2: return launch<KIND, 0, 2, BN, PERSIST>(a, b, p, grid, s);
-    case 4: return launch<KIND, 0, 4, BN, PERSIST>(a, b, p, grid, s);
-    case 8: return launch<KIND, 0, 8, BN, PERSIST>(a, b, p, grid, s);
-    case 16: return launch<KIND, 0, 16, BN, PERSIST>(a, b, p, grid, s);
-    case 32: return launch<KIND, 0, 32, BN, PERSIST>(a, b, p, grid, s);
-    case 64: return launch<KIND, 0, 64, BN, PERSIST>(a, b, p, grid, s);
+    case 1: return launch<KIND, 0, 1, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 2: return launch<KIND, 0, 2, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 4: return launch<KIND, 0, 4, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 8: return launch<KIND, 0, 8, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 16: return launch<KIND, 0, 16, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 32: return launch<KIND, 0, 32, BN, PERSIST, BIAS>(a, b, p, grid, s);
+    case 64: return launch<KIND, 0, 64, BN, PERSIST, BIAS>(a, b, p, grid, s);
   }
   set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
   return EBSD_ERR_ARG;
@@ -620,6 +540,11 @@ static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const
 template <int KIND>
 static int launch_topk_shape(int kc, int tile_n, bool persist, const CUtensorMap& a, const CUtensorMap& b,
                              const GemmParams& p, int grid, cudaStream_t s) {
+  if (p.col_bias) {
+    // the euclidean variant exists for the default launch shape only
+    EBSD_ARG_CHECK(tile_n == 256 && !persist, "col_bias needs 256-row tiles and a non-persistent launch");
+    return launch_topk<KIND, 256, false, true>(kc, a, b, p, grid, s);
+  }
   if (tile_n == 128)
     return persist ? launch_topk<KIND, 128, true>(kc, a, b, p, grid, s)
                    : launch_topk<KIND, 128, false>(kc, a, b, p, grid, s);
@@ -652,10 +577,6 @@ using namespace ebsd;
 extern "C" int64_t ebsd_set_wait_limit_ns(int64_t ns) {
   const uint64_t prev = g_wait_limit_ns.exchange(ns > 0 ? (uint64_t)ns : 0u);
   return prev ? (int64_t)prev : (int64_t)kWaitLimitNs;
-}
-
-extern "C" int ebsd_set_match_pacing(int on) {
-  return g_pacing.exchange(on ? 1 : 0);
 }
 
 extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
@@ -717,13 +638,6 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   // loops over its units
   const bool persist = max_ctas > 0 && max_ctas < p.units;
   const int grid = persist ? max_ctas : p.units;
-  // pace one-wave launches over long rows: all CTAs are resident together
-  // and each streams many stages of shared operand tiles
-  if (!persist && g_pacing.load(std::memory_order_relaxed) && grid <= device_sm_count() && grid < kPaceSlots &&
-      p.k_iters >= 64) {
-    p.pace_window = p.k_iters / 2;
-    p.pace_epoch = g_pace_epoch.fetch_add(1, std::memory_order_relaxed) + 1;
-  }
   cudaStream_t s = as_stream(stream);
   return lp_dtype == EBSD_DT_BF16 ? launch_topk_shape<0>(n_cand, tile_n, persist, ta, tb, p, grid, s)
                                   : launch_topk_shape<1>(n_cand, tile_n, persist, ta, tb, p, grid, s);

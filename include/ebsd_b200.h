@@ -13,10 +13,9 @@
  * Conventions
  *  - All pointers are device pointers unless stated otherwise; buffers are
  *    allocated by the caller. The library makes no device allocation of its
- *    own; its only device memory is part of the module image, held by every
- *    GPU that loads the library until the process exits: the 32 MiB scratch
- *    array of ebsd_match_topk_noalloc and the 2 KB of pacing slots of the
- *    match kernel (see ebsd_set_match_pacing).
+ *    own; its only device memory is the 32 MiB scratch array of
+ *    ebsd_match_topk_noalloc, part of the module image, which every GPU
+ *    that loads the library holds until the process exits.
  *  - Work is enqueued on `stream` (a cudaStream_t passed as void*); calls are
  *    asynchronous unless stated otherwise.
  *  - Return value: 0 success, > 0 argument error (nothing launched),
@@ -176,15 +175,6 @@ int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad);
  * Meant for tests and for callers that want a tighter watchdog. */
 int64_t ebsd_set_wait_limit_ns(int64_t ns);
 
-/* No counterpart in the reference: switches pacing of one-wave match launches
- * on (1) or off (0, the default); returns the previous setting. With pacing,
- * the CTAs of a launch that stream long rows (>= 64 stages per tile) publish
- * their progress every 32 stages in a 2 KB module array and a CTA that is more
- * than half a tile ahead of another waits (at most 20 us per checkpoint), so
- * the CTAs that share operand tiles read them from L2 rather than DRAM.
- * Results do not depend on it. It is off by default because on B200 the
- * checkpoints cost more time than the saved DRAM traffic buys back. */
-int ebsd_set_match_pacing(int on);
 
 int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
                     int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,
