@@ -876,6 +876,7 @@ def refine_block(args, wl, mp, geom, truth, pats, di_ori, dev, steps) -> dict:
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
 
     exp = ExperimentPatterns(pats)
+    exp.phases = torch.zeros(pats.shape[0], dtype=torch.uint8, device=pats.device)  # one phase, as after DI
     before = torch.rad2deg(disori_angle_laue(di_ori.float().contiguous(), truth, 11, 11))
     kw = dict(grid_semi_edge_in_degrees=wl["res"], batch_size=wl["Q"], n_iter=3, kernel_radius_in_steps=1,
               fz_reduction="left")

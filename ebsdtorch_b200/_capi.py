@@ -35,6 +35,7 @@ SIGNATURES = {
     "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
     "ebsd_match_auto_splits": (i32, [i64, i64]),
     "ebsd_set_wait_limit_ns": (i64, [i64]),
+    "ebsd_manhattan_topk": (i32, [vp, i64, i64, i64, vp, i64, i64, i32, i32, i32, vp, vp, i32, i32, i32, vp]),
     "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
     "ebsd_match_topk_tiled": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, vp, vp, i32, i32, i32,
                                     i32, i32, vp, vp]),
@@ -80,7 +81,7 @@ SIGNATURES = {
 }
 
 DT_F32, DT_BF16, DT_E4M3 = 0, 1, 2
-SIM_DOT, SIM_COSINE, SIM_EUCLIDEAN = 0, 1, 2
+SIM_DOT, SIM_COSINE, SIM_EUCLIDEAN, SIM_MANHATTAN = 0, 1, 2, 3
 DEVICE_TIMEOUT = 0x7001
 
 # kernels launched by one successful call of each entry point
@@ -88,7 +89,7 @@ LAUNCHES_PER_CALL = {
     "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
     "ebsd_prep_patterns": 1, "ebsd_prep_patterns_typed": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1,
     "ebsd_match_topk": 1, "ebsd_match_topk_tiled": 1,
-    "ebsd_merge_rescore": 1, "ebsd_merge_rescore_gated": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
+    "ebsd_merge_rescore": 1, "ebsd_merge_rescore_gated": 1, "ebsd_manhattan_topk": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
     "ebsd_disori_angle": 1, "ebsd_match_topk_noalloc": 2, "ebsd_zh_to_qu": 1, "ebsd_qu_to_zh": 1,
     "ebsd_cell_to_row": 2, "ebsd_local_search": 1, "ebsd_refine_grid": 1,
     "ebsd_pattern_mean": 2, "ebsd_subtract_pattern": 1, "ebsd_normalize_patterns": 1, "ebsd_clahe": 1,

@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   __shared__ int sel[kMaxRescore];
   __shared__ float tau_s;
   __shared__ int n_sel;
+  __shared__ float part[(kMergeThreads / 32) * kMaxRescore];  // per-warp partial dots
 
   const int64_t q = blockIdx.x;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
@@ -103,6 +104,8 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   // that "larger ranks first" holds for every metric.
   const int nr = n_rescore;
   const bool euclid = similarity == EBSD_SIM_EUCLIDEAN;
+  // distances (euclidean, manhattan) are reported positive, smallest first
+  const bool dist = euclid || similarity == EBSD_SIM_MANHATTAN;
   if (d_f32) {
     // 2a. which of them can reach the exact top k_out (margin gate)
     const bool gate = gate_rel > 0.0f && nr > k_out && !euclid;
@@ -138,49 +141,70 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     }
     const int ns = n_sel;
     if (n_rescored && tid == 0) atomicAdd(n_rescored, (unsigned long long)ns);
-    // four rows per warp at once (four 16-byte loads in flight per lane)
-    constexpr int R = 4;
+    // Every warp takes a slice of the pixels of every selected row, R rows at
+    // a time (R 16-byte loads in flight per lane), so all warps stream even
+    // when few rows are selected; the per-warp partial dots are summed in a
+    // fixed order (deterministic).
+    constexpr int R = 8;
     const bool vec = (n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0;
-    for (int s0 = wid * R; s0 < ns; s0 += nw * R) {
-      int64_t di[R];
+    const int n4 = n_pix >> 2;
+    for (int s0 = 0; s0 < ns; s0 += R) {
       const float* d[R];
-      int cc[R];
 #pragma unroll
       for (int j = 0; j < R; ++j) {
-        cc[j] = s0 + j < ns ? sel[s0 + j] : -1;
-        const int c = cc[j];
-        di[j] = (c >= 0 && ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
-        d[j] = d_f32 + (di[j] >= 0 ? di[j] - d_base : 0) * ld_d;  // a missing row re-reads row 0
+        const int c = s0 + j < ns ? sel[s0 + j] : -1;
+        const int64_t i = (c >= 0 && ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
+        d[j] = d_f32 + (i >= 0 ? i - d_base : 0) * ld_d;  // a missing row re-reads row 0
       }
       float acc[R];
+#pragma unroll
+      for (int j = 0; j < R; ++j) acc[j] = 0.0f;
       if (vec) {
-        f32_dot_rows<R>(qrow, d, n_pix >> 2, lane, acc);
-      } else {
+        const float4* q4 = reinterpret_cast<const float4*>(qrow);
+        for (int v = tid; v < n4; v += blockDim.x) {
+          float4 x[R];
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          float a = 0.0f;
-          for (int p = lane; p < n_pix; p += 32) a = fmaf(__ldg(d[j] + p), qrow[p], a);
-          acc[j] = warp_sum(a);
-        }
-      }
-      if (lane == 0) {
+          for (int j = 0; j < R; ++j)  // rows past ns are skipped (uniform over the CTA)
+            x[j] = s0 + j < ns ? __ldg(reinterpret_cast<const float4*>(d[j]) + v) : make_float4(0.f, 0.f, 0.f, 0.f);
+          const float4 y = q4[v];
 #pragma unroll
-        for (int j = 0; j < R; ++j) {
-          const int c = cc[j];
-          if (c < 0) break;
-          float v = acc[j];
-          if (similarity == EBSD_SIM_COSINE && di[j] >= 0) {
-            const float den = q_norm[q] * d_norm[di[j] - d_base];
-            v = den > 0.0f ? v / den : 0.0f;
-          } else if (euclid && di[j] >= 0) {
-            // |q|^2 + |d|^2 - 2 q.d with FP32 norms of the zero-mean rows (knn.py:85-91)
-            const float qn = q_norm[q], dn = d_norm[di[j] - d_base];
-            v = -(fmaf(qn, qn, dn * dn) - 2.0f * v);
+          for (int j = 0; j < R; ++j) {
+            acc[j] = fmaf(x[j].x, y.x, acc[j]);
+            acc[j] = fmaf(x[j].y, y.y, acc[j]);
+            acc[j] = fmaf(x[j].z, y.z, acc[j]);
+            acc[j] = fmaf(x[j].w, y.w, acc[j]);
           }
-          fin_v[c] = di[j] >= 0 ? v : -INFINITY;
-          fin_i[c] = di[j];
+        }
+      } else {
+        for (int p = tid; p < n_pix; p += blockDim.x) {
+          const float y = qrow[p];
+#pragma unroll
+          for (int j = 0; j < R; ++j)
+            if (s0 + j < ns) acc[j] = fmaf(__ldg(d[j] + p), y, acc[j]);
         }
       }
+#pragma unroll
+      for (int j = 0; j < R; ++j) {
+        const float w = warp_sum(acc[j]);
+        if (lane == 0 && s0 + j < ns) part[wid * kMaxRescore + s0 + j] = w;
+      }
+    }
+    __syncthreads();
+    if (tid < ns) {
+      const int c = sel[tid];
+      const int64_t i = (ci[c] >= d_base && ci[c] < d_base + d_rows) ? ci[c] : -1;
+      float v = 0.0f;
+      for (int w = 0; w < nw; ++w) v += part[w * kMaxRescore + tid];
+      if (similarity == EBSD_SIM_COSINE && i >= 0) {
+        const float den = q_norm[q] * d_norm[i - d_base];
+        v = den > 0.0f ? v / den : 0.0f;
+      } else if (euclid && i >= 0) {
+        // |q|^2 + |d|^2 - 2 q.d with FP32 norms of the zero-mean rows (knn.py:85-91)
+        const float qn = q_norm[q], dn = d_norm[i - d_base];
+        v = -(fmaf(qn, qn, dn * dn) - 2.0f * v);
+      }
+      fin_v[c] = i >= 0 ? v : -INFINITY;
+      fin_i[c] = i;
     }
   } else {
     float qn = q_lp_scale ? q_lp_scale[q] : 1.0f;
@@ -198,7 +222,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
   if (run_val) {
     for (int c = tid; c < k_out; c += blockDim.x) {
       const float rv = run_val[q * k_out + c];
-      fin_v[nr + c] = euclid ? -rv : rv;
+      fin_v[nr + c] = dist ? -rv : rv;
       fin_i[nr + c] = run_idx[q * k_out + c];
     }
     nf += k_out;
@@ -215,12 +239,12 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     for (int o = 0; o < nf; ++o)
       if (o != tid && ranks_before(fin_v[o], fin_i[o], v, i)) ++rank;
     if (rank < k_out) {
-      out_val[q * k_out + rank] = euclid ? -v : v;
+      out_val[q * k_out + rank] = dist ? -v : v;
       out_idx[q * k_out + rank] = i;
     }
   }
   for (int r = n_valid + tid; r < k_out; r += blockDim.x) {
-    out_val[q * k_out + r] = euclid ? INFINITY : -INFINITY;
+    out_val[q * k_out + r] = dist ? INFINITY : -INFINITY;
     out_idx[q * k_out + r] = -1;
   }
 }
@@ -246,8 +270,10 @@ extern "C" int ebsd_merge_rescore_gated(const float* part_val, const int32_t* pa
   EBSD_ARG_CHECK(n_rescore >= 1 && n_rescore <= kMaxRescore && n_rescore <= n_list,
                  "n_rescore %d outside [1, min(%d, %d)]", n_rescore, kMaxRescore, n_list);
   EBSD_ARG_CHECK(!(run_val == nullptr) == !(run_idx == nullptr), "run_val/run_idx must be given together");
-  EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || similarity == EBSD_SIM_COSINE || similarity == EBSD_SIM_EUCLIDEAN,
-                 "similarity must be EBSD_SIM_DOT, EBSD_SIM_COSINE or EBSD_SIM_EUCLIDEAN");
+  EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || similarity == EBSD_SIM_COSINE || similarity == EBSD_SIM_EUCLIDEAN ||
+                     similarity == EBSD_SIM_MANHATTAN,
+                 "similarity must be EBSD_SIM_DOT, EBSD_SIM_COSINE, EBSD_SIM_EUCLIDEAN or EBSD_SIM_MANHATTAN");
+  EBSD_ARG_CHECK(similarity != EBSD_SIM_MANHATTAN || !d_f32, "manhattan candidates are exact: no re-score");
   EBSD_ARG_CHECK(similarity != EBSD_SIM_EUCLIDEAN || q_norm, "euclidean scores need q_norm");
   if (d_f32) {
     EBSD_ARG_CHECK(q_f32 != nullptr, "q_f32 is required for re-scoring");

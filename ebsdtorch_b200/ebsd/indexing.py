@@ -44,7 +44,7 @@ def _device(mp, device) -> torch.device:
 
 
 def _check_common(distance_metric: str, average_pattern_center: bool):
-    if distance_metric not in ("angular", "euclidean"):
+    if distance_metric not in ("angular", "euclidean", "manhattan"):
         raise NotImplementedError(f"'{distance_metric}' not supported.")
     if not average_pattern_center:
         raise NotImplementedError(
@@ -55,11 +55,11 @@ def _check_common(distance_metric: str, average_pattern_center: bool):
 def _similarity(distance_metric: str, similarity: str) -> str:
     """The engine's score for the reference's distance_metric: "angular" is
     the raw dot of zero-mean rows (or its cosine when asked), "euclidean" the
-    squared euclidean distance (knn.py:85-97)."""
-    if distance_metric == "euclidean":
+    squared euclidean distance, "manhattan" the L1 distance (knn.py:85-97)."""
+    if distance_metric in ("euclidean", "manhattan"):
         if similarity != "dot":
             raise ValueError("similarity applies to distance_metric='angular' only")
-        return "euclidean"
+        return distance_metric
     return similarity
 
 

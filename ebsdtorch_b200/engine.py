@@ -21,7 +21,7 @@ from typing import Callable, Optional
 import torch
 
 from . import kernels
-from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT, SIM_EUCLIDEAN
+from ._capi import DEVICE_TIMEOUT, SIM_COSINE, SIM_DOT, SIM_EUCLIDEAN, SIM_MANHATTAN
 from .kernels import LP_DTYPES, LP_KMULT, LP_TORCH, TILE_D, TILE_Q, RowBuffers, round_up
 
 MAX_CAND = 64
@@ -45,7 +45,8 @@ class SearchConfig:
     low-precision score). similarity: "dot" is the reference's angular metric
     (raw dot of zero-mean rows, knn.py:96-97); "cosine" divides it by both
     norms; "euclidean" is the reference's squared euclidean distance of the
-    zero-mean rows (knn.py:85-91), smallest first.
+    zero-mean rows (knn.py:85-91), smallest first; "manhattan" their L1
+    distance (knn.py:92-93), exact FP32 on the CUDA cores, smallest first.
     workspace_bytes: device-memory budget (default: 90 % of free memory)."""
 
     precision: str = "bf16"
@@ -72,8 +73,9 @@ class SearchConfig:
     def validate(self):
         if self.precision not in LP_DTYPES:
             raise ValueError(f"precision must be one of {sorted(LP_DTYPES)}, got {self.precision!r}")
-        if self.similarity not in ("dot", "cosine", "euclidean"):
-            raise ValueError(f"similarity must be 'dot', 'cosine' or 'euclidean', got {self.similarity!r}")
+        if self.similarity not in ("dot", "cosine", "euclidean", "manhattan"):
+            raise ValueError(f"similarity must be 'dot', 'cosine', 'euclidean' or 'manhattan', "
+                             f"got {self.similarity!r}")
         if not 0 <= self.rescore_k <= 128:
             raise ValueError("rescore_k must be in [0, 128]")
         if self.tile_n not in (0, 128, 256):
@@ -211,16 +213,21 @@ class Searcher:
         self.n_dict, self.n_queries, self.n_pix, self.k, self.cfg = n_dict, n_queries, n_pix, k, cfg
         self.device = torch.device(device)
         self.lp_dtype = LP_DTYPES[cfg.precision]
-        self.rescore = cfg.rescore_k > 0
-        self.n_cand = min(MAX_CAND, _pow2_at_least(max(k, cfg.rescore_k)))
+        self.manhattan = cfg.similarity == "manhattan"
+        # manhattan candidates are exact FP32 distances: nothing to re-score,
+        # but the FP32 rows are the kernel's input
+        self.rescore = cfg.rescore_k > 0 and not self.manhattan
+        self.keep_f32 = self.rescore or self.manhattan
+        self.n_cand = min(MAX_CAND, _pow2_at_least(max(k, cfg.rescore_k if self.rescore else k)))
         self.n_rescore = max(k, cfg.rescore_k) if self.rescore else k
-        self.sim = {"dot": SIM_DOT, "cosine": SIM_COSINE, "euclidean": SIM_EUCLIDEAN}[cfg.similarity]
+        self.sim = {"dot": SIM_DOT, "cosine": SIM_COSINE, "euclidean": SIM_EUCLIDEAN,
+                    "manhattan": SIM_MANHATTAN}[cfg.similarity]
         self._plan()
 
     def _plan(self):
         budget = self.cfg.workspace_bytes or default_budget(self.device)
-        drow = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
-        qrow_base = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.rescore)
+        drow = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.keep_f32)
+        qrow_base = RowSet.bytes_per_row(self.n_pix, self.lp_dtype, self.keep_f32)
         qrow = qrow_base + self.k * 12
         q_min = min(round_up(self.n_queries, TILE_Q), 16384)
         if self.cfg.dict_chunk:
@@ -257,14 +264,14 @@ class Searcher:
             status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.status = status
         if resident is not None:
-            if resident.n_rows != D or resident.lp_dtype != self.lp_dtype or (self.rescore and resident.f32 is None):
+            if resident.n_rows != D or resident.lp_dtype != self.lp_dtype or (self.keep_f32 and resident.f32 is None):
                 raise ValueError("resident dictionary rows do not match the search")
             self.dict_chunk = D
             dict_rows = resident
         else:
-            dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.rescore, dev)
+            dict_rows = RowSet(self.dict_chunk, self.n_pix, TILE_D, self.lp_dtype, self.keep_f32, dev)
         qc = self.query_chunk
-        q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.rescore, dev)
+        q_rows = RowSet(qc, self.n_pix, TILE_Q, self.lp_dtype, self.keep_f32, dev)
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         cfg = self.cfg
         split_cap = MAX_MERGE_CANDIDATES // self.n_cand
@@ -318,10 +325,16 @@ class Searcher:
                         ev0 = torch.cuda.Event(enable_timing=True)
                         ev1 = torch.cuda.Event(enable_timing=True)
                         ev0.record()
-                    kernels.match_topk(q_rows.lp[s0:s0 + ns_pad], d_lp, nd, self.lp_dtype, col_scale, self.n_cand,
-                                       splits, part_val, part_idx, splits, 0, d0, status, tile_n=cfg.tile_n,
-                                       max_ctas=max_ctas, col_bias=col_bias,
-                                       row_scale=row_scale[s0:] if row_scale is not None else None)
+                    if self.manhattan:
+                        splits = max(1, min(max_splits, split_cap, (nd + 63) // 64,
+                                            2 * sms // max(1, ns_pad // 64) + 1))
+                        kernels.manhattan_topk(q_rows.f32[s0:s1], ns, ns_pad, dict_rows.f32[:nd], self.n_pix,
+                                               self.n_cand, splits, part_val, part_idx, splits, 0, d0)
+                    else:
+                        kernels.match_topk(q_rows.lp[s0:s0 + ns_pad], d_lp, nd, self.lp_dtype, col_scale,
+                                           self.n_cand, splits, part_val, part_idx, splits, 0, d0, status,
+                                           tile_n=cfg.tile_n, max_ctas=max_ctas, col_bias=col_bias,
+                                           row_scale=row_scale[s0:] if row_scale is not None else None)
                     if timers is not None:
                         ev1.record()
                         timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))
@@ -336,9 +349,10 @@ class Searcher:
                         part_val, part_idx, ns, splits, self.n_cand,
                         q_rows.f32[s0:s1] if self.rescore else None,
                         dict_rows.f32[:nd] if self.rescore else None, d0,
-                        self.n_pix, q_rows.norm[s0:], dict_rows.norm,
-                        q_rows.lp_scale[s0:] if q_rows.lp_scale is not None else None, self.sim,
-                        min(self.n_rescore, splits * self.n_cand), k,
+                        self.n_pix, None if self.manhattan else q_rows.norm[s0:], dict_rows.norm,
+                        q_rows.lp_scale[s0:] if (q_rows.lp_scale is not None and not self.manhattan) else None,
+                        self.sim, min(max(self.n_rescore, self.n_cand if self.manhattan else 0),
+                                      splits * self.n_cand, 128), k,
                         out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
                         out_val[g0:g1], out_idx[g0:g1], gate_rel=gate, n_rescored=RESCORE_COUNTER)
                     if mtimers is not None:

@@ -179,6 +179,17 @@ def match_topk(q_lp, d_lp, n_dict_valid: int, lp_dtype: int, col_scale, n_cand: 
          _stream(q_lp.device))
 
 
+def manhattan_topk(q_f32, n_queries: int, n_queries_pad: int, d_f32, n_pix: int, n_cand: int, splits: int,
+                   part_val, part_idx, part_slots: int, slot_base: int, index_base: int) -> None:
+    """L1-distance candidates (score -L1) of FP32 query rows against FP32
+    dictionary rows, in the candidate layout of match_topk."""
+    _cuda(q_f32, "q_f32", torch.float32, contiguous=False)
+    _cuda(d_f32, "d_f32", torch.float32, contiguous=False)
+    call("ebsd_manhattan_topk", ptr(q_f32), q_f32.stride(0), int(n_queries), int(n_queries_pad), ptr(d_f32),
+         d_f32.stride(0), d_f32.shape[0], int(n_pix), int(n_cand), int(splits), ptr(part_val), ptr(part_idx),
+         int(part_slots), int(slot_base), int(index_base), _stream(q_f32.device))
+
+
 def rescore_gate(lp_dtype: int, k_pad: int, n_pix: int) -> float:
     """Bound on |s' - s| / w for unit low-precision rows (see
     ebsd_merge_rescore_gated), or 0 (no gate) for e4m3, whose bound is too

@@ -212,6 +212,8 @@ int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const v
  *                               q_norm[q]^2 + d_norm[.]^2 - 2 dot (knn.py:85-91); the
  *                               best k_out are the smallest, sorted ascending, and
  *                               missing entries are +inf / -1; run_val holds distances
+ *   similarity EBSD_SIM_MANHATTAN: candidates scored -L1 (ebsd_manhattan_topk), no
+ *                               re-score (d_f32 NULL); distances out, as for euclidean
  * (candidate indices are global; d_f32/d_norm hold rows d_index_base ..
  * d_index_base + d_rows - 1; a candidate outside that range is dropped)
  * With d_f32 == NULL nothing is re-scored and the score is
@@ -220,6 +222,7 @@ int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const v
 #define EBSD_SIM_DOT 0
 #define EBSD_SIM_COSINE 1
 #define EBSD_SIM_EUCLIDEAN 2
+#define EBSD_SIM_MANHATTAN 3
 int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n_queries,
                        int part_slots, int n_cand, const float* q_f32, int64_t ld_q,
                        const float* d_f32, int64_t ld_d, int64_t d_index_base, int64_t d_rows,
@@ -228,6 +231,21 @@ int ebsd_merge_rescore(const float* part_val, const int32_t* part_idx, int64_t n
                        int similarity, int n_rescore,
                        int k_out, const float* run_val, const int64_t* run_idx, float* out_val,
                        int64_t* out_idx, void* stream);
+
+/* ---- distance_metric="manhattan" -------------------------------------------
+ * Replaces knn_batch's manhattan branch (knn.py:92-93: the L1 distance of the
+ * zero-mean rows, smallest first), which is not a contraction: FP32 rows on
+ * the CUDA cores. q_f32 (n_queries x n_pix, row stride ld_q; n_queries_pad a
+ * multiple of 64), d_f32 (n_dict x n_pix, stride ld_d). The dictionary is cut
+ * into `splits` ranges (1 <= splits <= ceil(n_dict / 64)); each (64-query
+ * tile, range) writes its best n_cand (score = -L1, index + index_base),
+ * sorted best first, in ebsd_match_topk's candidate layout (rows up to
+ * n_queries_pad). ebsd_merge_rescore(_gated) with EBSD_SIM_MANHATTAN and no
+ * re-score turns them into distances. */
+int ebsd_manhattan_topk(const float* q_f32, int64_t ld_q, int64_t n_queries, int64_t n_queries_pad,
+                        const float* d_f32, int64_t ld_d, int64_t n_dict, int n_pix, int n_cand, int splits,
+                        float* part_val, int32_t* part_idx, int part_slots, int slot_base, int32_t index_base,
+                        void* stream);
 
 /* As ebsd_merge_rescore, with a margin gate on the FP32 re-score (no
  * counterpart in the reference, which scores every candidate in its match

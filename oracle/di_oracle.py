@@ -587,6 +587,27 @@ def topk_euclidean(queries: np.ndarray, data: np.ndarray, k: int, chunk: int = 4
     return best_i, best_v
 
 
+def topk_manhattan(queries: np.ndarray, data: np.ndarray, k: int, chunk: int = 256):
+    """Top-k by the smallest L1 distance sum |q - d| (knn.py:92-93 with
+    largest=False), sorted ascending; ties resolve to the lower index.
+    Returns (indices int64 (Q, k), distances (Q, k))."""
+    Q = queries.shape[0]
+    best_v = np.full((Q, k), np.inf, dtype=np.result_type(queries, data))
+    best_i = np.zeros((Q, k), dtype=np.int64)
+    for d0 in range(0, data.shape[0], chunk):
+        blk = data[d0 : d0 + chunk]
+        dist = np.abs(queries[:, None, :] - blk[None, :, :]).sum(axis=2)
+        kk = min(k, blk.shape[0])
+        part = np.argpartition(dist, kk - 1, axis=1)[:, :kk]
+        pv = np.take_along_axis(dist, part, axis=1)
+        allv = np.concatenate((best_v, pv), axis=1)
+        alli = np.concatenate((best_i, part + d0), axis=1)
+        o = np.lexsort((alli, allv), axis=1)[:, :k]
+        best_v = np.take_along_axis(allv, o, axis=1)
+        best_i = np.take_along_axis(alli, o, axis=1)
+    return best_i, best_v
+
+
 # --------------------------------------------------------------------------
 # End-to-end plain DI (A1-A13)
 # --------------------------------------------------------------------------
@@ -635,8 +656,9 @@ def dictionary_index(
 ):
     """Plain DI for one phase (indexing.py:14-211). Returns
     (orientations (Q, k, 4), metrics (Q, k), indices (Q, k), dictionary (D, 4));
-    distance_metric "angular" (largest raw dot first) or "euclidean"
-    (smallest squared distance first, knn.py:85-91)."""
+    distance_metric "angular" (largest raw dot first), "euclidean"
+    (smallest squared distance first, knn.py:85-91) or "manhattan" (smallest
+    L1 distance first, knn.py:92-93)."""
     if dictionary is None:
         dictionary = sample_ori_fz_laue_angle(laue_id, resolution_deg, permutation)
     mp = avg_pool(np.asarray(master_pattern, dtype=np.float64), binning)
@@ -646,6 +668,8 @@ def dictionary_index(
     q = prep_patterns(patterns, binning, mask, True, dtype)
     if distance_metric == "euclidean":
         idx, val = topk_euclidean(q, d, top_k)
+    elif distance_metric == "manhattan":
+        idx, val = topk_manhattan(q, d, top_k)
     elif distance_metric == "angular":
         idx, val = topk_dot(q, d, top_k)
     else:

@@ -327,9 +327,10 @@ def config0_goldens(root=None):
 
 def euclidean_goldens(root=None):
     """The reference's plain DI with distance_metric="euclidean" (knn.py:85-91,
-    squared distance of the zero-mean rows, smallest first), float32 matching
-    on its chunked query path, top-3, plus a second case with a signal mask
-    and binning 2 on the all-at-once path."""
+    squared distance of the zero-mean rows) and "manhattan" (:92-93, L1
+    distance), smallest first, float32 matching: per metric one case on its
+    chunked query path (top-3) and one with a signal mask and binning 2 on
+    the all-at-once path (top-2)."""
     ref_idx, _ = load_reference(root)
     from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
     from ebsdtorch.ebsd.geometry import EBSDGeometry
@@ -340,8 +341,14 @@ def euclidean_goldens(root=None):
     from ebsdtorch.s2_and_so3.sampling import so3_uniform_quat
 
     out = {}
-    for ci, c in enumerate((dict(det=(20, 20), res=8.0, Q=31, k=3, b=1, mask=False, ec=8, dcs=50, seed=91),
-                            dict(det=(24, 24), res=9.0, Q=19, k=2, b=2, mask=True, ec=4096, dcs=4096, seed=92))):
+    for ci, c in enumerate((dict(det=(20, 20), res=8.0, Q=31, k=3, b=1, mask=False, ec=8, dcs=50, seed=91,
+                                 metric="euclidean"),
+                            dict(det=(24, 24), res=9.0, Q=19, k=2, b=2, mask=True, ec=4096, dcs=4096, seed=92,
+                                 metric="euclidean"),
+                            dict(det=(20, 20), res=8.0, Q=23, k=3, b=1, mask=False, ec=8, dcs=50, seed=93,
+                                 metric="manhattan"),
+                            dict(det=(24, 24), res=9.0, Q=17, k=2, b=2, mask=True, ec=4096, dcs=4096, seed=94,
+                                 metric="manhattan"))):
         torch.manual_seed(c["seed"])
         mp_t = smooth_master_pattern(c["seed"], 41)
         mp = MasterPattern(mp_t.clone(), laue_group=11)
@@ -361,7 +368,7 @@ def euclidean_goldens(root=None):
             ref_idx.dictionary_index_orientations(
                 mp, geom, exp, signal_mask=mask, experiment_chunk_size=c["ec"],
                 dictionary_resolution_degrees=c["res"], dictionary_chunk_size=c["dcs"], virtual_binning=c["b"],
-                top_k_matches=c["k"], distance_metric="euclidean", match_dtype=torch.float32,
+                top_k_matches=c["k"], distance_metric=c["metric"], match_dtype=torch.float32,
                 quantized_if_x86=False)
         torch.manual_seed(c["seed"] + 1000)
         dictionary = sample_ori_fz_laue_angle(11, c["res"], torch.device("cpu"), permute=True).numpy()
@@ -370,6 +377,7 @@ def euclidean_goldens(root=None):
         out[f"case{ci}_mask"] = mask.numpy() if mask is not None else np.zeros(0, bool)
         out[f"case{ci}_meta"] = np.array([*c["det"], c["res"], c["Q"], c["k"], c["b"], c["ec"], c["dcs"],
                                           c["seed"] + 1000], dtype=np.float64)
+        out[f"case{ci}_metric"] = np.array(c["metric"])
         out[f"case{ci}_quats"] = exp.raw_indexing_results[0][0].numpy()
         out[f"case{ci}_dists"] = exp.raw_indexing_results[0][1].numpy()
         out[f"case{ci}_best"] = exp.best_metrics.numpy()

@@ -183,11 +183,12 @@ def test_synthetic_small_config_parity_and_accuracy():
     assert torch.median(ang).item() < np.deg2rad(4.0)
 
 
-@pytest.mark.parametrize("case", [0, 1])
+@pytest.mark.parametrize("case", [0, 1, 2, 3])
 @pytest.mark.parametrize("precision", ["bf16", "fp8"])
-def test_euclidean_distance_matches_reference(golden, case, precision):
-    """distance_metric="euclidean": the reference's squared distances
-    (knn.py:85-91), smallest first, combined with higher_is_better=False."""
+def test_distance_metric_matches_reference(golden, case, precision):
+    """distance_metric="euclidean" (cases 0, 1: the reference's squared
+    distances, knn.py:85-91) and "manhattan" (cases 2, 3: L1 distances,
+    :92-93), smallest first, combined with higher_is_better=False."""
     from ebsdtorch_b200.ebsd import EBSDGeometry, ExperimentPatterns, MasterPattern, dictionary_index_orientations
 
     d = golden("di_euclid")
@@ -201,8 +202,8 @@ def test_euclidean_distance_matches_reference(golden, case, precision):
     torch.manual_seed(seed)
     dictionary_index_orientations(mp, geom, exp, signal_mask=mask, experiment_chunk_size=ec,
                                   dictionary_resolution_degrees=res, dictionary_chunk_size=dcs, virtual_binning=b,
-                                  top_k_matches=k, distance_metric="euclidean", match_dtype=torch.float32,
-                                  precision=precision)
+                                  top_k_matches=k, distance_metric=str(d[f"case{case}_metric"]),
+                                  match_dtype=torch.float32, precision=precision)
     quats, dists = exp.raw_indexing_results[0]
     ref = d[f"case{case}_dists"]
     assert np.abs(quats.cpu().numpy() - d[f"case{case}_quats"]).max() < 1e-5
@@ -231,3 +232,26 @@ def test_euclidean_matches_oracle_with_dictionary_chunks():
     assert (gi[:, 0] == oi[:, 0]).mean() >= 0.99
     same = gi == oi
     assert np.abs(gv - ov)[same].max() <= 1e-4 * np.abs(ov).max()
+
+
+def test_manhattan_matches_oracle_with_dictionary_chunks():
+    """The manhattan candidates (exact FP32 L1 distances on the CUDA cores)
+    merged across dictionary chunks and ranges, against the FP64 oracle."""
+    from ebsdtorch_b200 import synthetic
+    from ebsdtorch_b200.ebsd import dictionary_index_orientations
+
+    mp, geom, exp, _ = synthetic.make_case(129, (32, 32), 300, seed=6, mean_counts=80.0)
+    torch.manual_seed(4)
+    dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=4.0, top_k_matches=5,
+                                  distance_metric="manhattan", match_dtype=torch.float32, workspace_bytes=6 << 20)
+    dic = exp.dictionaries[0].cpu().numpy().astype(np.float64)
+    rays = O.unit_rays(O.detector_coords_sample_frame((32, 32), (0.5, 0.5, 0.6), (0.0, 70.0, 0.0)))
+    rows = O.dictionary_rows(mp.master_pattern.cpu().numpy(), rays, dic)
+    q = O.prep_patterns(exp.patterns.cpu().numpy())
+    oi, ov = O.topk_manhattan(q, rows, 5)
+    gi = exp.raw_indexing_indices[0].cpu().numpy()
+    gv = exp.raw_indexing_results[0][1].cpu().numpy()
+    assert (gi[:, 0] == oi[:, 0]).mean() >= 0.99
+    same = gi == oi
+    assert np.abs(gv - ov)[same].max() <= 1e-4 * np.abs(ov).max()
+    assert (np.diff(gv, axis=1) >= 0).all()

@@ -474,10 +474,10 @@ def test_config0_inputs_reproduce_the_golden_checksums(golden):
     assert (np.abs(val - ref_m)[same] / np.abs(ref_m[:, :1]).repeat(4, 1)[same]).max() < 1e-4
 
 
-@pytest.mark.parametrize("case", [0, 1])
-def test_euclidean_dictionary_index_matches_reference(golden, case):
-    """distance_metric="euclidean" (knn.py:85-91): squared distances of the
-    zero-mean rows, smallest first."""
+@pytest.mark.parametrize("case", [0, 1, 2, 3])
+def test_distance_metric_dictionary_index_matches_reference(golden, case):
+    """distance_metric="euclidean" (knn.py:85-91, squared distances) and
+    "manhattan" (:92-93, L1 distances) of the zero-mean rows, smallest first."""
     d = golden("di_euclid")
     m = d[f"case{case}_meta"]
     det, res, k, b = (int(m[0]), int(m[1])), m[2], int(m[4]), int(m[5])
@@ -485,7 +485,7 @@ def test_euclidean_dictionary_index_matches_reference(golden, case):
     oq, ov, _, _ = O.dictionary_index(d[f"case{case}_master_pattern"], 11, d[f"case{case}_patterns"], det,
                                       (0.5, 0.5, 0.6), (0, 70, 0), res, top_k=k, mask=mask, binning=b,
                                       dictionary=d[f"case{case}_dictionary"].astype(np.float64),
-                                      distance_metric="euclidean")
+                                      distance_metric=str(d[f"case{case}_metric"]))
     assert np.abs(oq - d[f"case{case}_quats"]).max() < 1e-6
     assert np.abs(ov - d[f"case{case}_dists"]).max() <= 1e-4 * np.abs(d[f"case{case}_dists"]).max()
     assert (np.diff(ov, axis=1) >= 0).all()
