@@ -322,7 +322,7 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, retu
 # (dram__bytes_read.sum + dram__bytes_write.sum) at two dictionary sizes. The
 # traffic is affine in the dictionary rows; the full launch's figure is its
 # extrapolation.
-MATCH_DRAM_BYTES = ((36829, 8432610816 + 6049792), (89312, 16465764864 + 9438208))
+MATCH_DRAM_BYTES = ((36829, 6738486528 + 6209024), (89312, 16461514240 + 7201792))
 
 
 def match_traffic_estimate(d_rows: int) -> float:
