@@ -68,8 +68,9 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     float* __restrict__ out_val, int64_t* __restrict__ out_idx, float gate_rel,
     unsigned long long* __restrict__ n_rescored) {
   extern __shared__ float dyn[];
-  float* qrow = dyn;                                            // n_pix (re-score only)
-  float* cv = dyn + (d_f32 ? ((n_pix + 3) & ~3) : 0);           // sort_n
+  // the query row is read from global memory (L1/L2-resident after its
+  // first pass): staging it in shared memory would cap the CTAs per SM
+  float* cv = dyn;                                                     // sort_n
   int64_t* ci = reinterpret_cast<int64_t*>(cv + ((sort_n + 1) & ~1));  // sort_n
   __shared__ float fin_v[kMaxRescore + kMaxKOut];
   __shared__ int64_t fin_i[kMaxRescore + kMaxKOut];
@@ -93,10 +94,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
       ci[t] = -1;
     }
   }
-  if (d_f32) {
-    const float* src = q_f32 + q * ld_q;
-    for (int p = tid; p < n_pix; p += blockDim.x) qrow[p] = src[p];
-  }
+  const float* qrow = d_f32 ? q_f32 + q * ld_q : nullptr;
   bitonic_sort(cv, ci, sort_n);
 
   // 2. exact FP32 scores of the best n_rescore (or approximate * |q|).
@@ -146,7 +144,8 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
     // when few rows are selected; the per-warp partial dots are summed in a
     // fixed order (deterministic).
     constexpr int R = 8;
-    const bool vec = (n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0;
+    const bool vec = (n_pix & 3) == 0 && (ld_d & 3) == 0 && ((uintptr_t)d_f32 & 15) == 0 && (ld_q & 3) == 0 &&
+                     ((uintptr_t)q_f32 & 15) == 0;
     const int n4 = n_pix >> 2;
     for (int s0 = 0; s0 < ns; s0 += R) {
       const float* d[R];
@@ -166,7 +165,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
 #pragma unroll
           for (int j = 0; j < R; ++j)  // rows past ns are skipped (uniform over the CTA)
             x[j] = s0 + j < ns ? __ldg(reinterpret_cast<const float4*>(d[j]) + v) : make_float4(0.f, 0.f, 0.f, 0.f);
-          const float4 y = q4[v];
+          const float4 y = __ldg(q4 + v);
 #pragma unroll
           for (int j = 0; j < R; ++j) {
             acc[j] = fmaf(x[j].x, y.x, acc[j]);
@@ -177,7 +176,7 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_rescore(
         }
       } else {
         for (int p = tid; p < n_pix; p += blockDim.x) {
-          const float y = qrow[p];
+          const float y = __ldg(qrow + p);
 #pragma unroll
           for (int j = 0; j < R; ++j)
             if (s0 + j < ns) acc[j] = fmaf(__ldg(d[j] + p), y, acc[j]);
@@ -280,7 +279,6 @@ extern "C" int ebsd_merge_rescore_gated(const float* part_val, const int32_t* pa
     EBSD_ARG_CHECK(similarity == EBSD_SIM_DOT || (q_norm && d_norm),
                    "cosine and euclidean re-scoring need q_norm and d_norm");
     EBSD_ARG_CHECK(n_pix >= 1 && ld_q >= n_pix && ld_d >= n_pix, "bad re-score row length");
-    EBSD_ARG_CHECK(n_pix <= 40960, "re-score row length %d exceeds 40960", n_pix);
     EBSD_ARG_CHECK(d_rows >= 1 && d_index_base >= 0, "bad dictionary row range");
     EBSD_ARG_CHECK(!(gate_rel > 0.0f) || similarity == EBSD_SIM_COSINE || d_norm,
                    "the margin gate of the dot metric needs d_norm");
@@ -289,8 +287,7 @@ extern "C" int ebsd_merge_rescore_gated(const float* part_val, const int32_t* pa
   if (n_queries == 0) return 0;
   int sort_n = 1;
   while (sort_n < n_list) sort_n <<= 1;
-  const size_t smem = (d_f32 ? (size_t)((n_pix + 3) & ~3) * 4 : 0) + (size_t)((sort_n + 1) & ~1) * 4 +
-                      (size_t)sort_n * 8 + 16;
+  const size_t smem = (size_t)((sort_n + 1) & ~1) * 4 + (size_t)sort_n * 8 + 16;
   EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_merge_rescore, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
   EBSD_ARG_CHECK(n_queries < INT32_MAX, "too many queries");

@@ -150,8 +150,8 @@ def test_argument_errors_are_loud():
     geom = EBSDGeometry((8, 8))
     mp = MasterPattern(torch.rand(9, 18), laue_group=11).to(DEV)
     exp = ExperimentPatterns(torch.randn(2, 8, 8, device=DEV))
-    with pytest.raises(NotImplementedError):
-        dictionary_index_orientations(mp, geom, exp, distance_metric="manhattan", dictionary_resolution_degrees=15)
+    with pytest.raises(NotImplementedError, match="'chebyshev' not supported"):  # knn.py:98-99's message
+        dictionary_index_orientations(mp, geom, exp, distance_metric="chebyshev", dictionary_resolution_degrees=15)
     with pytest.raises(NotImplementedError):
         dictionary_index_orientations(mp, geom, exp, average_pattern_center=False, dictionary_resolution_degrees=15)
     with pytest.raises(ValueError):
