@@ -1,10 +1,15 @@
 """Batched indexing of uneven maps (several phases, detector shapes, pattern
 storage types, FP32 and bf16 paths) in one autotuned, graph-captured batch."""
 
+import numpy as np
 import pytest
 import torch
 
+from oracle import di_oracle as O
+
 pytestmark = pytest.mark.gpu
+
+N_ORACLE = 64  # patterns per map checked against the FP64 oracle
 
 DEV = "cuda"
 
@@ -31,21 +36,18 @@ def _jobs():
     return jobs
 
 
-def _fp32_topk(job, ori, k):
-    """Exact FP32 top-k of the reference algorithm over the batch's dictionary."""
-    import bench
-    from ebsdtorch_b200.ebsd.indexing import _unit_rays_soa
-
-    rays = _unit_rays_soa(job.geometry, 1, None, DEV)
-    pats = job.experiment_patterns.patterns.to(DEV).float()
-    q = pats.reshape(pats.shape[0], -1)
-    q = q - q.mean(dim=1, keepdim=True)
-    idx, _, _, val = bench.plain_fp32_gpu_di(None, job.master_pattern.master_pattern, rays, ori, q, k,
-                                             return_values=True)
-    return idx, val
+def _oracle_topk(job, ori, k, n):
+    """FP64 oracle top-k (the reference algorithm, indexing.py:96-146 and
+    knn.py:96-103) of the map's first n patterns over the batch's dictionary."""
+    det = tuple(job.geometry.detector_shape)
+    rays = O.unit_rays(O.detector_coords_sample_frame(det, (0.5, 0.5, 0.6), (0.0, 70.0, 0.0)))
+    rows = O.dictionary_rows(job.master_pattern.master_pattern.cpu().numpy(), rays,
+                             ori.cpu().numpy().astype(np.float64))
+    q = O.prep_patterns(job.experiment_patterns.patterns[:n].cpu().numpy().astype(np.float64))
+    return O.topk_dot(q, rows, k)
 
 
-def test_batch_matches_per_map_fp32_search_and_graph_replays():
+def test_batch_matches_the_oracle_per_map_and_graph_replays():
     from ebsdtorch_b200.batch import LAUNCH_SHAPES, BatchIndexer
 
     jobs = _jobs()
@@ -64,14 +66,17 @@ def test_batch_matches_per_map_fp32_search_and_graph_replays():
               j.experiment_patterns.raw_indexing_results[0][1].clone()) for j in jobs]
     for job in jobs:
         exp = job.experiment_patterns
-        idx = exp.raw_indexing_indices[0]
-        ref_i, ref_v = _fp32_topk(job, exp.dictionaries[0], job.top_k)
+        idx = exp.raw_indexing_indices[0][:N_ORACLE].cpu().numpy()
+        ref_i, ref_v = _oracle_topk(job, exp.dictionaries[0], job.top_k, N_ORACLE)
         if job.rescore_k > 0:
-            assert (idx == ref_i).float().mean() >= 0.999
-            v = exp.raw_indexing_results[0][1]
-            assert float((v - ref_v).abs().max()) <= 1e-4 * float(ref_v.abs().max())
+            # FP32 re-scored maps: the exact top-k and the reference's metric
+            assert (idx == ref_i).mean() >= 0.99
+            v = exp.raw_indexing_results[0][1][:N_ORACLE].double().cpu().numpy()
+            same = idx == ref_i
+            assert np.abs(v - ref_v)[same].max() <= 1e-4 * np.abs(ref_v).max()
         else:
-            assert (idx[:, 0] == ref_i[:, 0]).float().mean() >= 0.99
+            # bf16-only maps: the top-1 of the low-precision scores
+            assert (idx[:, 0] == ref_i[:, 0]).mean() >= 0.95
         assert torch.equal(exp.orientations, exp.raw_indexing_results[0][0][:, 0])
     for _ in range(2):
         b.run(use_graph=True)
