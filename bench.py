@@ -1246,12 +1246,16 @@ def run_pca(args):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     _capi.load()
-    wl = WORKLOADS["full"]
+    # the profiling workload keeps the projection and match launches' shapes
+    # (16,384-row sub-chunks, 1,024 components) at a few GB: 8,192 patterns,
+    # the 1.0 deg dictionary, and a basis fitted on the 2.0 deg dictionary
+    wl = WORKLOADS["profile" if args.workload == "profile" else "full"]
+    learn_res = 2.0 if args.workload == "profile" else 0.9
     mp, geom, truth, pats = _full_workload_inputs(wl, dev)
-    print(json.dumps(pca_block(args, wl, mp, geom, truth, pats, dev)), flush=True)
+    print(json.dumps(pca_block(args, wl, mp, geom, truth, pats, dev, learn_res=learn_res)), flush=True)
 
 
-def pca_block(args, wl, mp, geom, truth, pats, dev) -> dict:
+def pca_block(args, wl, mp, geom, truth, pats, dev, learn_res: float = 0.9) -> dict:
     """PCA dictionary indexing at the full size: 128 x 128 px, a basis of
     1,024 components fitted on the m-3m 0.9 deg dictionary (51,312 rows),
     indexing against the 0.5 deg dictionary (328,720 rows), 262,144 patterns,
@@ -1268,7 +1272,7 @@ def pca_block(args, wl, mp, geom, truth, pats, dev) -> dict:
     from ebsdtorch_b200.s2_and_so3.laue_fz_misori import disori_angle_laue
     from ebsdtorch_b200.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
 
-    n_comp, learn_res = 1024, 0.9
+    n_comp = 1024
     exp = ExperimentPatterns(pats)
 
     # ---- one-time fit ----
