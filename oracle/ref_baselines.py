@@ -24,7 +24,6 @@ import os
 import time
 from typing import Dict, Optional, Sequence, Tuple
 
-
 from . import ref_loader
 
 
