@@ -628,13 +628,14 @@ def run_ours(args, wl):
         try:
             pk8 = gemm_peak_tflops("e4m3", dev)
         except Exception as exc:  # torch._scaled_mm unavailable: no measured e4m3 denominator
-            pk8 = {"sustained": float("nan"), "burst": float("nan"), "how": f"not measured ({exc})"}
+            pk8 = {"sustained": None, "burst": None, "how": f"not measured ({exc})"}
         i8 = exp8.raw_indexing_indices[0][:, 0]
         fp8 = {"value": n * wl["Q"] * args.steps / t8, "unit": UNIT, "ms_per_step": t8 / args.steps * 1e3,
                "same_top1_index_as_bf16": float((i8 == exp.raw_indexing_indices[0][:, 0]).float().mean()),
                "precision": "e4m3 match (per-row absmax scale) + FP32 re-score of top-32",
                "roofline": {"bound": "tensor", "achieved": ach8, "peak": pk8["sustained"], "unit": "TFLOP/s",
-                            "frac": ach8 / pk8["sustained"], "kernel": "k_tc_gemm kind::f8f6f4 (match + top-k)",
+                            "frac": ach8 / pk8["sustained"] if pk8["sustained"] else None,
+                            "kernel": "k_tc_gemm kind::f8f6f4 (match + top-k)",
                             "peak_source": "measured here: " + pk8["how"], "peak_burst": pk8["burst"],
                             "share_of_step": sum(ms8) / 1e3 / t8}}
         if fp32_cmp is not None:
