@@ -1544,7 +1544,7 @@ def main():
     ap.add_argument("--preprocess", action="store_true", help="time pattern preprocessing (clean + NLPAR) instead")
     ap.add_argument("--pcfit", action="store_true", help="time pattern-centre fitting instead")
     ap.add_argument("--pca", action="store_true", help="time PCA dictionary indexing (1,024 components) instead")
-    ap.add_argument("--train-steps", type=int, default=3000)
+    ap.add_argument("--train-steps", type=int, default=8000)
     ap.add_argument("--max-angle", type=float, default=16.0)
     ap.add_argument("--fallback-ratio", type=float, default=0.95)
     ap.add_argument("--stage-margin", type=float, default=1.6)
