@@ -1111,10 +1111,10 @@ PCFIT = dict(det=(60, 60), n=16, x=(0.35, 0.65), y=(0.35, 0.65), z=(0.4, 0.7, 8)
 
 def run_pcfit(args):
     """Pattern-centre fitting (spatial_fft_pc_fitter, fitting.py:359-540):
-    whole fits on the device, and the four stages of one dictionary chunk
-    timed apart (projection on the enlarged detector, rfft2, spectrum
-    product + irfft2, the fused fftshift / max / argmax reduction)."""
-    import numpy as np
+    whole fits on the device (the tensor-core correlation path), the stages
+    of one dictionary batch timed apart (projection on the enlarged detector,
+    spectra, fused inverse transforms + max over the batch, fold), and the
+    same fits through the cuFFT path for comparison."""
     import torch
 
     from ebsdtorch_b200 import _capi, kernels, synthetic
@@ -1137,52 +1137,71 @@ def run_pcfit(args):
     kw = dict(pc_x_min=cfg["x"][0], pc_x_max=cfg["x"][1], pc_y_min=cfg["y"][0], pc_y_max=cfg["y"][1],
               pc_z_min=cfg["z"][0], pc_z_max=cfg["z"][1], pc_z_steps=cfg["z"][2], dictionary_resolution_deg=cfg["res"],
               dictionary_indexing_batch_size=cfg["bs"], orientation_index="global")
-    steps = _short_step_counts(args, lambda: spatial_fft_pc_fitter(mp, pats, **kw))
-    l0 = _capi.launch_count
-    with ClockSampler(int(dev.index or 0)) as clocks:
+    H, W = cfg["det"]
+    pix, pad, (hp, wp) = F.get_3D_pixel_coords_with_periphery((H, W), torch.device("cpu"), *cfg["x"], *cfg["y"], 1)
+    if not F.xcorr_supported(hp, wp):
+        raise RuntimeError(f"the {hp} x {wp} enlarged detector is outside the correlation kernels' range")
+
+    def timed_fits(steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         for _ in range(steps):
-            pc, q = spatial_fft_pc_fitter(mp, pats, **kw)
+            res = spatial_fft_pc_fitter(mp, pats, **kw)
         e1.record()
         torch.cuda.synchronize()
-    secs = e0.elapsed_time(e1) / 1e3 / steps
+        return e0.elapsed_time(e1) / 1e3 / steps, res
+
+    steps = _short_step_counts(args, lambda: spatial_fft_pc_fitter(mp, pats, **kw))
+    l0 = _capi.launch_count
+    with ClockSampler(int(dev.index or 0)) as clocks:
+        secs, (pc, q) = timed_fits(steps)
     launches = (_capi.launch_count - l0) // steps
     n_dict = sample_ori_fz_laue_angle(11, cfg["res"], dev).shape[0]
-    H, W = cfg["det"]
-    pix, pad, (hp, wp) = F.get_3D_pixel_coords_with_periphery((H, W), torch.device("cpu"), *cfg["x"], *cfg["y"], 1)
     z_steps = cfg["z"][2]
     evals = n_dict * z_steps * cfg["n"] * hp * wp  # (orientation, pc_z, pattern, pc_x / pc_y shift) scores
 
-    # stages of one chunk of 1024 orientations
+    # the same fits through cuFFT (torch.fft) + ebsd_pcfit_reduce
+    supported = F.xcorr_supported
+    F.xcorr_supported = lambda h, w: False
+    try:
+        spatial_fft_pc_fitter(mp, pats, **kw)
+        fft_secs, (pc_fft, q_fft) = timed_fits(max(1, min(steps, 5)))
+    finally:
+        F.xcorr_supported = supported
+
+    # stages of one batch of cfg["bs"] orientations
     rays = F._rays_soa(pix.double().numpy(), 0.55, 70.0, 0.0, (H, W), dev)
     quats = sample_ori_fz_laue_angle(11, cfg["res"], dev)[:cfg["bs"]].float().contiguous()
-    n = quats.shape[0]
+    n, B = quats.shape[0], cfg["n"]
+    spec_len = 4 * (hp // 2 + 1) * (wp // 2 + 1)
     sims = torch.empty((n, hp * wp), device=dev)
-    padded = torch.randn((cfg["n"], hp, wp), device=dev)
-    pat_fft = torch.fft.rfft2(padded).conj()
+    spec = torch.empty((n, spec_len), device=dev)
+    tables = torch.empty((int(_capi.load().ebsd_pcfit_xcorr_table_bytes(hp, wp)),), dtype=torch.uint8, device=dev)
+    _capi.call("ebsd_pcfit_xcorr_tables", hp, wp, tables.data_ptr(), tables.numel(), None)
+    terms = torch.randn((B, spec_len), device=dev)
+    keys = torch.zeros((B * hp * wp,), dtype=torch.int64, device=dev)
+    best = torch.zeros((B, hp, wp), device=dev)
+    best_i = torch.zeros((B, hp, wp), dtype=torch.int64, device=dev)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
     mp_b = _master_pattern_tensor(mp, 1, dev)
-    best = torch.zeros((cfg["n"], hp, wp), device=dev)
-    best_i = torch.zeros((cfg["n"], hp, wp), dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev).cuda_stream
-    state = {}
 
     def st_project():
         kernels.project(mp_b, rays, quats, RowBuffers(f32=sims), subtract_mean=False)
 
-    def st_rfft():
-        state["spec"] = torch.fft.rfft2(sims.view(n, hp, wp))
+    def st_spectra():
+        _capi.call("ebsd_pcfit_spectra", sims.data_ptr(), hp * wp, n, hp, wp, tables.data_ptr(), spec.data_ptr(),
+                   status.data_ptr(), stream)
 
-    def st_corr():
-        state["corr"] = torch.fft.irfft2(state["spec"][:, None] * pat_fft[None], s=(hp, wp)).contiguous()
+    def st_xcorr():
+        _capi.call("ebsd_pcfit_xcorr_max", spec.data_ptr(), n, terms.data_ptr(), B, hp, wp, tables.data_ptr(),
+                   keys.data_ptr(), 0, status.data_ptr(), stream)
 
-    def st_reduce():
-        _capi.call("ebsd_pcfit_reduce", state["corr"].data_ptr(), n, cfg["n"], hp, wp, 0, best.data_ptr(),
-                   best_i.data_ptr(), stream)
+    def st_fold():
+        _capi.call("ebsd_pcfit_fold", keys.data_ptr(), keys.numel(), best.data_ptr(), best_i.data_ptr(), stream)
 
     stages = {}
-    for name, fn in (("project", st_project), ("rfft2", st_rfft), ("product_irfft2", st_corr),
-                     ("reduce", st_reduce)):
+    for name, fn in (("project", st_project), ("spectra", st_spectra), ("xcorr_max", st_xcorr), ("fold", st_fold)):
         fn()
         ts = []
         for _ in range(5):
@@ -1193,21 +1212,32 @@ def run_pcfit(args):
             torch.cuda.synchronize()
             ts.append(a.elapsed_time(b))
         stages[name] = statistics.median(ts)
+    if int(status.item()) != 0:
+        raise RuntimeError("pattern-centre correlation kernels reported a device timeout")
     peaks, src = _peaks()
-    red_bytes = n * cfg["n"] * hp * wp * 4 + 2 * cfg["n"] * hp * wp * 12  # correlations + best / index read-write
-    red_gbs = red_bytes / (stages["reduce"] / 1e3) / 1e9
+    # bf16 tensor FLOPs of the 3-term split per (pattern, simulated pattern)
+    # pair: stage A (2 WF rows x H x 2 H2) + stage B (H x W x 2 WF)
+    h2, wf = hp // 2 + 1, wp // 2 + 1
+    pair_flops = 2 * 3 * (2 * wf * hp * 2 * h2 + hp * wp * 2 * wf)
+    xc_tflops = pair_flops * n * B / (stages["xcorr_max"] / 1e3) / 1e12
     line = {
         "metric": "pattern-centre fits/s (spatial FFT search)", "value": 1.0 / secs, "unit": "fits/s", "n_gpus": 1,
         "steps": steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3 (FP32-class split)", "data": "synthetic",
         "config": {"workload": cfg["name"] + " (%d orientations)" % n_dict,
-                   "l2": "correlation tensors of 0.4 GB per chunk, larger than L2"},
+                   "l2": "spectra and maps stay on chip; the projected batch (25 MB) is L2-resident"},
         "gpu_launches": launches,
         "scores_per_s": evals / secs,
         "fit": {"pc": [float(v) for v in pc.cpu()], "simulated_pc": list(cfg["pc"])},
-        "chunk_stages_ms": stages,
-        "roofline": {"bound": "hbm", "kernel": "k_pcfit_reduce", "achieved": red_gbs, "peak": peaks["hbm_gbs"],
-                     "unit": "GB/s", "frac": red_gbs / peaks["hbm_gbs"], "traffic": None, "peak_source": src},
+        "fft_path": {"fits_per_s": 1.0 / fft_secs, "same_pc": bool(torch.equal(pc, pc_fft)),
+                     "same_orientations": bool(torch.equal(q, q_fft)),
+                     "how": "the same fits with cuFFT rfft2 / spectrum product / irfft2 + ebsd_pcfit_reduce"},
+        "batch_stages_ms": stages,
+        "roofline": {"bound": "tensor", "kernel": "k_xc_max (inverse DFTs + max over the batch)",
+                     "achieved": xc_tflops, "peak": peaks["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": xc_tflops / peaks["bf16_tflops"], "traffic": None,
+                     "peak_source": src + " bf16_tflops (burst; the kernel is timed alone)",
+                     "flops": "bf16 tensor FLOPs of the 3-term split, unpadded: 6 (4 WF H H2 + 2 H W WF) per pair"},
         "clocks": clocks.summary(),
     }
     if not args.no_cpu_baseline:

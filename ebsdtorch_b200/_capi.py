@@ -44,6 +44,7 @@ SIGNATURES = {
     "ebsd_merge_rescore_gated": (i32, [vp, vp, i64, i32, i32, vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, i32,
                                  vp, vp, vp, vp, f32, vp, vp]),
     "ebsd_gemm_nt": (i32, [vp, i64, vp, i64, i64, i32, f32, i32, vp, i64, i64, i64, i32, vp, vp]),
+    "ebsd_gemm_f32": (i32, [vp, i64, i64, vp, i64, i64, i64, f32, i32, vp, i64, i32, vp, vp]),
     "ebsd_col_mean": (i32, [vp, i64, i32, i64, vp, vp]),
     "ebsd_split3_bf16": (i32, [vp, i64, i32, i64, vp, i32, i32, vp, i64, i64, vp]),
     "ebsd_disori_angle": (i32, [vp, vp, i64, i32, vp, vp]),
@@ -60,6 +61,12 @@ SIGNATURES = {
     "ebsd_nlpar_workspace_bytes": (sz, [i32, i32]),
     "ebsd_pcfit_prep": (i32, [vp, i32, i32, i32, i32, i32, i32, i32, i32, vp, vp]),
     "ebsd_pcfit_reduce": (i32, [vp, i32, i32, i32, i32, i64, vp, vp, vp]),
+    "ebsd_pcfit_xcorr_table_bytes": (i64, [i32, i32]),
+    "ebsd_pcfit_xcorr_tables": (i32, [i32, i32, vp, i64, vp]),
+    "ebsd_pcfit_spectra": (i32, [vp, i64, i64, i32, i32, vp, vp, vp, vp]),
+    "ebsd_pcfit_pattern_terms": (i32, [vp, i64, i32, i32, vp, vp]),
+    "ebsd_pcfit_xcorr_max": (i32, [vp, i64, vp, i32, i32, i32, vp, vp, i64, vp, vp]),
+    "ebsd_pcfit_fold": (i32, [vp, i64, vp, vp, vp]),
     "ebsd_nlpar_weights": (i32, [vp, i32, i32, i32, vp, i32, f32, f32, f32, vp, sz, vp]),
     "ebsd_local_search": (i32, [vp, i64, i64, vp, i32, i32, vp, vp, vp, i64, vp, i32, i64, vp, vp, i32, i64, i32,
                                 i32, f32, i32, vp, vp, vp, vp]),
@@ -89,12 +96,13 @@ LAUNCHES_PER_CALL = {
     "ebsd_grid_fz_count": 2, "ebsd_grid_fz_write": 1, "ebsd_gather_rows": 1, "ebsd_project_dictionary": 1,
     "ebsd_prep_patterns": 1, "ebsd_prep_patterns_typed": 1, "ebsd_sample_master_pattern": 1, "ebsd_avg_pool": 1,
     "ebsd_match_topk": 1, "ebsd_match_topk_tiled": 1,
-    "ebsd_merge_rescore": 1, "ebsd_merge_rescore_gated": 1, "ebsd_manhattan_topk": 1, "ebsd_gemm_nt": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
+    "ebsd_merge_rescore": 1, "ebsd_merge_rescore_gated": 1, "ebsd_manhattan_topk": 1, "ebsd_gemm_nt": 1, "ebsd_gemm_f32": 1, "ebsd_col_mean": 1, "ebsd_split3_bf16": 1,
     "ebsd_disori_angle": 1, "ebsd_match_topk_noalloc": 2, "ebsd_zh_to_qu": 1, "ebsd_qu_to_zh": 1,
     "ebsd_cell_to_row": 2, "ebsd_local_search": 1, "ebsd_refine_grid": 1,
     "ebsd_pattern_mean": 2, "ebsd_subtract_pattern": 1, "ebsd_normalize_patterns": 1, "ebsd_clahe": 1,
     "ebsd_nlpar_dists": 1, "ebsd_nlpar_average": 1, "ebsd_nlpar_weights": 14,
-    "ebsd_pcfit_prep": 1, "ebsd_pcfit_reduce": 1,
+    "ebsd_pcfit_prep": 1, "ebsd_pcfit_reduce": 1, "ebsd_pcfit_xcorr_tables": 1, "ebsd_pcfit_spectra": 1,
+    "ebsd_pcfit_pattern_terms": 1, "ebsd_pcfit_xcorr_max": 1, "ebsd_pcfit_fold": 1,
     "ebsd_rot6d_sym_loss": 1, "ebsd_cnn_im2col": 1, "ebsd_cnn_col2im": 1, "ebsd_cnn_bias_act": 1,
     "ebsd_cnn_conv_fwd": 1, "ebsd_cnn_conv_c1": 1, "ebsd_cnn_relu_grad": 1, "ebsd_cnn_col_sum": 1,
     "ebsd_cnn_transpose": 1, "ebsd_cnn_scale_cast": 1,

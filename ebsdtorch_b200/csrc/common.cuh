@@ -23,6 +23,9 @@
 namespace ebsd {
 
 void set_error(const char* fmt, ...);
+// Limit of the bounded waits of the next tensor-core kernel launches
+// (ebsd_set_wait_limit_ns; kWaitLimitNs by default).
+uint64_t wait_limit_ns();
 
 #define EBSD_ARG_CHECK(cond, ...)              \
   do {                                         \
@@ -354,13 +357,19 @@ __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
 }
 
 // D[tmem] (+)= A[smem] * B[smem]^T, one instruction, issued by one thread.
-template <int KIND>  // 0: kind::f16 (bf16/f16 inputs), 1: kind::f8f6f4
+template <int KIND>  // 0: kind::f16 (bf16/f16 inputs), 1: kind::f8f6f4, 2: kind::tf32
 __device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                        uint32_t idesc, uint32_t accumulate) {
   if constexpr (KIND == 0) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+  } else if constexpr (KIND == 2) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
   } else {

@@ -78,12 +78,19 @@ struct GemmParams {
   uint64_t wait_ns;  // limit of every role's waits (kWaitLimitNs by default)
 };
 
+// Operand kinds: 0 kind::f16 with BF16, 1 kind::f8f6f4 with E4M3, 2 kind::tf32.
+template <int KIND>
+__host__ __device__ constexpr int kind_elem_bytes() {
+  return KIND == 0 ? 2 : KIND == 1 ? 1 : 4;
+}
+
 template <int KIND, int BN>
 __host__ __device__ constexpr uint32_t make_idesc() {
   // c_format F32 (bit 4); a/b format bits 7-9 / 10-12 (kind::f16: 1 = BF16;
-  // kind::f8f6f4: 0 = E4M3); K-major A and B; N >> 3 at bit 17; M >> 4 at bit 24.
-  return (1u << 4) | (KIND == 0 ? ((1u << 7) | (1u << 10)) : 0u) | ((uint32_t)(BN >> 3) << 17) |
-         ((uint32_t)(BM >> 4) << 24);
+  // kind::tf32: 2 = TF32; kind::f8f6f4: 0 = E4M3); K-major A and B; N >> 3 at
+  // bit 17; M >> 4 at bit 24.
+  return (1u << 4) | (KIND == 0 ? ((1u << 7) | (1u << 10)) : KIND == 2 ? ((2u << 7) | (2u << 10)) : 0u) |
+         ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
 template <int KC>
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
             const uint32_t a_dst = sbase + stage * STAGE_BYTES;
             mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
-            const int kx = k * (KIND == 0 ? BKB / 2 : BKB);  // element coordinate
+            const int kx = k * (BKB / kind_elem_bytes<KIND>());  // element coordinate
             tma_load_2d(a_dst, &tmA, kx, a_row, full_bar(stage));
             tma_load_2d(a_dst + A_BYTES, &tmB, kx, n * BN, full_bar(stage));
             ++issued;
@@ -463,7 +470,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 // Wait limit handed to every tensor-core kernel launch (0 = kWaitLimitNs).
 static std::atomic<uint64_t> g_wait_limit_ns{0};
 
-static uint64_t wait_limit_ns() {
+uint64_t wait_limit_ns() {
   const uint64_t v = g_wait_limit_ns.load(std::memory_order_relaxed);
   return v ? v : kWaitLimitNs;
 }
@@ -503,6 +510,30 @@ static int make_tmap(CUtensorMap* map, const void* ptr, int lp_dtype, int64_t ro
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed (CUresult %d) for rows=%lld k=%lld", (int)r,
               (long long)rows, (long long)k_pad);
+    return EBSD_ERR_ARG;
+  }
+  return 0;
+}
+
+// FP32 rows (ld floats apart) of `rows` x `k` valid elements, read as TF32
+// (the copy rounds each element to TF32); reads past either extent return
+// zeros, so the operands need no padding.
+static int make_tmap_f32(CUtensorMap* map, const float* ptr, int64_t ld, int64_t rows, int64_t k, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable from the CUDA driver");
+    return EBSD_ERR_UNSUPPORTED;
+  }
+  cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * 4)};
+  cuuint32_t box[2] = {(cuuint32_t)(BKB / 4), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32, 2, const_cast<float*>(ptr), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (CUresult %d) for FP32 rows=%lld k=%lld ld=%lld", (int)r,
+              (long long)rows, (long long)k, (long long)ld);
     return EBSD_ERR_ARG;
   }
   return 0;
@@ -583,8 +614,9 @@ extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad)
   // One wave: query tiles x dictionary ranges ~= number of SMs, so all units
   // start and finish together. Measured on B200 at 128^2 px x 328,720 rows:
   // one-wave shapes with 16-37 query tiles x 4-9 ranges run at ~1.26 PFLOP/s
-  // and ~1.3 GHz under the power cap; multi-wave or 1-range shapes that keep
-  // many more operand tiles in flight settle at 0.68-1.1 PFLOP/s.
+  // and ~1.3 GHz under the power cap (18 x 8 fastest: its query tiles stay
+  // in L2); multi-wave or 1-range shapes that keep many more operand tiles in
+  // flight settle at 0.68-1.1 PFLOP/s.
   const int64_t m_tiles = std::max<int64_t>(1, n_queries_pad / BM);
   const int64_t n_tiles = std::max<int64_t>(1, n_dict_pad / 256);
   const int64_t sms = device_sm_count();
@@ -686,6 +718,35 @@ extern "C" int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t
   cudaStream_t s = as_stream(stream);
   return lp_dtype == EBSD_DT_BF16 ? launch<0, 1, 1, 256>(ta, tb, p, p.units, s)
                                   : launch<1, 1, 1, 256>(ta, tb, p, p.units, s);
+}
+
+extern "C" int ebsd_gemm_f32(const float* A, int64_t lda, int64_t m, const float* B, int64_t ldb, int64_t n,
+                             int64_t k, float alpha, int accumulate, float* C, int64_t ldc, int splits, int* d_status,
+                             void* stream) {
+  EBSD_ARG_CHECK(A && B && C && d_status, "ebsd_gemm_f32: null pointer");
+  EBSD_ARG_CHECK(m > 0 && n > 0 && k > 0, "empty product");
+  EBSD_ARG_CHECK(lda >= k && ldb >= k && ldc >= n, "leading dimensions smaller than the extents");
+  EBSD_ARG_CHECK(lda % 4 == 0 && ldb % 4 == 0, "lda and ldb must be multiples of 4 floats (16-byte rows)");
+  EBSD_ARG_CHECK(((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0, "operands must be 16-byte aligned");
+  const int64_t m_tiles = (m + BM - 1) / BM, n_tiles = (n + 255) / 256;
+  EBSD_ARG_CHECK(m_tiles < (1 << 20) && n_tiles < (1 << 22), "operand too large");
+  CUtensorMap ta, tb;
+  if (int rc = make_tmap_f32(&ta, A, lda, m, k, BM)) return rc;
+  if (int rc = make_tmap_f32(&tb, B, ldb, n, k, 256)) return rc;
+  GemmParams p{};
+  p.n_tiles = (int)n_tiles;
+  p.splits = splits <= 0 ? p.n_tiles : std::min<int>(splits, p.n_tiles);
+  p.k_iters = (int)((k + BKB / 4 - 1) / (BKB / 4));
+  p.n_valid = n;
+  p.C = C;
+  p.ldc = ldc;
+  p.m_valid = m;
+  p.alpha = alpha;
+  p.accumulate = accumulate;
+  p.status = d_status;
+  EBSD_ARG_CHECK(m_tiles * p.splits < INT32_MAX, "too many work units");
+  p.units = (int)(m_tiles * p.splits);
+  return launch<2, 1, 1, 256>(ta, tb, p, p.units, as_stream(stream));
 }
 
 extern "C" int ebsd_cnn_conv_fwd(const void* w16, int64_t cout_pad, const void* cols, int64_t rows_pad,

@@ -6,13 +6,18 @@ each pc_z of linspace(pc_z_min, pc_z_max, pc_z_steps) the orientation
 dictionary is simulated on the detector enlarged by the pc_x / pc_y search
 range (`ebsd_project_dictionary`, the same projector as dictionary
 indexing) and circularly cross-correlated with every zero-padded
-experimental pattern by FFT, which scores all (pc_x, pc_y) shifts at once.
-The FFTs are cuFFT (torch.fft). One kernel then reduces each dictionary
-chunk (`ebsd_pcfit_reduce`): it applies the fftshift, takes the max and
-argmax over the chunk and folds them into the running best per (pc_z,
-pattern, shift). A second kernel prepares the patterns (`ebsd_pcfit_prep`):
-min-max, zero-mean and zero padding in one pass. The fit is the argmax
-of the mean over patterns; nothing synchronises with the host before it.
+experimental pattern, which scores all (pc_x, pc_y) shifts at once.
+Up to 127 x 127 enlarged pixels the correlation runs in the project's
+kernels: 2-D DFTs as tensor-core matrix products (`ebsd_pcfit_spectra`
+for the spectra, `ebsd_pcfit_xcorr_max` for the inverse transforms of the
+spectrum products fused with the max over the batch per (pattern, shift),
+`ebsd_pcfit_fold` for the running best per pc_z); no correlation map
+reaches memory. Larger detectors use cuFFT (torch.fft) and
+`ebsd_pcfit_reduce`, which applies the fftshift, takes the max and argmax
+over the chunk and folds them into the running best. A second kernel
+prepares the patterns (`ebsd_pcfit_prep`): min-max, zero-mean and zero
+padding in one pass. The fit is the argmax of the mean over patterns;
+nothing synchronises with the host before it.
 
 Differences, by design:
 
@@ -37,7 +42,7 @@ import torch
 from torch import Tensor
 
 from .. import kernels
-from .._capi import call, ptr
+from .._capi import call, load, ptr
 from ..kernels import RowBuffers
 from ..s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
 from .geometry import bruker_geometry_to_SE3
@@ -177,10 +182,8 @@ def spatial_fft_pc_fitter(
                                                             pc_y_min, pc_y_max, b)
     padded = torch.empty((B, hp, wp), dtype=torch.float32, device=dev)
     call("ebsd_pcfit_prep", ptr(x), B, hb, wb, hp, wp, pad[2], pad[0], 1, ptr(padded), stream)
-    pat_fft = torch.fft.rfft2(padded).conj()  # (B, hp, wp // 2 + 1)
 
     quats = sample_ori_fz_laue_angle(mp.laue_group, dictionary_resolution_deg, dev).float().contiguous()
-    n_dict = quats.shape[0]
     mp_t = _master_pattern_tensor(mp, b, dev)
     pix64 = pix.double().numpy()
     z_vals = torch.linspace(pc_z_min, pc_z_max, pc_z_steps)  # float32, as the reference's
@@ -188,21 +191,12 @@ def spatial_fft_pc_fitter(
     best_idx = torch.zeros((pc_z_steps, B, hp, wp), dtype=torch.int64, device=dev)
 
     bs = int(dictionary_indexing_batch_size)
-    wf = wp // 2 + 1
-    sub = max(1, min(bs, MAX_PRODUCT_BYTES // (B * hp * wf * 8)))
-    sims = torch.empty((min(sub, n_dict), hp * wp), dtype=torch.float32, device=dev)
-    for zi in range(pc_z_steps):
-        rays = _rays_soa(pix64, float(z_vals[zi]), float(primary_tilt_deg), float(secondary_tilt_deg), (H, W), dev)
-        for j in range(0, n_dict, bs):
-            j_end = min(j + bs, n_dict)
-            for s in range(j, j_end, sub):
-                n = min(sub, j_end - s)
-                kernels.project(mp_t, rays, quats[s:s + n], RowBuffers(f32=sims[:n]), subtract_mean=False)
-                spec = torch.fft.rfft2(sims[:n].view(n, hp, wp))
-                corr = torch.fft.irfft2(spec[:, None] * pat_fft[None], s=(hp, wp)).contiguous()
-                base = (s - j) if orientation_index == "reference" else s
-                call("ebsd_pcfit_reduce", ptr(corr), n, B, hp, wp, base, ptr(best[zi]), ptr(best_idx[zi]), stream)
-                del spec, corr
+    if xcorr_supported(hp, wp):
+        _search_dft(mp_t, padded, quats, pix64, z_vals, float(primary_tilt_deg), float(secondary_tilt_deg), (H, W),
+                    bs, orientation_index == "reference", best, best_idx, stream)
+    else:
+        _search_fft(mp_t, padded, quats, pix64, z_vals, float(primary_tilt_deg), float(secondary_tilt_deg), (H, W),
+                    bs, orientation_index == "reference", best, best_idx, stream)
 
     avg = best.mean(dim=1)
     zi, yi, xi = (int(v) for v in torch.unravel_index(avg.argmax(), avg.shape))
@@ -211,3 +205,75 @@ def spatial_fft_pc_fitter(
     best_pc = torch.tensor([pc_x, pc_y, float(z_vals[zi])], device=patterns.device)
     best_quats = quats[best_idx[zi, :, yi, xi]].to(patterns.device)
     return best_pc, best_quats
+
+
+def xcorr_supported(hp: int, wp: int) -> bool:
+    """Whether the enlarged detector fits the tensor-core correlation
+    kernels (2..127 rows and columns); larger ones use cuFFT."""
+    return int(load().ebsd_pcfit_xcorr_table_bytes(int(hp), int(wp))) > 0
+
+
+# sub-batch of the dictionary projected and transformed at once (the
+# correlation itself runs per dictionary batch on the spectra)
+MAX_SIM_BYTES = 2 << 30
+
+
+def _search_dft(mp_t, padded, quats, pix64, z_vals, tilt, sec_tilt, det, bs, batch_local, best, best_idx, stream):
+    """The search with the correlation in the project's kernels: spectra of
+    the patterns and of each projected dictionary sub-batch
+    (ebsd_pcfit_spectra), the per-batch max over all shifts
+    (ebsd_pcfit_xcorr_max) and the running best (ebsd_pcfit_fold)."""
+    dev = padded.device
+    B, hp, wp = padded.shape
+    n_dict = quats.shape[0]
+    spec_len = 4 * (hp // 2 + 1) * (wp // 2 + 1)
+    tables = torch.empty((int(load().ebsd_pcfit_xcorr_table_bytes(hp, wp)),), dtype=torch.uint8, device=dev)
+    call("ebsd_pcfit_xcorr_tables", hp, wp, ptr(tables), tables.numel(), stream)
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    pspec = torch.empty((B, spec_len), dtype=torch.float32, device=dev)
+    call("ebsd_pcfit_spectra", ptr(padded), hp * wp, B, hp, wp, ptr(tables), ptr(pspec), ptr(status), stream)
+    terms = torch.empty_like(pspec)
+    call("ebsd_pcfit_pattern_terms", ptr(pspec), B, hp, wp, ptr(terms), stream)
+    keys = torch.zeros((B * hp * wp,), dtype=torch.int64, device=dev)
+    sub = max(1, min(bs, n_dict, MAX_SIM_BYTES // (hp * wp * 4)))
+    sims = torch.empty((sub, hp * wp), dtype=torch.float32, device=dev)
+    spec = torch.empty((sub, spec_len), dtype=torch.float32, device=dev)
+    for zi in range(len(z_vals)):
+        rays = _rays_soa(pix64, float(z_vals[zi]), tilt, sec_tilt, det, dev)
+        for j in range(0, n_dict, bs):
+            j_end = min(j + bs, n_dict)
+            for s in range(j, j_end, sub):
+                n = min(sub, j_end - s)
+                kernels.project(mp_t, rays, quats[s:s + n], RowBuffers(f32=sims[:n]), subtract_mean=False)
+                call("ebsd_pcfit_spectra", ptr(sims), hp * wp, n, hp, wp, ptr(tables), ptr(spec), ptr(status), stream)
+                call("ebsd_pcfit_xcorr_max", ptr(spec), n, ptr(terms), B, hp, wp, ptr(tables), ptr(keys),
+                     (s - j) if batch_local else s, ptr(status), stream)
+            call("ebsd_pcfit_fold", ptr(keys), keys.numel(), ptr(best[zi]), ptr(best_idx[zi]), stream)
+    if int(status.item()) != 0:
+        raise RuntimeError("pattern-centre correlation kernels reported a device timeout")
+
+
+def _search_fft(mp_t, padded, quats, pix64, z_vals, tilt, sec_tilt, det, bs, batch_local, best, best_idx, stream):
+    """The search with cuFFT (torch.fft) for detectors beyond the
+    tensor-core kernels' 127 x 127: rfft2 of each chunk, spectrum product
+    with the patterns' conjugate spectra, irfft2, then the max over the
+    chunk (ebsd_pcfit_reduce)."""
+    dev = padded.device
+    B, hp, wp = padded.shape
+    n_dict = quats.shape[0]
+    pat_fft = torch.fft.rfft2(padded).conj()  # (B, hp, wp // 2 + 1)
+    wf = wp // 2 + 1
+    sub = max(1, min(bs, MAX_PRODUCT_BYTES // (B * hp * wf * 8)))
+    sims = torch.empty((min(sub, n_dict), hp * wp), dtype=torch.float32, device=dev)
+    for zi in range(len(z_vals)):
+        rays = _rays_soa(pix64, float(z_vals[zi]), tilt, sec_tilt, det, dev)
+        for j in range(0, n_dict, bs):
+            j_end = min(j + bs, n_dict)
+            for s in range(j, j_end, sub):
+                n = min(sub, j_end - s)
+                kernels.project(mp_t, rays, quats[s:s + n], RowBuffers(f32=sims[:n]), subtract_mean=False)
+                spec = torch.fft.rfft2(sims[:n].view(n, hp, wp))
+                corr = torch.fft.irfft2(spec[:, None] * pat_fft[None], s=(hp, wp)).contiguous()
+                base = (s - j) if batch_local else s
+                call("ebsd_pcfit_reduce", ptr(corr), n, B, hp, wp, base, ptr(best[zi]), ptr(best_idx[zi]), stream)
+                del spec, corr

@@ -239,6 +239,21 @@ def gemm_nt(A, B, out, alpha: float = 1.0, accumulate: bool = False, m_valid=Non
     return status
 
 
+def gemm_f32(A: torch.Tensor, B: torch.Tensor, out: torch.Tensor, alpha: float = 1.0, accumulate: bool = False,
+             status=None, splits: int = 0) -> torch.Tensor:
+    """out[:m, :n] = alpha * A @ B.T (+ out) from FP32 rows read as TF32
+    (ebsd_gemm_f32); A (m x k), B (n x k) with unit column stride."""
+    _cuda(A, "A", torch.float32, contiguous=False)
+    _cuda(B, "B", torch.float32, contiguous=False)
+    if A.stride(1) != 1 or B.stride(1) != 1 or out.stride(1) != 1:
+        raise ValueError("gemm_f32 needs rows with unit column stride")
+    if status is None:
+        status = torch.zeros(1, dtype=torch.int32, device=A.device)
+    call("ebsd_gemm_f32", ptr(A), A.stride(0), A.shape[0], ptr(B), B.stride(0), B.shape[0], A.shape[1],
+         float(alpha), int(bool(accumulate)), ptr(out), out.stride(0), int(splits), ptr(status), _stream(A.device))
+    return status
+
+
 def col_mean(X: torch.Tensor) -> torch.Tensor:
     _cuda(X, "X", torch.float32, contiguous=False)
     out = torch.empty(X.shape[1], dtype=torch.float32, device=X.device)

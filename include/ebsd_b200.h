@@ -310,6 +310,14 @@ int ebsd_gemm_nt(const void* A, int64_t m_pad, const void* B, int64_t n_pad, int
                  int lp_dtype, float alpha, int accumulate, float* C, int64_t ldc, int64_t m_valid,
                  int64_t n_valid, int splits, int* d_status, void* stream);
 
+/* C (m x n, row stride ldc) = alpha * A B^T (+ C if accumulate) from FP32
+ * rows A (m x k, stride lda) and B (n x k, stride ldb), read as TF32
+ * (rounded on the copy) by the same tcgen05 kernel (kind::tf32); no padding
+ * needed (lda, ldb multiples of 4, 16-byte aligned operands). The PCA
+ * projections (indexing.py:401, 421, 452). splits as for ebsd_gemm_nt. */
+int ebsd_gemm_f32(const float* A, int64_t lda, int64_t m, const float* B, int64_t ldb, int64_t n, int64_t k,
+                  float alpha, int accumulate, float* C, int64_t ldc, int splits, int* d_status, void* stream);
+
 /* Column means of an (n_rows x n_cols) fp32 matrix (row stride ld). */
 int ebsd_col_mean(const float* X, int64_t n_rows, int n_cols, int64_t ld, float* mean, void* stream);
 
@@ -423,6 +431,42 @@ int ebsd_pcfit_prep(const float* patterns, int n, int height, int width, int pad
                     int pad_left, int zero_mean, float* out, void* stream);
 int ebsd_pcfit_reduce(const float* corr, int n, int n_patterns, int padded_h, int padded_w, int64_t index_base,
                       float* best, int64_t* best_index, void* stream);
+
+/* The cross-correlation itself without an FFT library (replaces
+ * fitting.py:413 rfft2 and fitting.py:484-485 irfft2(sim_fft * pattern_fft)
+ * plus the max over the batch, fitting.py:493-507), for enlarged detectors
+ * of 2..127 rows and columns; larger ones return EBSD_ERR_ARG (and
+ * ebsd_pcfit_xcorr_table_bytes returns 0).
+ * Spectra hold 4 * (padded_h / 2 + 1) * (padded_w / 2 + 1) floats per image:
+ * [trig][part][ky][kx] with Cc = sum_y T cos(2 pi ky y / H), Ss = sum_y T sin(.)
+ * of the row transform T (S[ky] = Cc - i Ss, S[H - ky] = Cc + i Ss).
+ * ebsd_pcfit_xcorr_tables: DFT matrices (hi / lo bf16 halves, in the
+ *   shared-memory layout the kernels copy) into `tables` (16-byte aligned,
+ *   ebsd_pcfit_xcorr_table_bytes bytes), once per detector size.
+ * ebsd_pcfit_spectra: spectra of n images (rows of padded_h x padded_w
+ *   floats, `ld` floats apart).
+ * ebsd_pcfit_pattern_terms: the terms of the experimental patterns' conjugate
+ *   spectra that the correlation uses, from their spectra (same layout).
+ * ebsd_pcfit_xcorr_max: for every (pattern, shift), the maximum over the
+ *   n_sims simulated patterns (their spectra) of the circular
+ *   cross-correlation, read through fftshift, and its index (index_base +
+ *   entry; the first maximum wins), merged into keys (n_patterns x padded_h
+ *   x padded_w uint64, zero before a batch) by atomicMax. Tensor-core DFTs
+ *   in a 3-term bf16 split (about 3e-5 of the maps' RMS). Bounded waits:
+ *   EBSD_DEVICE_TIMEOUT in *status.
+ * ebsd_pcfit_fold: folds a batch's keys into the running best of one pc_z
+ *   (best = max(best, batch max); best_index replaced where they are equal)
+ *   and clears the keys. */
+int64_t ebsd_pcfit_xcorr_table_bytes(int padded_h, int padded_w);
+int ebsd_pcfit_xcorr_tables(int padded_h, int padded_w, void* tables, int64_t bytes, void* stream);
+int ebsd_pcfit_spectra(const float* images, int64_t ld, int64_t n, int padded_h, int padded_w, const void* tables,
+                       float* spectra, int* status, void* stream);
+int ebsd_pcfit_pattern_terms(const float* spectra, int64_t n, int padded_h, int padded_w, float* terms,
+                             void* stream);
+int ebsd_pcfit_xcorr_max(const float* sim_spectra, int64_t n_sims, const float* pattern_terms, int n_patterns,
+                         int padded_h, int padded_w, const void* tables, unsigned long long* keys,
+                         int64_t index_base, int* status, void* stream);
+int ebsd_pcfit_fold(unsigned long long* keys, int64_t n, float* best, int64_t* best_index, void* stream);
 
 /* ---- local dictionary search around orientation proposals --------------------
  * No counterpart in the reference (search step of the learned-proposal path).

@@ -97,6 +97,34 @@ def test_preprocessing_and_fitting_argument_errors_need_no_gpu():
         _capi.call("ebsd_pcfit_reduce", fake, 0, 4, 8, 8, 0, fake, fake, None)
 
 
+def test_pcfit_correlation_kernels_size_limits_need_no_gpu():
+    """The tensor-core correlation kernels take enlarged detectors of 2..127
+    rows and columns; the table size query says which, and every entry point
+    rejects other sizes and bad arguments on the host."""
+    import pytest
+
+    lib = _capi.load()
+    assert lib.ebsd_pcfit_xcorr_table_bytes(78, 78) == 163840
+    assert lib.ebsd_pcfit_xcorr_table_bytes(127, 127) > 0
+    for h, w in ((128, 78), (78, 128), (1, 40), (40, 1), (0, 0)):
+        assert lib.ebsd_pcfit_xcorr_table_bytes(h, w) == 0
+    fake = 256  # never dereferenced
+    with pytest.raises(ValueError, match="not supported"):
+        _capi.call("ebsd_pcfit_xcorr_tables", 128, 60, fake, 1 << 20, None)
+    with pytest.raises(ValueError, match="needed"):
+        _capi.call("ebsd_pcfit_xcorr_tables", 78, 78, fake, 1024, None)
+    with pytest.raises(ValueError, match="16-byte aligned"):
+        _capi.call("ebsd_pcfit_xcorr_tables", 78, 78, fake + 4, 1 << 20, None)
+    with pytest.raises(ValueError, match="not supported"):
+        _capi.call("ebsd_pcfit_spectra", fake, 78 * 78, 4, 200, 78, fake, fake, fake, None)
+    with pytest.raises(ValueError, match="leading dimension"):
+        _capi.call("ebsd_pcfit_spectra", fake, 78, 4, 78, 78, fake, fake, fake, None)
+    with pytest.raises(ValueError, match="32 bits"):
+        _capi.call("ebsd_pcfit_xcorr_max", fake, 16, fake, 2, 78, 78, fake, fake, (1 << 32) - 4, fake, None)
+    with pytest.raises(ValueError, match="null pointer"):
+        _capi.call("ebsd_pcfit_fold", None, 10, fake, fake, None)
+
+
 def test_noalloc_argument_checks_need_no_gpu():
     """ebsd_match_topk_noalloc rejects bad arguments on the host, before any
     CUDA call: k_out outside 1..64, more queries than padded rows, null
