@@ -317,12 +317,13 @@ def plain_fp32_gpu_di(wl, mp, rays, dictionary, queries_f32, k, chunk=8192, retu
     return torch.gather(best_i, 1, order), t_proj, t_match
 
 
-# DRAM bytes (read + write) of one one-wave match launch (4,736 queries
-# against the whole dictionary, bf16 rows of 128^2 px), captured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) at two dictionary sizes. The
-# traffic is affine in the dictionary rows; the full launch's figure is its
-# extrapolation.
-MATCH_DRAM_BYTES = ((36829, 6738486528 + 6209024), (89312, 16461514240 + 7201792))
+# DRAM bytes (read + write) of one one-wave match launch (18 query tiles,
+# 2,304 queries, against the whole dictionary, bf16 rows of 128^2 px),
+# captured with ncu (dram__bytes_read.sum + dram__bytes_write.sum) at two
+# dictionary sizes. The traffic is affine in the dictionary rows; the full
+# launch's figure is its extrapolation.
+MATCH_DRAM_BYTES = ((36829, 2549037056 + 3763456), (89312, 6199060224 + 5258240))
+MATCH_WAVE_QUERIES = 2304
 
 
 def match_traffic_estimate(d_rows: int) -> float:
@@ -714,8 +715,10 @@ def run_ours(args, wl):
         "roofline": {"bound": "tensor", "achieved": achieved_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved_tflops / peak, "traffic": traffic,
                      "traffic_source": ("ncu DRAM bytes of one-wave launches at 36,829 and 89,312 dictionary rows, "
-                                        "extrapolated (affine in the rows) to %d rows; per one-wave launch of 4,736 "
-                                        "queries" % n_dict_rows) if traffic is not None else None,
+                                        "extrapolated (affine in the rows) to %d rows; per one-wave launch of %d "
+                                        "queries" % (n_dict_rows, MATCH_WAVE_QUERIES)) if traffic is not None else None,
+                     "algorithmic_bytes": ((n_dict_rows + MATCH_WAVE_QUERIES) * 128 * 128 * 2
+                                           if traffic is not None else None),
                      "kernel": "k_tc_gemm (match + streaming top-k)",
                      "peak_source": f"{peak_kind} bf16_tflops_sustained" + (" x2 for fp8" if args.precision == "fp8"
                                                                              else ""),
@@ -1398,8 +1401,8 @@ def pca_block(args, wl, mp, geom, truth, pats, dev, learn_res: float = 0.9) -> d
         "dtype": "bf16", "data": "synthetic",
         "config": {"workload": f"PCA DI 128x128 px, {n_comp} components fitted on the m-3m {learn_res} deg dictionary "
                                f"({fit['learn_rows']:,}), indexing {D:,} rows, {wl['Q']:,} patterns, top-{wl['k']}",
-                   "precision": "PCA projections FP32-class (3-term bf16 split on tcgen05); bf16 match + FP32 "
-                                "re-score of top-32 in PCA space",
+                   "precision": "PCA projections TF32 on tcgen05 (kind::tf32, FP32 accumulation); bf16 match + "
+                                "FP32 re-score of top-32 in PCA space",
                    "l2": "inputs larger than L2"},
         "e2e": e2e,
         "gpu_launches": int(launches * args.steps),
@@ -1408,9 +1411,9 @@ def pca_block(args, wl, mp, geom, truth, pats, dev, learn_res: float = 0.9) -> d
                      "peak_source": f"{peak_kind} bf16_tflops_sustained",
                      "share_of_step": sum(match_ms) / 1e3 / t},
         "projection": {"share_of_step": sum(proj_ms) / 1e3 / t,
-                       "tflops_fp32_equivalent": sum(proj_fl) / (sum(proj_ms) / 1e3) / 1e12,
+                       "tflops": sum(proj_fl) / (sum(proj_ms) / 1e3) / 1e12,
                        "max_rel_error_vs_fp64": proj_err,
-                       "how": "3-term bf16 split (x = hi + lo) of rows and components, one tcgen05 GEMM over 3K"},
+                       "how": "TF32 tcgen05 GEMM (kind::tf32, ebsd_gemm_f32) straight from the FP32 rows"},
         "algorithmic_flops_per_pattern": {"match_2DK": 2.0 * D * n_comp, "query_projection_2PK": 2.0 * P * n_comp,
                                           "dictionary_projection_amortised": 2.0 * D * P * n_comp / wl["Q"]},
         "fit_one_time": fit,
