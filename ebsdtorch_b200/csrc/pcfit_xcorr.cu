@@ -112,21 +112,50 @@ __host__ __device__ inline uint32_t op_offset(int rows, int row, int k) {
 // Bytes of one constant matrix image (hi or lo) of `rows` rows, `planes` planes.
 __host__ __device__ constexpr int mat_bytes(int rows, int planes) { return rows * 128 * planes; }
 
-// Table layout: inverse [A hi | A lo | B hi | B lo], then forward
-// [F1 hi | F1 lo | F2 hi | F2 lo].
+// The constant matrices, each stored as two images (hi and lo halves of the
+// bf16 split, or for the mixed stage-B matrix of the TMEM kernel the
+// [hi | hi] and [lo | 0] images described at k_xc_max_tm):
+//   0 inverse stage A        rows y (NA), K [cos | sin] over ky
+//   1 inverse stage B        rows x (NB), K [a cos | -a sin] / (H W) over kx
+//   2 forward F1             rows (re/im, kx) (N1), K x
+//   3 forward F2             rows (cos/sin, ky) (N2), K y
+//   4 inverse stage A (TMEM) matrix 0 with 128 rows (the MMA's A operand)
+//   5 inverse stage B (TMEM) rows x (NB), K' = 2 * RW: per 8 K elements of
+//     matrix 1, 16 K' elements
+// Matrices are stored one after the other; kernels copy a contiguous run.
+constexpr int N_MATS = 6;
 struct Tables {
-  int inv_a, inv_b, fwd_1, fwd_2;  // bytes of one hi (or lo) image
-  int inv_bytes, fwd_bytes;
+  int rows[N_MATS], planes[N_MATS];
+  int img[N_MATS];  // bytes of one image
+  int off[N_MATS];  // byte offset of the matrix's first image
+  int total;
+  // contiguous runs per kernel: inverse (0, 1), forward (2, 3), TMEM inverse (4, 5)
+  int inv_bytes, fwd_bytes, tm_bytes;
+  int inv_a, inv_b, fwd_1, fwd_2, tm_a, tm_b;  // image bytes, for the kernels' layouts
 };
 
 __host__ __device__ inline Tables table_sizes(const Geo& g) {
   Tables t{};
-  t.inv_a = mat_bytes(g.NA, g.KPA);
-  t.inv_b = mat_bytes(g.NB, g.KPB);
-  t.fwd_1 = mat_bytes(g.N1, g.KP1);
-  t.fwd_2 = mat_bytes(g.N2, g.KP2);
-  t.inv_bytes = 2 * (t.inv_a + t.inv_b);
-  t.fwd_bytes = 2 * (t.fwd_1 + t.fwd_2);
+  const int rows[N_MATS] = {g.NA, g.NB, g.N1, g.N2, 128, g.NB};
+  const int planes[N_MATS] = {g.KPA, g.KPB, g.KP1, g.KP2, g.KPA, cdiv(2 * g.RW, 64)};
+  int off = 0;
+  for (int m = 0; m < N_MATS; ++m) {
+    t.rows[m] = rows[m];
+    t.planes[m] = planes[m];
+    t.img[m] = mat_bytes(rows[m], planes[m]);
+    t.off[m] = off;
+    off += 2 * t.img[m];
+  }
+  t.total = off;
+  t.inv_bytes = 2 * (t.img[0] + t.img[1]);
+  t.fwd_bytes = 2 * (t.img[2] + t.img[3]);
+  t.tm_bytes = 2 * (t.img[4] + t.img[5]);
+  t.inv_a = t.img[0];
+  t.inv_b = t.img[1];
+  t.fwd_1 = t.img[2];
+  t.fwd_2 = t.img[3];
+  t.tm_a = t.img[4];
+  t.tm_b = t.img[5];
   return t;
 }
 
@@ -157,66 +186,69 @@ __device__ inline void split_bf16(double v, __nv_bfloat16& hi, __nv_bfloat16& lo
   lo = __float2bfloat16_rn((float)(v - (double)__bfloat162float(hi)));
 }
 
-// One thread per (matrix, row, k) element of the four constant matrices.
+// Entry (row, k) of the inverse transforms: stage A (y, [cos | sin] over ky)
+// and stage B (x, [a cos | -a sin] / (H W) over kx).
+__device__ inline double inv_a_value(const Geo& g, int y, int k) {
+  const int part = k >= g.KOA, ky = k - part * g.KOA;
+  if (y >= g.H || ky >= g.H2) return 0.0;
+  double c, s;
+  cos_sin_turn((int64_t)ky * (y - g.H / 2), g.H, c, s);
+  return part ? s : c;
+}
+
+__device__ inline double inv_b_value(const Geo& g, int x, int k) {
+  const int part = k >= g.KOB, kx = k - part * g.KOB;
+  if (x >= g.W || kx >= g.WF || part > 1) return 0.0;
+  double c, s;
+  cos_sin_turn((int64_t)kx * (x - g.W / 2), g.W, c, s);
+  const double a = (kx == 0 || 2 * kx == g.W) ? 1.0 : 2.0;
+  return a * (part ? -s : c) / ((double)g.H * (double)g.W);
+}
+
+// One thread per (matrix, row, k) element; writes both images.
 __global__ void k_xc_tables(Geo g, Tables t, uint8_t* __restrict__ out) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t nA = (int64_t)g.NA * 64 * g.KPA, nB = (int64_t)g.NB * 64 * g.KPB;
-  const int64_t n1 = (int64_t)g.N1 * 64 * g.KP1, n2 = (int64_t)g.N2 * 64 * g.KP2;
-  int64_t r = e;
-  int which;
-  int rows, planes;
-  if (r < nA) {
-    which = 0, rows = g.NA, planes = g.KPA;
-  } else if ((r -= nA) < nB) {
-    which = 1, rows = g.NB, planes = g.KPB;
-  } else if ((r -= nB) < n1) {
-    which = 2, rows = g.N1, planes = g.KP1;
-  } else if ((r -= n1) < n2) {
-    which = 3, rows = g.N2, planes = g.KP2;
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int m = 0;
+  for (; m < N_MATS; ++m) {
+    const int64_t n = (int64_t)t.rows[m] * 64 * t.planes[m];
+    if (r < n) break;
+    r -= n;
+  }
+  if (m == N_MATS) return;
+  const int width = 64 * t.planes[m];
+  const int row = (int)(r / width), k = (int)(r % width);
+  __nv_bfloat16 v0, v1;
+  if (m == 5) {
+    // K' = 16 q + 8 half + j holds K = 8 q + j: image 0 [hi | hi], image 1 [lo | 0]
+    const int q = k / 16, half = (k / 8) & 1, j = k & 7, kk = 8 * q + j;
+    __nv_bfloat16 hi, lo;
+    split_bf16(kk < g.RW ? inv_b_value(g, row, kk) : 0.0, hi, lo);
+    v0 = hi;
+    v1 = half ? __float2bfloat16_rn(0.0f) : lo;
   } else {
-    return;
+    double v = 0.0, c, s;
+    if (m == 0 || m == 4) {
+      v = inv_a_value(g, row, k);
+    } else if (m == 1) {
+      v = inv_b_value(g, row, k);
+    } else if (m == 2) {  // forward F1: rows (part, kx), K = x: cos / -sin
+      const int part = row >= g.KOB, kx = row - part * g.KOB, x = k;
+      if (kx < g.WF && x < g.W) {
+        cos_sin_turn((int64_t)kx * x, g.W, c, s);
+        v = part ? -s : c;
+      }
+    } else {  // forward F2: rows (trig, ky), K = y: cos / sin
+      const int trig = row >= g.KOA, ky = row - trig * g.KOA, y = k;
+      if (ky < g.H2 && y < g.H) {
+        cos_sin_turn((int64_t)ky * y, g.H, c, s);
+        v = trig ? s : c;
+      }
+    }
+    split_bf16(v, v0, v1);
   }
-  (void)planes;
-  const int row = (int)(r / (64 * planes)), k = (int)(r % (64 * planes));
-  double v = 0.0, c, s;
-  if (which == 0) {  // inverse A: rows y, K = [cos | sin] over ky, y' = y - H/2
-    const int y = row;
-    const int part = k >= g.KOA, ky = k - part * g.KOA;
-    if (y < g.H && ky < g.H2) {
-      cos_sin_turn((int64_t)ky * (y - g.H / 2), g.H, c, s);
-      v = part ? s : c;
-    }
-  } else if (which == 1) {  // inverse B: rows x, K = [a cos | -a sin] / (H W) over kx
-    const int x = row;
-    const int part = k >= g.KOB, kx = k - part * g.KOB;
-    if (x < g.W && kx < g.WF) {
-      cos_sin_turn((int64_t)kx * (x - g.W / 2), g.W, c, s);
-      const double a = (kx == 0 || 2 * kx == g.W) ? 1.0 : 2.0;
-      v = a * (part ? -s : c) / ((double)g.H * (double)g.W);
-    }
-  } else if (which == 2) {  // forward F1: rows (part, kx), K = x: cos / -sin
-    const int part = row >= g.KOB, kx = row - part * g.KOB, x = k;
-    if (kx < g.WF && x < g.W) {
-      cos_sin_turn((int64_t)kx * x, g.W, c, s);
-      v = part ? -s : c;
-    }
-  } else {  // forward F2: rows (trig, ky), K = y: cos / sin
-    const int trig = row >= g.KOA, ky = row - trig * g.KOA, y = k;
-    if (ky < g.H2 && y < g.H) {
-      cos_sin_turn((int64_t)ky * y, g.H, c, s);
-      v = trig ? s : c;
-    }
-  }
-  __nv_bfloat16 hi, lo;
-  split_bf16(v, hi, lo);
-  const int img = which == 0 ? t.inv_a : which == 1 ? t.inv_b : which == 2 ? t.fwd_1 : t.fwd_2;
-  const int64_t base = which == 0 ? 0
-                       : which == 1 ? 2 * (int64_t)t.inv_a
-                       : which == 2 ? (int64_t)t.inv_bytes
-                                    : (int64_t)t.inv_bytes + 2 * (int64_t)t.fwd_1;
-  const uint32_t off = op_offset(rows, row, k);
-  *reinterpret_cast<__nv_bfloat16*>(out + base + off) = hi;
-  *reinterpret_cast<__nv_bfloat16*>(out + base + img + off) = lo;
+  const uint32_t o = op_offset(t.rows[m], row, k);
+  *reinterpret_cast<__nv_bfloat16*>(out + t.off[m] + o) = v0;
+  *reinterpret_cast<__nv_bfloat16*>(out + t.off[m] + t.img[m] + o) = v1;
 }
 
 // ---------------------------------------------------------------------------
@@ -292,6 +324,28 @@ __device__ __forceinline__ void issue_stage(uint32_t d_tmem, int n, int n_tiles,
   }
 }
 
+// D[tmem] (+)= A[tmem] * B[smem]^T (kind::f16, BF16 A packed two per TMEM
+// column, the even K element in the low half), issued by one thread.
+__device__ __forceinline__ void tc_mma_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit columns into TMEM (lane i of the warp
+// writes row lane base + i).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+      "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 struct XcParams {
   Geo g;
   int mt;          // 128-row tiles per pass (1 or 2)
@@ -312,6 +366,7 @@ struct XcParams {
   const float* pat_terms;
   int n_pats;
   int slices;
+  int pp_tm;  // TMEM kernel: pairs per pass
   int64_t index_base;
   unsigned long long* keys;
   int* status;
@@ -651,6 +706,166 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max(const XcParams p) {
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
+// k_xc_max_tm: k_xc_max with stage A's output kept in TMEM as stage B's A
+// operand (no shared-memory transpose, no staged maps):
+//   stage A  D_A[y, (pair, part, kx)] = CA[y, K] . Data[(pair, part, kx), K]^T
+//            with the constant (128 rows y) as the A operand and the pass's
+//            [E | O] rows as B (N = pairs * RW);
+//   convert  each thread rewrites its own 8-column chunks of D_A in place as
+//            [hi x 8 | lo x 8] bf16, 8 columns = 16 K' elements;
+//   stage B  D_B[y, (pair, x)] = sum over chunks q of A'(q) . P(q)^T +
+//            A'(q) . Q(q)^T, with P = [Bhi | Bhi] and Q = [Blo | 0] over the
+//            chunk's 8 K elements: hi Bhi + lo Bhi + hi Blo, the 3-term split;
+//   epilogue each thread owns lane y and CPT x chunks; the max over the
+//            pass's pairs and over passes stays in its registers.
+template <int CPT>  // x chunks of 8 per thread: NB / 8 <= 4 CPT
+__global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_s = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
+  const Geo& g = p.g;
+  const Smem s = carve(base, p, p.tb.tm_a, p.tb.tm_b);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int lg = warp & 3, cg = warp >> 2;
+  const int b = blockIdx.x / p.slices, sl = blockIdx.x - b * p.slices;
+  const int64_t s_begin = p.n_sims * sl / p.slices, s_end = p.n_sims * (sl + 1) / p.slices;
+
+  load_constants(s, p.tables + p.tb.off[4], p.tb.tm_bytes, p);
+  if (tid == 0) {
+    mbar_init(smem_u32(s.bar), 1);
+    *s.flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(smem_u32(s.tmem_slot), 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s.tmem_slot;
+  const uint32_t da = tmem, db = tmem + 256u;
+  const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
+  const uint32_t d_hi = smem_u32(s.a_hi), d_lo = smem_u32(s.a_lo);
+  const uint32_t ca_hi = smem_u32(s.c0), ca_lo = ca_hi + p.tb.tm_a;
+  const uint32_t cp = smem_u32(s.c1), cq = cp + p.tb.tm_b;
+  const int ng = g.KOA / 8, hwf = g.H2 * g.WF, nb8 = g.NB / 8, rw8 = g.RW / 8;
+  const float* pt = p.pat_terms + (int64_t)b * g.spec;
+  const int y = lg * 32 + lane;
+
+  float best_v[CPT][8];
+  int best_i[CPT][8];
+#pragma unroll
+  for (int j = 0; j < CPT; ++j)
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      best_v[j][i] = -INFINITY;
+      best_i[j][i] = -1;
+    }
+  uint32_t phase = 0;
+
+  for (int64_t s0 = s_begin; s0 < s_end; s0 += p.pp_tm) {
+    const int np = (int)(s_end - s0 < p.pp_tm ? s_end - s0 : p.pp_tm);
+    // stage A's B operand: rows (pair, part, kx), K = [E part | O part] over ky
+    for (int it = tid; it < np * g.WF * ng; it += THREADS) {
+      const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng, grp = rem / g.WF, kx = rem - grp * g.WF;
+      const float* cs = p.sim_spec + (s0 + pr) * (int64_t)g.spec + kx;
+      float er[8], ei[8], orr[8], noi[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int ky = grp * 8 + j;
+        er[j] = ei[j] = orr[j] = noi[j] = 0.0f;
+        if (ky < g.H2) {
+          const int o = ky * g.WF;
+          const float a = __ldg(cs + o), bi = __ldg(cs + hwf + o);                // Cc
+          const float c = __ldg(cs + 2 * hwf + o), d = __ldg(cs + 3 * hwf + o);   // Ss
+          const float e = __ldg(pt + o + kx), f = __ldg(pt + hwf + o + kx);       // Pe
+          const float gg = __ldg(pt + 2 * hwf + o + kx), h = __ldg(pt + 3 * hwf + o + kx);  // Po
+          er[j] = a * e - bi * f + c * h + d * gg;
+          ei[j] = a * f + bi * e - c * gg + d * h;
+          orr[j] = a * gg - bi * h + c * f + d * e;
+          noi[j] = -(a * h + bi * gg - c * e + d * f);
+        }
+      }
+      const int row_re = pr * g.RW + kx, row_im = row_re + g.KOB;
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_re, grp * 8, er);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_re, g.KOA + grp * 8, noi);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_im, grp * 8, ei);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_im, g.KOA + grp * 8, orr);
+    }
+    if (!run_stage(s, p, phase, [&] {
+          const int n = np * g.RW;
+          const uint32_t idesc = xc_idesc(n);
+          for (int ks = 0; ks < g.KSA; ++ks) {
+            const uint32_t aoff = (uint32_t)(ks >> 2) * 128u * 128u + (uint32_t)(ks & 3) * 32u;
+            const uint32_t boff = (uint32_t)(ks >> 2) * (uint32_t)p.buf_rows * 128u + (uint32_t)(ks & 3) * 32u;
+            tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_hi + boff), idesc, ks > 0 ? 1u : 0u);
+            tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_lo + boff), idesc, 1u);
+            tc_mma<0>(da, smem_desc_sw128(ca_lo + aoff), smem_desc_sw128(d_hi + boff), idesc, 1u);
+          }
+        }))
+      break;
+    // D_A chunks -> [hi | lo] bf16 in place (this thread's lanes and columns only)
+    for (int c8 = cg; c8 < np * rw8; c8 += 4) {
+      float v[8];
+      tmem_ld8(da + lane_off + (uint32_t)(c8 * 8), v);
+      uint32_t w[8];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * j]), h1 = __float2bfloat16_rn(v[2 * j + 1]);
+        w[j] = pack_bf16(h0, h1);
+        w[4 + j] = pack_bf16(__float2bfloat16_rn(v[2 * j] - __bfloat162float(h0)),
+                             __float2bfloat16_rn(v[2 * j + 1] - __bfloat162float(h1)));
+      }
+      tmem_st8(da + lane_off + (uint32_t)(c8 * 8), w);
+    }
+    tmem_wait_st();
+    if (!run_stage(s, p, phase, [&] {
+          const uint32_t idesc = xc_idesc(g.NB);
+          for (int pr = 0; pr < np; ++pr) {
+            for (int q = 0; q < rw8; ++q) {
+              const uint32_t boff = (uint32_t)((16 * q) >> 6) * (uint32_t)g.NB * 128u + (uint32_t)(q & 3) * 32u;
+              const uint32_t a = da + (uint32_t)(pr * g.RW + 8 * q);
+              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cp + boff), idesc, q > 0 ? 1u : 0u);
+              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cq + boff), idesc, 1u);
+            }
+          }
+        }))
+      break;
+    // maps: lane y, columns (pair, x); max over the pairs, then the running max
+    for (int pr = 0; pr < np; ++pr) {
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        const int c8 = cg + 4 * j;
+        if (c8 < nb8) {
+          float v[8];
+          tmem_ld8(db + lane_off + (uint32_t)(pr * g.NB + c8 * 8), v);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            if (v[i] > best_v[j][i]) {
+              best_v[j][i] = v[i];
+              best_i[j][i] = (int)(s0 + pr);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (*s.flag == 0 && y < g.H) {
+    unsigned long long* keys = p.keys + ((int64_t)b * g.H + y) * g.W;
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int x = (cg + 4 * j) * 8 + i;
+        if (x < g.W && best_i[j][i] >= 0)
+          atomicMax(keys + x, max_key(best_v[j][i], (uint32_t)(p.index_base + best_i[j][i])));
+      }
+    }
+  }
+  drain(s, phase ^ 1u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
 // Running best of one pc_z (fitting.py:498-507) from a batch's keys:
 // best = max(best, batch max); index replaced where best == batch max; the
 // keys are cleared for the next batch.
@@ -704,6 +919,7 @@ struct Plan {
   Geo g;
   Tables tb;
   int mt, pp, buf_rows, buf_planes, buf_bytes, smem_fwd, smem_inv, pos;
+  int pp_tm, smem_tm, cpt;  // TMEM kernel (pp_tm 0: the detector does not fit it)
 };
 
 bool make_plan(int hp, int wp, Plan& pl) {
@@ -729,6 +945,18 @@ bool make_plan(int hp, int wp, Plan& pl) {
   if (pl.mt == 0) return false;
   const int pos = cdiv(hp * wp, THREADS);
   pl.pos = pos <= 8 ? 8 : pos <= 16 ? 16 : 32;
+  // TMEM kernel: pairs per pass limited by N <= 256 for both stages, the
+  // 256 + 256 TMEM columns and shared memory
+  pl.pp_tm = 0;
+  for (int pp = std::min(256 / g.RW, 256 / g.NB); pp >= 1; --pp) {
+    const int bytes = smem_bytes(pp * g.RW * 128 * g.KPA, pl.tb.tm_a, pl.tb.tm_b);
+    if (bytes <= SMEM_LIMIT) {
+      pl.pp_tm = pp;
+      pl.smem_tm = std::max(bytes, SMEM_ONE_CTA);
+      break;
+    }
+  }
+  pl.cpt = cdiv(g.NB / 8, 4);
   // every CTA allocates all 512 TMEM columns: ask for enough shared memory
   // that no second CTA fits on the SM
   pl.smem_inv = std::max(pl.smem_inv, SMEM_ONE_CTA);
@@ -763,7 +991,7 @@ XcParams base_params(const Plan& pl, const void* tables, int* status) {
 extern "C" int64_t ebsd_pcfit_xcorr_table_bytes(int hp, int wp) {
   Plan pl;
   if (!make_plan(hp, wp, pl)) return 0;
-  return (int64_t)pl.tb.inv_bytes + pl.tb.fwd_bytes;
+  return pl.tb.total;
 }
 
 extern "C" int ebsd_pcfit_xcorr_tables(int hp, int wp, void* tables, int64_t bytes, void* stream) {
@@ -771,11 +999,11 @@ extern "C" int ebsd_pcfit_xcorr_tables(int hp, int wp, void* tables, int64_t byt
   EBSD_ARG_CHECK(make_plan(hp, wp, pl), "enlarged detector %d x %d not supported (2..%d each)", hp, wp, MAX_HW);
   EBSD_ARG_CHECK(tables != nullptr, "ebsd_pcfit_xcorr_tables: null pointer");
   EBSD_ARG_CHECK(((uintptr_t)tables & 15) == 0, "tables must be 16-byte aligned");
-  const int64_t need = (int64_t)pl.tb.inv_bytes + pl.tb.fwd_bytes;
+  const int64_t need = pl.tb.total;
   EBSD_ARG_CHECK(bytes >= need, "tables hold %lld bytes, %lld needed", (long long)bytes, (long long)need);
   const Geo& g = pl.g;
-  const int64_t n = (int64_t)g.NA * 64 * g.KPA + (int64_t)g.NB * 64 * g.KPB + (int64_t)g.N1 * 64 * g.KP1 +
-                    (int64_t)g.N2 * 64 * g.KP2;
+  int64_t n = 0;
+  for (int m = 0; m < N_MATS; ++m) n += (int64_t)pl.tb.rows[m] * 64 * pl.tb.planes[m];
   k_xc_tables<<<(unsigned)((n + 255) / 256), 256, 0, as_stream(stream)>>>(g, pl.tb, static_cast<uint8_t*>(tables));
   EBSD_LAUNCH_CHECK();
   return 0;
@@ -832,11 +1060,35 @@ extern "C" int ebsd_pcfit_xcorr_max(const float* sim_spectra, int64_t n_sims, co
   p.n_pats = n_pats;
   p.index_base = index_base;
   p.keys = keys;
-  const int64_t passes = (n_sims + pl.pp - 1) / pl.pp;
+  const int pp = pl.pp_tm > 0 ? pl.pp_tm : pl.pp;
+  const int64_t passes = (n_sims + pp - 1) / pp;
   p.slices = (int)std::max<int64_t>(1, std::min<int64_t>(passes, sm_count() / std::max(1, n_pats)));
   const int64_t grid = (int64_t)n_pats * p.slices;
   EBSD_ARG_CHECK(grid < INT32_MAX, "too many patterns");
   cudaStream_t s = as_stream(stream);
+  if (pl.pp_tm > 0) {
+    p.pp_tm = pl.pp_tm;
+    p.buf_rows = pl.pp_tm * pl.g.RW;
+    p.buf_planes = pl.g.KPA;
+    p.buf_bytes = p.buf_rows * 128 * p.buf_planes;
+    switch (pl.cpt) {
+#define EBSD_XC_TM_CASE(CPT)                                                                                       \
+  case CPT:                                                                                                         \
+    EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_xc_max_tm<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.smem_tm)); \
+    k_xc_max_tm<CPT><<<(int)grid, THREADS, pl.smem_tm, s>>>(p);                                                     \
+    break;
+      EBSD_XC_TM_CASE(1)
+      EBSD_XC_TM_CASE(2)
+      EBSD_XC_TM_CASE(3)
+      EBSD_XC_TM_CASE(4)
+#undef EBSD_XC_TM_CASE
+      default:
+        set_error("internal: no kernel for %d column chunks per thread", pl.cpt);
+        return EBSD_ERR_ARG;
+    }
+    EBSD_LAUNCH_CHECK();
+    return 0;
+  }
   switch (pl.pos) {
 #define EBSD_XC_CASE(POS)                                                                                         \
   case POS:                                                                                                        \

@@ -75,4 +75,6 @@ def test_match_traffic_model_reproduces_its_captures():
 
     for rows, dram in bench.MATCH_DRAM_BYTES:
         assert abs(bench.match_traffic_estimate(rows) - dram) < 1.0
-    assert bench.match_traffic_estimate(328720) > 4 * (328960 * 16384 * 2)  # ~5 reads per row
+    # the 18-query-tile launches read each dictionary row about twice
+    operands = (328960 + bench.MATCH_WAVE_QUERIES) * 16384 * 2
+    assert 1.5 * operands < bench.match_traffic_estimate(328720) < 2.5 * operands
