@@ -52,7 +52,7 @@ def _run(inp, precision, small_plan, monkeypatch):
         # dictionary in chunks of ~6,900 rows merged into a running top-k, and
         # match launches of 8 query tiles (4 launches per query chunk)
         kw["workspace_bytes"] = 300 << 20
-        monkeypatch.setattr(engine, "wave_query_tiles", lambda dev: 8)
+        monkeypatch.setattr(engine, "wave_query_tiles", lambda dev, row_bytes=0: 8)
     torch.manual_seed(c["perm_seed"])
     dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=c["res"], top_k_matches=c["k"],
                                   dictionary_chunk_size=c["dictionary_chunk_size"],
