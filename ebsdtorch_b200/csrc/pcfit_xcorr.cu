@@ -16,7 +16,7 @@
 //     F2  Cc[ky, kx]    = sum_y T[y, kx] cos(2 pi ky y / H)       ky < H2 = H/2+1
 //         Ss[ky, kx]    = sum_y T[y, kx] sin(2 pi ky y / H)
 //     so that S[ky] = Cc - i Ss and S[H - ky] = Cc + i Ss.
-//   inverse (k_xc_max_tm, per (pattern, simulated pattern) pair), with
+//   inverse (k_xc_max, per (pattern, simulated pattern) pair), with
 //     Pe = conj(P[ky]) + conj(P[H-ky]), Po = conj(P[ky]) - conj(P[H-ky])
 //     (one term only at ky = 0 and ky = H/2):
 //     E = Cc Pe - i Ss Po,  O = Cc Po - i Ss Pe     (the even / odd parts of
@@ -26,19 +26,20 @@
 //     with y' = y - H/2, x' = x - W/2 (the fftshift) and a_kx = 1 for the
 //     DC and Nyquist columns, 2 otherwise (the c2r Hermitian fold).
 //
-// Each stage is D[128 lanes, N] = A[128 rows, K] B[N rows, K]^T. The
-// constant DFT matrices are built once per detector size and copied by each
-// CTA into shared memory; data operands are written by the CTA's threads in
-// the 128-byte-swizzled K-major layout the MMA descriptors read, or, for the
-// inverse's second stage, taken from TMEM where the first stage left them.
+// Each stage is D[128 lanes, N] = A[128 rows, K] B[N rows, K]^T with the
+// constant DFT matrix as B (copied once per CTA into shared memory) and the
+// data as A, written by the CTA's threads into shared memory in the
+// 128-byte-swizzled K-major layout the MMA descriptors read. Between the
+// stages the TMEM result is read back (tcgen05.ld) and written transposed as
+// the next stage's A operand.
 //
-// k_xc_max_tm: a CTA owns one experimental pattern and a slice of the batch;
-// per pass it correlates PP simulated patterns with it (3 at 78 x 78). Its
-// threads own TMEM lanes y, so the max over the pass's pairs and over passes
-// is kept per (y, x) in registers (the first maximum wins on ties, i.e. the
-// smaller index). At the end each (shift, max, index) is merged into a
-// 64-bit key (ordered float bits, inverted index) with atomicMax;
-// ebsd_pcfit_fold applies the reference's running-best rule
+// k_xc_max: a CTA owns one experimental pattern and a slice of the batch;
+// per pass it correlates PP simulated patterns with it (PP * 2 WF rows in
+// stage A, PP * H rows in stage B), then the passes' maps (staged in shared
+// memory) are max-reduced per shift into registers (the first maximum wins
+// on ties, i.e. the smaller index). At the end each (shift, max, index) is
+// merged into a 64-bit key (ordered float bits, inverted index) with
+// atomicMax; ebsd_pcfit_fold applies the reference's running-best rule
 // (fitting.py:498-507) per batch and clears the keys.
 //
 // Supported: enlarged detectors up to 127 x 127 (one 128-row tile per
@@ -66,7 +67,7 @@ struct Geo {
   int H2, WF;     // ky < H2 = H/2 + 1, kx < WF = W/2 + 1
   int KOA, KOB;   // H2, WF rounded up to 8 (the second half of a K row starts there)
   int RW;         // rows per image in the (part, kx) layout: 2 KOB
-  int NB;         // inverse: N of stage B (x)
+  int NA, NB;     // inverse: N of stage A (y) and stage B (x)
   int N1, N2;     // forward: N of F1 ((part, kx)) and F2 ((trig, ky))
   int KSA, KSB;   // inverse: 16-element K steps of stage A (2 KOA) and B (2 KOB)
   int KS1, KS2;   // forward: K steps of F1 (W) and F2 (H)
@@ -83,6 +84,7 @@ __host__ __device__ inline Geo make_geo(int H, int W) {
   g.KOA = round_up_i(g.H2, 8);
   g.KOB = round_up_i(g.WF, 8);
   g.RW = 2 * g.KOB;
+  g.NA = round_up_i(H, 16);
   g.NB = round_up_i(W, 16);
   g.N1 = round_up_i(2 * g.KOB, 16);
   g.N2 = round_up_i(2 * g.KOA, 16);
@@ -110,28 +112,32 @@ __host__ __device__ inline uint32_t op_offset(int rows, int row, int k) {
 // Bytes of one constant matrix image (hi or lo) of `rows` rows, `planes` planes.
 __host__ __device__ constexpr int mat_bytes(int rows, int planes) { return rows * 128 * planes; }
 
-// The constant matrices, each stored as two images (the hi and lo halves of
-// the bf16 split):
-//   0 inverse stage A  rows y (128: the MMA's A operand), K [cos | sin] over ky
-//   1 inverse stage B  rows x (NB), K [a cos | -a sin] / (H W) over kx
-//   2 forward F1       rows (re/im, kx) (N1), K x
-//   3 forward F2       rows (cos/sin, ky) (N2), K y
-// Matrices are stored one after the other; each kernel copies its run.
-constexpr int N_MATS = 4;
+// The constant matrices, each stored as two images (hi and lo halves of the
+// bf16 split, or for the mixed stage-B matrix of the TMEM kernel the
+// [hi | hi] and [lo | 0] images described at k_xc_max_tm):
+//   0 inverse stage A        rows y (NA), K [cos | sin] over ky
+//   1 inverse stage B        rows x (NB), K [a cos | -a sin] / (H W) over kx
+//   2 forward F1             rows (re/im, kx) (N1), K x
+//   3 forward F2             rows (cos/sin, ky) (N2), K y
+//   4 inverse stage A (TMEM) matrix 0 with 128 rows (the MMA's A operand)
+//   5 inverse stage B (TMEM) rows x (NB), K' = 2 * RW: per 8 K elements of
+//     matrix 1, 16 K' elements
+// Matrices are stored one after the other; kernels copy a contiguous run.
+constexpr int N_MATS = 6;
 struct Tables {
   int rows[N_MATS], planes[N_MATS];
   int img[N_MATS];  // bytes of one image
   int off[N_MATS];  // byte offset of the matrix's first image
   int total;
-  // contiguous runs per kernel: inverse (0, 1), forward (2, 3)
-  int inv_bytes, fwd_bytes;
-  int inv_a, inv_b, fwd_1, fwd_2;  // image bytes, for the kernels' layouts
+  // contiguous runs per kernel: inverse (0, 1), forward (2, 3), TMEM inverse (4, 5)
+  int inv_bytes, fwd_bytes, tm_bytes;
+  int inv_a, inv_b, fwd_1, fwd_2, tm_a, tm_b;  // image bytes, for the kernels' layouts
 };
 
 __host__ __device__ inline Tables table_sizes(const Geo& g) {
   Tables t{};
-  const int rows[N_MATS] = {128, g.NB, g.N1, g.N2};
-  const int planes[N_MATS] = {g.KPA, g.KPB, g.KP1, g.KP2};
+  const int rows[N_MATS] = {g.NA, g.NB, g.N1, g.N2, 128, g.NB};
+  const int planes[N_MATS] = {g.KPA, g.KPB, g.KP1, g.KP2, g.KPA, cdiv(2 * g.RW, 64)};
   int off = 0;
   for (int m = 0; m < N_MATS; ++m) {
     t.rows[m] = rows[m];
@@ -143,10 +149,13 @@ __host__ __device__ inline Tables table_sizes(const Geo& g) {
   t.total = off;
   t.inv_bytes = 2 * (t.img[0] + t.img[1]);
   t.fwd_bytes = 2 * (t.img[2] + t.img[3]);
+  t.tm_bytes = 2 * (t.img[4] + t.img[5]);
   t.inv_a = t.img[0];
   t.inv_b = t.img[1];
   t.fwd_1 = t.img[2];
   t.fwd_2 = t.img[3];
+  t.tm_a = t.img[4];
+  t.tm_b = t.img[5];
   return t;
 }
 
@@ -209,9 +218,16 @@ __global__ void k_xc_tables(Geo g, Tables t, uint8_t* __restrict__ out) {
   const int width = 64 * t.planes[m];
   const int row = (int)(r / width), k = (int)(r % width);
   __nv_bfloat16 v0, v1;
-  {
+  if (m == 5) {
+    // K' = 16 q + 8 half + j holds K = 8 q + j: image 0 [hi | hi], image 1 [lo | 0]
+    const int q = k / 16, half = (k / 8) & 1, j = k & 7, kk = 8 * q + j;
+    __nv_bfloat16 hi, lo;
+    split_bf16(kk < g.RW ? inv_b_value(g, row, kk) : 0.0, hi, lo);
+    v0 = hi;
+    v1 = half ? __float2bfloat16_rn(0.0f) : lo;
+  } else {
     double v = 0.0, c, s;
-    if (m == 0) {
+    if (m == 0 || m == 4) {
       v = inv_a_value(g, row, k);
     } else if (m == 1) {
       v = inv_b_value(g, row, k);
@@ -328,12 +344,6 @@ __device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8])
       : "memory");
 }
 
-__device__ __forceinline__ void tmem_st4(uint32_t taddr, const uint32_t (&v)[4]) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
-               "r"(v[2]), "r"(v[3])
-               : "memory");
-}
-
 __device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 struct XcParams {
@@ -356,7 +366,7 @@ struct XcParams {
   const float* pat_terms;
   int n_pats;
   int slices;
-
+  int pp_tm;  // TMEM kernel: pairs per pass
   int64_t index_base;
   unsigned long long* keys;
   int* status;
@@ -546,29 +556,15 @@ __device__ __forceinline__ unsigned long long max_key(float v, uint32_t idx) {
   return ((unsigned long long)ord << 32) | (unsigned long long)(0xFFFFFFFFu - idx);
 }
 
-// k_xc_max_tm: the inverse transforms and the max over the batch, with
-// stage A's output kept in TMEM as stage B's A operand. TMEM columns:
-// [0, 256) stage A's accumulators, later stage B's; [256, 384) and
-// [384, 512) the hi and lo halves of stage B's A operand.
-//   stage A  D_A[y, (pair, part, kx)] = CA[y, K] . Data[(pair, part, kx), K]^T
-//            with the constant (128 rows y) as the A operand and the pass's
-//            [E | O] rows as B (N = pairs * RW);
-//   convert  each thread splits its own 8-column chunks of D_A into bf16
-//            hi and lo halves, packed two per column into the operand regions
-//            (K contiguous per pair);
-//   stage B  D_B[y, (pair, x)] = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
-//            with A from TMEM, written over D_A (consumed by then);
-//   epilogue each thread owns lane y and CPT x chunks; the max over the
-//            pass's pairs and over passes stays in its registers.
-template <int CPT>  // x chunks of 8 per thread: NB / 8 <= 4 CPT
-__global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
+template <int POS>  // shifts per thread: H * W <= POS * THREADS
+__global__ void __launch_bounds__(THREADS, 1) k_xc_max(const XcParams p) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw_s = smem_u32(smem_raw);
   uint8_t* base = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
   const Geo& g = p.g;
   const Smem s = carve(base, p, p.tb.inv_a, p.tb.inv_b);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int lg = warp & 3, cg = warp >> 2;
+  const int lg = warp & 3, t_of_warp = (warp >> 2) % p.mt, cg = (warp >> 2) / p.mt, n_cg = 4 / p.mt;
   const int b = blockIdx.x / p.slices, sl = blockIdx.x - b * p.slices;
   const int64_t s_begin = p.n_sims * sl / p.slices, s_end = p.n_sims * (sl + 1) / p.slices;
 
@@ -583,11 +579,173 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s.tmem_slot;
-  const uint32_t da = tmem, db = tmem, ta_hi = tmem + 256u, ta_lo = tmem + 384u;
-  const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
-  const uint32_t d_hi = smem_u32(s.a_hi), d_lo = smem_u32(s.a_lo);
+  const uint32_t da = tmem, db = tmem + (uint32_t)(p.mt * g.NA);
+  const uint32_t a_hi = smem_u32(s.a_hi), a_lo = smem_u32(s.a_lo);
   const uint32_t ca_hi = smem_u32(s.c0), ca_lo = ca_hi + p.tb.inv_a;
   const uint32_t cb_hi = smem_u32(s.c1), cb_lo = cb_hi + p.tb.inv_b;
+  float* scratch = reinterpret_cast<float*>(s.a_hi);  // the pass's maps, [pair][y][x]
+  const int hw = g.H * g.W, ng = g.KOA / 8, hwf = g.H2 * g.WF;
+  const float* pt = p.pat_terms + (int64_t)b * g.spec;
+
+  float best_v[POS];
+  int best_i[POS];  // index inside the launch's batch (n_sims < 2^31)
+#pragma unroll
+  for (int j = 0; j < POS; ++j) {
+    best_v[j] = -INFINITY;
+    best_i[j] = -1;
+  }
+  uint32_t phase = 0;
+
+  for (int64_t s0 = s_begin; s0 < s_end; s0 += p.pp) {
+    const int np = (int)(s_end - s0 < p.pp ? s_end - s0 : p.pp);
+    // stage A operand: rows (pair, part, kx), K = [E part | O part] over ky
+    for (int it = tid; it < np * g.WF * ng; it += THREADS) {
+      const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng, grp = rem / g.WF, kx = rem - grp * g.WF;
+      const float* cs = p.sim_spec + (s0 + pr) * (int64_t)g.spec + kx;
+      float er[8], ei[8], orr[8], oi[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int ky = grp * 8 + j;
+        er[j] = ei[j] = orr[j] = oi[j] = 0.0f;
+        if (ky < g.H2) {
+          const int o = ky * g.WF;
+          const float a = __ldg(cs + o), bi = __ldg(cs + hwf + o);                // Cc
+          const float c = __ldg(cs + 2 * hwf + o), d = __ldg(cs + 3 * hwf + o);   // Ss
+          const float e = __ldg(pt + o + kx), f = __ldg(pt + hwf + o + kx);       // Pe
+          const float gg = __ldg(pt + 2 * hwf + o + kx), h = __ldg(pt + 3 * hwf + o + kx);  // Po
+          er[j] = a * e - bi * f + c * h + d * gg;
+          ei[j] = a * f + bi * e - c * gg + d * h;
+          orr[j] = a * gg - bi * h + c * f + d * e;
+          oi[j] = a * h + bi * gg - c * e + d * f;
+        }
+      }
+      float neg_oi[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) neg_oi[j] = -oi[j];
+      const int row_re = pr * g.RW + kx, row_im = row_re + g.KOB;
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_re, grp * 8, er);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_re, g.KOA + grp * 8, neg_oi);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_im, grp * 8, ei);
+      put8(s.a_hi, s.a_lo, p.buf_rows, row_im, g.KOA + grp * 8, orr);
+    }
+    if (!run_stage(s, p, phase, [&] {
+          issue_stage(da, g.NA, cdiv(np * g.RW, 128), a_hi, a_lo, p.buf_rows, ca_hi, ca_lo, g.NA, g.KSA);
+        }))
+      break;
+    // stage B operand: rows (pair, y), K = [Ur | Ui] over kx, from U (lanes
+    // (pair, part, kx), columns y)
+    {
+      const int r = t_of_warp * 128 + lg * 32 + lane;
+      const int pr = r / g.RW, c = r - pr * g.RW;
+      const int part = c >= g.KOB, kx = c - part * g.KOB;
+      const bool valid = r < np * g.RW && kx < g.WF;
+      if (t_of_warp * 128 < np * g.RW) {
+        for (int c8 = cg; c8 < g.NA / 8; c8 += n_cg) {
+          float v[8];
+          tmem_ld8(da + ((uint32_t)(lg * 32) << 16) + (uint32_t)(t_of_warp * g.NA + c8 * 8), v);
+          if (valid) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int y = c8 * 8 + j;
+              if (y < g.H) put1(s.a_hi, s.a_lo, p.buf_rows, pr * g.H + y, part * g.KOB + kx, v[j]);
+            }
+          }
+        }
+      }
+    }
+    if (!run_stage(s, p, phase, [&] {
+          issue_stage(db, g.NB, cdiv(np * g.H, 128), a_hi, a_lo, p.buf_rows, cb_hi, cb_lo, g.NB, g.KSB);
+        }))
+      break;
+    // maps (lanes (pair, y), columns x) into scratch, then the max over the pass
+    {
+      const int r = t_of_warp * 128 + lg * 32 + lane;
+      const bool valid = r < np * g.H;
+      if (t_of_warp * 128 < np * g.H) {
+        for (int c8 = cg; c8 < g.NB / 8; c8 += n_cg) {
+          float v[8];
+          tmem_ld8(db + ((uint32_t)(lg * 32) << 16) + (uint32_t)(t_of_warp * g.NB + c8 * 8), v);
+          if (valid) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              const int x = c8 * 8 + j;
+              if (x < g.W) scratch[r * g.W + x] = v[j];
+            }
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < POS; ++j) {
+      const int pos = tid + j * THREADS;
+      if (pos < hw) {
+        for (int pr = 0; pr < np; ++pr) {
+          const float v = scratch[pr * hw + pos];
+          if (v > best_v[j]) {
+            best_v[j] = v;
+            best_i[j] = (int)(s0 + pr);
+          }
+        }
+      }
+    }
+    __syncthreads();  // scratch (the A buffers) is rewritten by the next pass
+  }
+  if (*s.flag == 0) {
+    unsigned long long* keys = p.keys + (int64_t)b * hw;
+#pragma unroll
+    for (int j = 0; j < POS; ++j) {
+      const int pos = tid + j * THREADS;
+      if (pos < hw && best_i[j] >= 0) atomicMax(keys + pos, max_key(best_v[j], (uint32_t)(p.index_base + best_i[j])));
+    }
+  }
+  drain(s, phase ^ 1u);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, 512);
+}
+
+// k_xc_max_tm: k_xc_max with stage A's output kept in TMEM as stage B's A
+// operand (no shared-memory transpose, no staged maps):
+//   stage A  D_A[y, (pair, part, kx)] = CA[y, K] . Data[(pair, part, kx), K]^T
+//            with the constant (128 rows y) as the A operand and the pass's
+//            [E | O] rows as B (N = pairs * RW);
+//   convert  each thread rewrites its own 8-column chunks of D_A in place as
+//            [hi x 8 | lo x 8] bf16, 8 columns = 16 K' elements;
+//   stage B  D_B[y, (pair, x)] = sum over chunks q of A'(q) . P(q)^T +
+//            A'(q) . Q(q)^T, with P = [Bhi | Bhi] and Q = [Blo | 0] over the
+//            chunk's 8 K elements: hi Bhi + lo Bhi + hi Blo, the 3-term split;
+//   epilogue each thread owns lane y and CPT x chunks; the max over the
+//            pass's pairs and over passes stays in its registers.
+template <int CPT>  // x chunks of 8 per thread: NB / 8 <= 4 CPT
+__global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_s = smem_u32(smem_raw);
+  uint8_t* base = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
+  const Geo& g = p.g;
+  const Smem s = carve(base, p, p.tb.tm_a, p.tb.tm_b);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int lg = warp & 3, cg = warp >> 2;
+  const int b = blockIdx.x / p.slices, sl = blockIdx.x - b * p.slices;
+  const int64_t s_begin = p.n_sims * sl / p.slices, s_end = p.n_sims * (sl + 1) / p.slices;
+
+  load_constants(s, p.tables + p.tb.off[4], p.tb.tm_bytes, p);
+  if (tid == 0) {
+    mbar_init(smem_u32(s.bar), 1);
+    *s.flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(smem_u32(s.tmem_slot), 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s.tmem_slot;
+  const uint32_t da = tmem, db = tmem + 256u;
+  const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
+  const uint32_t d_hi = smem_u32(s.a_hi), d_lo = smem_u32(s.a_lo);
+  const uint32_t ca_hi = smem_u32(s.c0), ca_lo = ca_hi + p.tb.tm_a;
+  const uint32_t cp = smem_u32(s.c1), cq = cp + p.tb.tm_b;
   const int ng = g.KOA / 8, hwf = g.H2 * g.WF, nb8 = g.NB / 8, rw8 = g.RW / 8;
   const float* pt = p.pat_terms + (int64_t)b * g.spec;
   const int y = lg * 32 + lane;
@@ -603,8 +761,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
     }
   uint32_t phase = 0;
 
-  for (int64_t s0 = s_begin; s0 < s_end; s0 += p.pp) {
-    const int np = (int)(s_end - s0 < p.pp ? s_end - s0 : p.pp);
+  for (int64_t s0 = s_begin; s0 < s_end; s0 += p.pp_tm) {
+    const int np = (int)(s_end - s0 < p.pp_tm ? s_end - s0 : p.pp_tm);
     // stage A's B operand: rows (pair, part, kx), K = [E part | O part] over ky
     for (int it = tid; it < np * g.WF * ng; it += THREADS) {
       const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng, grp = rem / g.WF, kx = rem - grp * g.WF;
@@ -644,32 +802,29 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
           }
         }))
       break;
-    // D_A chunks -> hi and lo bf16 halves (this thread's lanes and columns only)
+    // D_A chunks -> [hi | lo] bf16 in place (this thread's lanes and columns only)
     for (int c8 = cg; c8 < np * rw8; c8 += 4) {
       float v[8];
       tmem_ld8(da + lane_off + (uint32_t)(c8 * 8), v);
-      uint32_t wh[4], wl[4];
+      uint32_t w[8];
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
         const __nv_bfloat16 h0 = __float2bfloat16_rn(v[2 * j]), h1 = __float2bfloat16_rn(v[2 * j + 1]);
-        wh[j] = pack_bf16(h0, h1);
-        wl[j] = pack_bf16(__float2bfloat16_rn(v[2 * j] - __bfloat162float(h0)),
-                          __float2bfloat16_rn(v[2 * j + 1] - __bfloat162float(h1)));
+        w[j] = pack_bf16(h0, h1);
+        w[4 + j] = pack_bf16(__float2bfloat16_rn(v[2 * j] - __bfloat162float(h0)),
+                             __float2bfloat16_rn(v[2 * j + 1] - __bfloat162float(h1)));
       }
-      tmem_st4(ta_hi + lane_off + (uint32_t)(c8 * 4), wh);
-      tmem_st4(ta_lo + lane_off + (uint32_t)(c8 * 4), wl);
+      tmem_st8(da + lane_off + (uint32_t)(c8 * 8), w);
     }
     tmem_wait_st();
     if (!run_stage(s, p, phase, [&] {
           const uint32_t idesc = xc_idesc(g.NB);
           for (int pr = 0; pr < np; ++pr) {
-            const uint32_t d = db + (uint32_t)(pr * g.NB), a0 = (uint32_t)(pr * g.RW / 2);
-            for (int ks = 0; ks < g.KSB; ++ks) {
-              const uint32_t boff = (uint32_t)(ks >> 2) * (uint32_t)g.NB * 128u + (uint32_t)(ks & 3) * 32u;
-              const uint32_t a = a0 + (uint32_t)(8 * ks);
-              tc_mma_ta(d, ta_hi + a, smem_desc_sw128(cb_hi + boff), idesc, ks > 0 ? 1u : 0u);
-              tc_mma_ta(d, ta_hi + a, smem_desc_sw128(cb_lo + boff), idesc, 1u);
-              tc_mma_ta(d, ta_lo + a, smem_desc_sw128(cb_hi + boff), idesc, 1u);
+            for (int q = 0; q < rw8; ++q) {
+              const uint32_t boff = (uint32_t)((16 * q) >> 6) * (uint32_t)g.NB * 128u + (uint32_t)(q & 3) * 32u;
+              const uint32_t a = da + (uint32_t)(pr * g.RW + 8 * q);
+              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cp + boff), idesc, q > 0 ? 1u : 0u);
+              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cq + boff), idesc, 1u);
             }
           }
         }))
@@ -763,10 +918,8 @@ namespace {
 struct Plan {
   Geo g;
   Tables tb;
-  // forward kernel: images per pass (mt 128-row tiles) and its A buffers
-  int mt, buf_rows, buf_planes, buf_bytes, smem_fwd;
-  // inverse kernel: pairs per pass, shared memory, x chunks per thread
-  int pp, smem_inv, cpt;
+  int mt, pp, buf_rows, buf_planes, buf_bytes, smem_fwd, smem_inv, pos;
+  int pp_tm, smem_tm, cpt;  // TMEM kernel (pp_tm 0: the detector does not fit it)
 };
 
 bool make_plan(int hp, int wp, Plan& pl) {
@@ -774,29 +927,35 @@ bool make_plan(int hp, int wp, Plan& pl) {
   pl.g = make_geo(hp, wp);
   pl.tb = table_sizes(pl.g);
   const Geo& g = pl.g;
-  pl.buf_planes = std::max(g.KP1, g.KP2);
-  pl.mt = 0;
-  for (int mt = 2; mt >= 1 && pl.mt == 0; --mt) {
-    const int buf = mt * 128 * 128 * pl.buf_planes;
-    if (smem_bytes(buf, pl.tb.fwd_1, pl.tb.fwd_2) <= SMEM_LIMIT) {
-      pl.mt = mt;
-      pl.buf_rows = mt * 128;
-      pl.buf_bytes = buf;
-      pl.smem_fwd = smem_bytes(buf, pl.tb.fwd_1, pl.tb.fwd_2);
-    }
+  pl.buf_planes = std::max(std::max(g.KPA, g.KPB), std::max(g.KP1, g.KP2));
+  for (int mt = 2; mt >= 1; --mt) {
+    pl.mt = mt;
+    pl.buf_rows = mt * 128;
+    pl.buf_bytes = pl.buf_rows * 128 * pl.buf_planes;
+    pl.smem_inv = smem_bytes(pl.buf_bytes, pl.tb.inv_a, pl.tb.inv_b);
+    pl.smem_fwd = smem_bytes(pl.buf_bytes, pl.tb.fwd_1, pl.tb.fwd_2);
+    pl.pp = std::min(pl.buf_rows / g.RW, pl.buf_rows / g.H);
+    // the pass's maps are staged in the A buffers
+    while (pl.pp > 1 && (int64_t)pl.pp * g.H * g.W * 4 > 2 * (int64_t)pl.buf_bytes) --pl.pp;
+    if (pl.smem_inv <= SMEM_LIMIT && pl.smem_fwd <= SMEM_LIMIT && pl.pp >= 1 &&
+        (int64_t)pl.pp * g.H * g.W * 4 <= 2 * (int64_t)pl.buf_bytes)
+      break;
+    pl.mt = 0;
   }
-  // inverse: pairs per pass limited by N <= 256 for both stages (stage B's
-  // accumulators overlay stage A's in TMEM columns [0, 256); the hi and lo
-  // operand halves take pp * RW / 2 <= 128 columns each) and shared memory
-  pl.pp = 0;
-  for (int pp = std::min(256 / g.RW, 256 / g.NB); pp >= 1 && pl.pp == 0; --pp) {
-    const int bytes = smem_bytes(pp * g.RW * 128 * g.KPA, pl.tb.inv_a, pl.tb.inv_b);
+  if (pl.mt == 0) return false;
+  const int pos = cdiv(hp * wp, THREADS);
+  pl.pos = pos <= 8 ? 8 : pos <= 16 ? 16 : 32;
+  // TMEM kernel: pairs per pass limited by N <= 256 for both stages, the
+  // 256 + 256 TMEM columns and shared memory
+  pl.pp_tm = 0;
+  for (int pp = std::min(256 / g.RW, 256 / g.NB); pp >= 1; --pp) {
+    const int bytes = smem_bytes(pp * g.RW * 128 * g.KPA, pl.tb.tm_a, pl.tb.tm_b);
     if (bytes <= SMEM_LIMIT) {
-      pl.pp = pp;
-      pl.smem_inv = bytes;
+      pl.pp_tm = pp;
+      pl.smem_tm = std::max(bytes, SMEM_ONE_CTA);
+      break;
     }
   }
-  if (pl.mt == 0 || pl.pp == 0) return false;
   pl.cpt = cdiv(g.NB / 8, 4);
   // every CTA allocates all 512 TMEM columns: ask for enough shared memory
   // that no second CTA fits on the SM
@@ -816,6 +975,7 @@ XcParams base_params(const Plan& pl, const void* tables, int* status) {
   XcParams p{};
   p.g = pl.g;
   p.mt = pl.mt;
+  p.pp = pl.pp;
   p.buf_rows = pl.buf_rows;
   p.buf_planes = pl.buf_planes;
   p.buf_bytes = pl.buf_bytes;
@@ -900,27 +1060,47 @@ extern "C" int ebsd_pcfit_xcorr_max(const float* sim_spectra, int64_t n_sims, co
   p.n_pats = n_pats;
   p.index_base = index_base;
   p.keys = keys;
-  const int64_t passes = (n_sims + pl.pp - 1) / pl.pp;
+  const int pp = pl.pp_tm > 0 ? pl.pp_tm : pl.pp;
+  const int64_t passes = (n_sims + pp - 1) / pp;
   p.slices = (int)std::max<int64_t>(1, std::min<int64_t>(passes, sm_count() / std::max(1, n_pats)));
   const int64_t grid = (int64_t)n_pats * p.slices;
   EBSD_ARG_CHECK(grid < INT32_MAX, "too many patterns");
   cudaStream_t s = as_stream(stream);
-  p.buf_rows = pl.pp * pl.g.RW;
-  p.buf_planes = pl.g.KPA;
-  p.buf_bytes = p.buf_rows * 128 * p.buf_planes;
-  switch (pl.cpt) {
-#define EBSD_XC_CASE(CPT)                                                                                            \
-  case CPT:                                                                                                           \
-    EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_xc_max_tm<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.smem_inv)); \
-    k_xc_max_tm<CPT><<<(int)grid, THREADS, pl.smem_inv, s>>>(p);                                                      \
+  if (pl.pp_tm > 0) {
+    p.pp_tm = pl.pp_tm;
+    p.buf_rows = pl.pp_tm * pl.g.RW;
+    p.buf_planes = pl.g.KPA;
+    p.buf_bytes = p.buf_rows * 128 * p.buf_planes;
+    switch (pl.cpt) {
+#define EBSD_XC_TM_CASE(CPT)                                                                                       \
+  case CPT:                                                                                                         \
+    EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_xc_max_tm<CPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.smem_tm)); \
+    k_xc_max_tm<CPT><<<(int)grid, THREADS, pl.smem_tm, s>>>(p);                                                     \
     break;
-    EBSD_XC_CASE(1)
-    EBSD_XC_CASE(2)
-    EBSD_XC_CASE(3)
-    EBSD_XC_CASE(4)
+      EBSD_XC_TM_CASE(1)
+      EBSD_XC_TM_CASE(2)
+      EBSD_XC_TM_CASE(3)
+      EBSD_XC_TM_CASE(4)
+#undef EBSD_XC_TM_CASE
+      default:
+        set_error("internal: no kernel for %d column chunks per thread", pl.cpt);
+        return EBSD_ERR_ARG;
+    }
+    EBSD_LAUNCH_CHECK();
+    return 0;
+  }
+  switch (pl.pos) {
+#define EBSD_XC_CASE(POS)                                                                                         \
+  case POS:                                                                                                        \
+    EBSD_CUDA_CHECK(cudaFuncSetAttribute(k_xc_max<POS>, cudaFuncAttributeMaxDynamicSharedMemorySize, pl.smem_inv)); \
+    k_xc_max<POS><<<(int)grid, THREADS, pl.smem_inv, s>>>(p);                                                      \
+    break;
+    EBSD_XC_CASE(8)
+    EBSD_XC_CASE(16)
+    EBSD_XC_CASE(32)
 #undef EBSD_XC_CASE
     default:
-      set_error("internal: no kernel for %d column chunks per thread", pl.cpt);
+      set_error("internal: no kernel for %d shifts per thread", pl.pos);
       return EBSD_ERR_ARG;
   }
   EBSD_LAUNCH_CHECK();

@@ -104,7 +104,7 @@ def test_pcfit_correlation_kernels_size_limits_need_no_gpu():
     import pytest
 
     lib = _capi.load()
-    assert lib.ebsd_pcfit_xcorr_table_bytes(78, 78) == 188416  # four matrices, hi and lo images each
+    assert lib.ebsd_pcfit_xcorr_table_bytes(78, 78) == 290816  # six matrices, hi and lo images each
     assert lib.ebsd_pcfit_xcorr_table_bytes(127, 127) > 0
     for h, w in ((128, 78), (78, 128), (1, 40), (40, 1), (0, 0)):
         assert lib.ebsd_pcfit_xcorr_table_bytes(h, w) == 0
