@@ -760,10 +760,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
       best_i[j][i] = -1;
     }
   uint32_t phase = 0;
+  const int64_t n_pass = (s_end - s_begin + p.pp_tm - 1) / p.pp_tm;
+  auto pass_np = [&](int64_t i) {
+    const int64_t left = s_end - (s_begin + i * p.pp_tm);
+    return (int)(left < p.pp_tm ? left : p.pp_tm);
+  };
 
-  for (int64_t s0 = s_begin; s0 < s_end; s0 += p.pp_tm) {
-    const int np = (int)(s_end - s0 < p.pp_tm ? s_end - s0 : p.pp_tm);
-    // stage A's B operand: rows (pair, part, kx), K = [E part | O part] over ky
+  // stage A's B operand of pass i: rows (pair, part, kx), K = [E | O] over ky
+  auto form = [&](int64_t i) {
+    const int64_t s0 = s_begin + i * p.pp_tm;
+    const int np = pass_np(i);
     for (int it = tid; it < np * g.WF * ng; it += THREADS) {
       const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng, grp = rem / g.WF, kx = rem - grp * g.WF;
       const float* cs = p.sim_spec + (s0 + pr) * (int64_t)g.spec + kx;
@@ -790,19 +796,31 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
       put8(s.a_hi, s.a_lo, p.buf_rows, row_im, grp * 8, ei);
       put8(s.a_hi, s.a_lo, p.buf_rows, row_im, g.KOA + grp * 8, orr);
     }
-    if (!run_stage(s, p, phase, [&] {
-          const int n = np * g.RW;
-          const uint32_t idesc = xc_idesc(n);
-          for (int ks = 0; ks < g.KSA; ++ks) {
-            const uint32_t aoff = (uint32_t)(ks >> 2) * 128u * 128u + (uint32_t)(ks & 3) * 32u;
-            const uint32_t boff = (uint32_t)(ks >> 2) * (uint32_t)p.buf_rows * 128u + (uint32_t)(ks & 3) * 32u;
-            tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_hi + boff), idesc, ks > 0 ? 1u : 0u);
-            tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_lo + boff), idesc, 1u);
-            tc_mma<0>(da, smem_desc_sw128(ca_lo + aoff), smem_desc_sw128(d_hi + boff), idesc, 1u);
-          }
-        }))
-      break;
-    // D_A chunks -> [hi | lo] bf16 in place (this thread's lanes and columns only)
+  };
+  auto issue_a = [&](int np) {
+    const int n = np * g.RW;
+    const uint32_t idesc = xc_idesc(n);
+    for (int ks = 0; ks < g.KSA; ++ks) {
+      const uint32_t aoff = (uint32_t)(ks >> 2) * 128u * 128u + (uint32_t)(ks & 3) * 32u;
+      const uint32_t boff = (uint32_t)(ks >> 2) * (uint32_t)p.buf_rows * 128u + (uint32_t)(ks & 3) * 32u;
+      tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_hi + boff), idesc, ks > 0 ? 1u : 0u);
+      tc_mma<0>(da, smem_desc_sw128(ca_hi + aoff), smem_desc_sw128(d_lo + boff), idesc, 1u);
+      tc_mma<0>(da, smem_desc_sw128(ca_lo + aoff), smem_desc_sw128(d_hi + boff), idesc, 1u);
+    }
+  };
+  auto issue_b = [&](int np) {
+    const uint32_t idesc = xc_idesc(g.NB);
+    for (int pr = 0; pr < np; ++pr) {
+      for (int q = 0; q < rw8; ++q) {
+        const uint32_t boff = (uint32_t)((16 * q) >> 6) * (uint32_t)g.NB * 128u + (uint32_t)(q & 3) * 32u;
+        const uint32_t a = da + (uint32_t)(pr * g.RW + 8 * q);
+        tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cp + boff), idesc, q > 0 ? 1u : 0u);
+        tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cq + boff), idesc, 1u);
+      }
+    }
+  };
+  // D_A chunks -> [hi | lo] bf16 in place (this thread's lanes and columns only)
+  auto convert = [&](int np) {
     for (int c8 = cg; c8 < np * rw8; c8 += 4) {
       float v[8];
       tmem_ld8(da + lane_off + (uint32_t)(c8 * 8), v);
@@ -817,19 +835,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
       tmem_st8(da + lane_off + (uint32_t)(c8 * 8), w);
     }
     tmem_wait_st();
-    if (!run_stage(s, p, phase, [&] {
-          const uint32_t idesc = xc_idesc(g.NB);
-          for (int pr = 0; pr < np; ++pr) {
-            for (int q = 0; q < rw8; ++q) {
-              const uint32_t boff = (uint32_t)((16 * q) >> 6) * (uint32_t)g.NB * 128u + (uint32_t)(q & 3) * 32u;
-              const uint32_t a = da + (uint32_t)(pr * g.RW + 8 * q);
-              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cp + boff), idesc, q > 0 ? 1u : 0u);
-              tc_mma_ta(db + (uint32_t)(pr * g.NB), a, smem_desc_sw128(cq + boff), idesc, 1u);
-            }
-          }
-        }))
-      break;
-    // maps: lane y, columns (pair, x); max over the pairs, then the running max
+  };
+  // maps of pass i: lane y, columns (pair, x); max over the pairs, then the running max
+  auto epilogue = [&](int64_t i) {
+    const int64_t s0 = s_begin + i * p.pp_tm;
+    const int np = pass_np(i);
     for (int pr = 0; pr < np; ++pr) {
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
@@ -838,14 +848,61 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
           float v[8];
           tmem_ld8(db + lane_off + (uint32_t)(pr * g.NB + c8 * 8), v);
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            if (v[i] > best_v[j][i]) {
-              best_v[j][i] = v[i];
-              best_i[j][i] = (int)(s0 + pr);
+          for (int i8 = 0; i8 < 8; ++i8) {
+            if (v[i8] > best_v[j][i8]) {
+              best_v[j][i8] = v[i8];
+              best_i[j][i8] = (int)(s0 + pr);
             }
           }
         }
       }
+    }
+  };
+  // Software pipeline, one MMA batch in flight at a time: stage B of pass i
+  // runs under the operand formation of pass i + 1, stage A of pass i + 1
+  // under the epilogue of pass i. issue(): writes made visible to the
+  // tensor core, thread 0 issues and commits; wait(): thread 0 waits
+  // (bounded), everyone learns the outcome.
+  auto issue = [&](auto&& mmas) {
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      mmas();
+      tc_commit(smem_u32(s.bar));
+    }
+  };
+  auto wait = [&]() {
+    if (tid == 0 && !mbar_wait(smem_u32(s.bar), phase, s.flag, p.wait_ns)) {
+      *s.flag = 1;
+      atomicExch(p.status, EBSD_DEVICE_TIMEOUT);
+    }
+    phase ^= 1u;
+    __syncthreads();
+    tc_fence_after();
+    return *s.flag == 0;
+  };
+  bool ok = true;
+  if (n_pass > 0) {
+    form(0);
+    issue([&] { issue_a(pass_np(0)); });
+    ok = wait();
+    if (ok) {
+      convert(pass_np(0));
+      issue([&] { issue_b(pass_np(0)); });
+    }
+  }
+  for (int64_t i = 0; ok && i < n_pass; ++i) {
+    const bool more = i + 1 < n_pass;
+    if (more) form(i + 1);  // the data operand is free: stage A of pass i is done
+    if (!(ok = wait())) break;  // stage B of pass i
+    if (more) issue([&] { issue_a(pass_np(i + 1)); });  // stage B of pass i has read D_A
+    epilogue(i);
+    if (more) {
+      if (!(ok = wait())) break;  // stage A of pass i + 1
+      convert(pass_np(i + 1));
+      issue([&] { issue_b(pass_np(i + 1)); });
     }
   }
   if (*s.flag == 0 && y < g.H) {
