@@ -766,12 +766,29 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
     return (int)(left < p.pp_tm ? left : p.pp_tm);
   };
 
+  // this thread's operand-formation items, the same in every pass (at most
+  // two: pp * WF * KOA / 8 <= 1024): (pair, ky group of 8, kx), decoded once
+  int it_pr[2], it_grp[2], it_kx[2];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int it = tid + k * THREADS;
+    it_pr[k] = INT_MAX;  // inactive
+    it_grp[k] = it_kx[k] = 0;
+    if (it < p.pp_tm * g.WF * ng) {
+      const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng;
+      it_pr[k] = pr;
+      it_grp[k] = rem / g.WF;
+      it_kx[k] = rem - it_grp[k] * g.WF;
+    }
+  }
   // stage A's B operand of pass i: rows (pair, part, kx), K = [E | O] over ky
   auto form = [&](int64_t i) {
     const int64_t s0 = s_begin + i * p.pp_tm;
     const int np = pass_np(i);
-    for (int it = tid; it < np * g.WF * ng; it += THREADS) {
-      const int pr = it / (g.WF * ng), rem = it - pr * g.WF * ng, grp = rem / g.WF, kx = rem - grp * g.WF;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (it_pr[k] >= np) continue;
+      const int pr = it_pr[k], grp = it_grp[k], kx = it_kx[k];
       const float* cs = p.sim_spec + (s0 + pr) * (int64_t)g.spec + kx;
       float er[8], ei[8], orr[8], noi[8];
 #pragma unroll
