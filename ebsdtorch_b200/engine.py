@@ -15,6 +15,7 @@ merged into a running result.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass
 from typing import Callable, Optional
 
@@ -36,6 +37,26 @@ RESCORE_COUNTER: Optional[torch.Tensor] = None
 # When set to a list, Searcher.run appends (start, end) CUDA-event pairs
 # around every merge + re-score launch (measurement only).
 MERGE_TIMERS: Optional[list] = None
+# NVTX ranges around the phases of Searcher.run (dictionary chunk fill,
+# query chunk preparation, match wave, merge) for timeline profilers; off
+# unless EBSD_NVTX=1 in the environment.
+NVTX = os.environ.get("EBSD_NVTX", "0") == "1"
+
+
+class _Range:
+    """NVTX range when NVTX is on, else nothing."""
+
+    def __init__(self, name: str):
+        self.name = name
+
+    def __enter__(self):
+        if NVTX:
+            torch.cuda.nvtx.range_push(self.name)
+
+    def __exit__(self, *exc):
+        if NVTX:
+            torch.cuda.nvtx.range_pop()
+        return False
 
 
 @dataclass
@@ -310,7 +331,8 @@ class Searcher:
                 if nd < dict_rows.n_rows:
                     dict_rows.lp[nd:].zero_()
                     dict_rows.norm[nd:].zero_()
-                fill_dict(d0, d1, dict_rows.buffers(0, nd))
+                with _Range(f"ebsd dictionary rows [{d0}, {d1})"):
+                    fill_dict(d0, d1, dict_rows.buffers(0, nd))
             col_scale = _col_scale(dict_rows, self.cfg.similarity)
             col_bias = _col_bias(dict_rows, self.cfg.similarity)
             nd_pad = round_up(nd, TILE_D)
@@ -318,7 +340,8 @@ class Searcher:
             for q0 in range(0, Q, qc):
                 q1 = min(Q, q0 + qc)
                 nq = q1 - q0
-                fill_queries(q0, q1, q_rows.buffers(0, nq))
+                with _Range(f"ebsd query rows [{q0}, {q1})"):
+                    fill_queries(q0, q1, q_rows.buffers(0, nq))
                 row_scale = _row_scale(q_rows, self.cfg.similarity)
                 # the next chunk's host-to-device copy runs under this chunk's matching
                 prefetch = getattr(fill_queries, "prefetch", None)
@@ -339,6 +362,8 @@ class Searcher:
                         ev0 = torch.cuda.Event(enable_timing=True)
                         ev1 = torch.cuda.Event(enable_timing=True)
                         ev0.record()
+                    rng = _Range(f"ebsd match queries [{q0 + s0}, {q0 + s1}) x dictionary [{d0}, {d1})")
+                    rng.__enter__()
                     if self.manhattan:
                         splits = max(1, min(max_splits, split_cap, (nd + 63) // 64,
                                             2 * sms // max(1, ns_pad // 64) + 1))
@@ -349,6 +374,7 @@ class Searcher:
                                            self.n_cand, splits, part_val, part_idx, splits, 0, d0, status,
                                            tile_n=cfg.tile_n, max_ctas=max_ctas, col_bias=col_bias,
                                            row_scale=row_scale[s0:] if row_scale is not None else None)
+                    rng.__exit__()
                     if timers is not None:
                         ev1.record()
                         timers.append((ev0, ev1, 2.0 * ns * nd * self.n_pix))
@@ -359,6 +385,8 @@ class Searcher:
                         m0 = torch.cuda.Event(enable_timing=True)
                         m1 = torch.cuda.Event(enable_timing=True)
                         m0.record()
+                    rng = _Range(f"ebsd merge queries [{g0}, {g1})")
+                    rng.__enter__()
                     kernels.merge_rescore(
                         part_val, part_idx, ns, splits, self.n_cand,
                         q_rows.f32[s0:s1] if self.rescore else None,
@@ -369,6 +397,7 @@ class Searcher:
                                       splits * self.n_cand, 128), k,
                         out_val[g0:g1] if run else None, out_idx[g0:g1] if run else None,
                         out_val[g0:g1], out_idx[g0:g1], gate_rel=gate, n_rescored=RESCORE_COUNTER)
+                    rng.__exit__()
                     if mtimers is not None:
                         m1.record()
                         mtimers.append((m0, m1))
