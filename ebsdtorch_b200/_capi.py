@@ -14,13 +14,16 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libebsd_b200.so")
+# EBSD_CHECK_BUILD=1 loads the checking build (`python -m ebsdtorch_b200.build --check`)
+LIB_PATH = os.path.join(_HERE, "_lib", "libebsd_b200_check.so" if os.environ.get("EBSD_CHECK_BUILD") == "1"
+                        else "libebsd_b200.so")
 
 vp, i32, i64, f32, sz = C.c_void_p, C.c_int, C.c_int64, C.c_float, C.c_size_t
 
 # name -> (restype, argtypes); mirrors include/ebsd_b200.h
 SIGNATURES = {
     "ebsd_version": (i32, []),
+    "ebsd_debug_check_line": (i32, [C.c_char_p, sz]),
     "ebsd_last_error": (i32, [C.c_char_p, sz]),
     "ebsd_device_check": (i32, [i32]),
     "ebsd_grid_workspace_bytes": (sz, [i32]),
@@ -133,6 +136,14 @@ def load() -> C.CDLL:
                 fn.argtypes = args
             _lib = lib
     return _lib
+
+
+def debug_check() -> tuple:
+    """(line, file) of the first failed device check since the last call in
+    the checking build, (0, "") when none, (-1, "") in the normal build."""
+    buf = C.create_string_buffer(512)
+    line = load().ebsd_debug_check_line(buf, len(buf))
+    return line, buf.value.decode(errors="replace")
 
 
 def last_error() -> str:

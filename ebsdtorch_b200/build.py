@@ -4,6 +4,9 @@ Every ``csrc/*.cu`` file is compiled for sm_100a only
 (``-gencode arch=compute_100a,code=sm_100a``) and linked into one shared
 library with the static CUDA runtime. Usage: ``python -m ebsdtorch_b200.build``.
 Objects are rebuilt only when a source or header is newer than the library.
+``--check`` builds ``_lib/libebsd_b200_check.so`` with -DEBSD_CHECK (device
+checks of computed offsets that record a failing line instead of accessing
+memory; loaded when EBSD_CHECK_BUILD=1).
 """
 
 from __future__ import annotations
@@ -19,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libebsd_b200.so")
+LIB_CHECK = os.path.join(LIBDIR, "libebsd_b200_check.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -43,13 +47,14 @@ def _newest_input() -> float:
     return max(os.path.getmtime(f) for f in files)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_input():
-        return LIB
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, check: bool = False) -> str:
+    lib = LIB_CHECK if check else LIB
+    if not force and os.path.exists(lib) and os.path.getmtime(lib) >= _newest_input():
+        return lib
     nvcc = _nvcc()
-    objdir = os.path.join(LIBDIR, "obj")
+    objdir = os.path.join(LIBDIR, "obj_check" if check else "obj")
     os.makedirs(objdir, exist_ok=True)
-    extra = ["-Xptxas", "-v"] if ptxas_info else []
+    extra = (["-Xptxas", "-v"] if ptxas_info else []) + (["-DEBSD_CHECK"] if check else [])
 
     def compile_one(src):
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
@@ -67,15 +72,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             if err.strip():
                 print(err, file=sys.stderr)
     objs = [o for o, _ in results]
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr}")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
     force = "--force" in sys.argv
-    print(build(force=force, verbose=True, ptxas_info="--ptxas-info" in sys.argv))
+    print(build(force=force, verbose=True, ptxas_info="--ptxas-info" in sys.argv, check="--check" in sys.argv))

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -17,6 +18,21 @@ void set_error(const char* fmt, ...) {
   vsnprintf(buf, sizeof(buf), fmt, ap);
   va_end(ap);
   g_last_error = buf;
+}
+
+struct CheckWord {
+  const void* symbol;
+  const char* file;
+};
+
+static std::vector<CheckWord>& check_words() {
+  static std::vector<CheckWord> words;
+  return words;
+}
+
+int register_check_word(const void* symbol, const char* file) {
+  check_words().push_back({symbol, file});
+  return 0;
 }
 
 int device_sm_count() {
@@ -61,6 +77,32 @@ __global__ void k_avg_pool(const float* __restrict__ in, int64_t n, int h, int w
 using namespace ebsd;
 
 extern "C" int ebsd_version(void) { return 100; }
+
+extern "C" int ebsd_debug_check_line(char* file, size_t n) {
+#ifdef EBSD_CHECK
+  int found = 0;
+  for (const CheckWord& w : check_words()) {
+    int line = 0;
+    EBSD_CUDA_CHECK(cudaMemcpyFromSymbol(&line, w.symbol, sizeof(int)));
+    if (line != 0) {
+      const int zero = 0;
+      EBSD_CUDA_CHECK(cudaMemcpyToSymbol(w.symbol, &zero, sizeof(int)));
+      if (found == 0) {
+        found = line;
+        if (file && n) {
+          strncpy(file, w.file, n - 1);
+          file[n - 1] = 0;
+        }
+      }
+    }
+  }
+  return found;
+#else
+  (void)file;
+  (void)n;
+  return -1;  // built without checks
+#endif
+}
 
 extern "C" int ebsd_last_error(char* buf, size_t n) {
   if (buf && n) {

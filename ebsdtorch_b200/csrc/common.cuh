@@ -27,6 +27,21 @@ void set_error(const char* fmt, ...);
 // (ebsd_set_wait_limit_ns; kWaitLimitNs by default).
 uint64_t wait_limit_ns();
 
+// Debug checks. In the checking build (-DEBSD_CHECK: `python -m
+// ebsdtorch_b200.build --check`, loaded when EBSD_CHECK_BUILD=1) a failed
+// EBSD_DCHECK(cond) records its source line in this translation unit's
+// device word (the first failure wins) and evaluates to false, so the caller
+// skips the access; ebsd_debug_check_line() reads and clears the words of
+// every translation unit. In the normal build the checks compile away.
+int register_check_word(const void* symbol, const char* file);
+#ifdef EBSD_CHECK
+static __device__ int g_check_line;
+static const int g_check_registered = register_check_word(&g_check_line, __FILE__);
+#define EBSD_DCHECK(cond) ((cond) ? true : (atomicCAS(&::ebsd::g_check_line, 0, __LINE__), false))
+#else
+#define EBSD_DCHECK(cond) true
+#endif
+
 #define EBSD_ARG_CHECK(cond, ...)              \
   do {                                         \
     if (!(cond)) {                             \

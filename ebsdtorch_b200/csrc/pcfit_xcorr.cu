@@ -490,7 +490,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_forward(const XcParams p) {
       float v[8];
 #pragma unroll
       for (int j = 0; j < 8; ++j) v[j] = x0 + j < g.W ? __ldg(row + x0 + j) : 0.0f;
-      put8(s.a_hi, s.a_lo, p.buf_rows, t * 128 + y, x0, v);
+      if (EBSD_DCHECK(t * 128 + y < p.buf_rows && x0 + 8 <= 64 * p.buf_planes))
+        put8(s.a_hi, s.a_lo, p.buf_rows, t * 128 + y, x0, v);
     }
     if (!run_stage(s, p, phase, [&] {
           issue_stage(d1, g.N1, ni, a_hi, a_lo, p.buf_rows, f1_hi, f1_lo, g.N1, g.KS1);
@@ -507,7 +508,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_forward(const XcParams p) {
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
             const int c = c8 * 8 + j;
-            if (c < g.RW) put1(s.a_hi, s.a_lo, p.buf_rows, t_of_warp * g.RW + c, y, v[j]);
+            if (c < g.RW && EBSD_DCHECK(t_of_warp * g.RW + c < p.buf_rows && y < 64 * p.buf_planes))
+              put1(s.a_hi, s.a_lo, p.buf_rows, t_of_warp * g.RW + c, y, v[j]);
           }
         }
       }
@@ -808,6 +810,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
         }
       }
       const int row_re = pr * g.RW + kx, row_im = row_re + g.KOB;
+      if (!EBSD_DCHECK(row_im < p.buf_rows && g.KOA + grp * 8 + 8 <= 64 * p.buf_planes)) continue;
       put8(s.a_hi, s.a_lo, p.buf_rows, row_re, grp * 8, er);
       put8(s.a_hi, s.a_lo, p.buf_rows, row_re, g.KOA + grp * 8, noi);
       put8(s.a_hi, s.a_lo, p.buf_rows, row_im, grp * 8, ei);
@@ -839,6 +842,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
   // D_A chunks -> [hi | lo] bf16 in place (this thread's lanes and columns only)
   auto convert = [&](int np) {
     for (int c8 = cg; c8 < np * rw8; c8 += 4) {
+      if (!EBSD_DCHECK(c8 * 8 + 8 <= 256)) break;  // warp-uniform
       float v[8];
       tmem_ld8(da + lane_off + (uint32_t)(c8 * 8), v);
       uint32_t w[8];
@@ -861,7 +865,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max_tm(const XcParams p) {
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         const int c8 = cg + 4 * j;
-        if (c8 < nb8) {
+        if (c8 < nb8 && EBSD_DCHECK(pr * g.NB + c8 * 8 + 8 <= 256)) {  // warp-uniform
           float v[8];
           tmem_ld8(db + lane_off + (uint32_t)(pr * g.NB + c8 * 8), v);
 #pragma unroll

@@ -51,6 +51,13 @@ extern "C" {
 /* Library version (major*10000 + minor*100 + patch). */
 int ebsd_version(void);
 
+/* Debug checks: in the library built with -DEBSD_CHECK, kernels test their
+ * computed shared-memory, TMEM and global offsets; a failed check records
+ * its source line and skips the access. Returns the first recorded line (0
+ * when none; the file name goes to `file`) and clears the records; -1 when
+ * the library was built without checks. */
+int ebsd_debug_check_line(char* file, size_t n);
+
 /* Copy the last error message of this host thread into buf (NUL-terminated).
  * Returns the full message length. */
 int ebsd_last_error(char* buf, size_t n);

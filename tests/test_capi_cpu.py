@@ -151,3 +151,10 @@ def test_noalloc_argument_checks_need_no_gpu():
         assert call(128, most + 1, k) == 1
         msg = _capi.last_error()
         assert "scratch" in msg and f"at most {most} padded queries" in msg, msg
+
+
+def test_check_build_query_without_checks_needs_no_gpu():
+    """The normal build reports that it carries no device checks (-1)."""
+    if _capi.LIB_PATH.endswith("_check.so"):
+        return
+    assert _capi.debug_check() == (-1, "")
