@@ -209,10 +209,12 @@ def wave_query_tiles(device, row_bytes: int = 0) -> int:
     the dictionary tiles in flight, a quarter of the SMs is used (37 tiles x
     4 ranges on a 148-SM B200), otherwise an eighth (18 x 8 = 144 CTAs).
     Measured at 128 x 128 px: bf16 rows (32 KB; 37 tiles are 151 MB) read
-    4.9x their operand bytes from DRAM per launch with 37 tiles and 2.0x
-    with 18, and the step ran 5.8 % faster in an A/B in one process; e4m3
-    rows (16 KB, 76 MB for 37 tiles) lose ~8 % with 18 tiles (fewer SMs,
-    no traffic to save). row_bytes 0 (unknown) takes the smaller count."""
+    4.9x their operand bytes from DRAM per launch with 37 tiles and 2.1x
+    with 18; in alternating runs of the full bench on one GPU the two shapes
+    came within about 1 % (18 tiles: 30 MHz more SM clock under the power
+    cap, four SMs idle), so the one that moves less data is used. e4m3 rows
+    (16 KB, 76 MB for 37 tiles) were ~2 % slower with 18 tiles (no traffic
+    to save). row_bytes 0 (unknown) takes the smaller count."""
     props = torch.cuda.get_device_properties(device)
     sms = props.multi_processor_count
     l2 = getattr(props, "L2_cache_size", 0) or (126 << 20)
