@@ -703,6 +703,16 @@ def run_ours(args, wl):
     peak = peaks.get("bf16_tflops_sustained", 1400.0)
     if args.precision == "fp8":
         peak = 2.0 * peak  # no measured fp8 denominator: twice the measured bf16
+    # the same kind of cuBLAS GEMM timed on this GPU in this run, under the
+    # same power cap: a second denominator beside the contract's peak
+    here = None
+    if n == 1 and args.precision == "bf16" and not args.no_companions:
+        try:
+            pk16 = gemm_peak_tflops("bf16", dev)
+            here = {"sustained": pk16["sustained"], "burst": pk16["burst"], "how": pk16["how"],
+                    "frac_of_sustained": achieved_tflops / pk16["sustained"]}
+        except Exception as exc:
+            here = {"sustained": None, "how": f"not measured ({exc})"}
     clk = clocks.summary()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": n, "steps": args.steps, "warmup": args.warmup,
@@ -722,6 +732,7 @@ def run_ours(args, wl):
                      "kernel": "k_tc_gemm (match + streaming top-k)",
                      "peak_source": f"{peak_kind} bf16_tflops_sustained" + (" x2 for fp8" if args.precision == "fp8"
                                                                              else ""),
+                     "peak_measured_here": here,
                      "share_of_step": match_share},
         "rescore": rescore,
         "accuracy": {"within_0.5deg_of_truth": within_half, "median_misori_deg": median_deg},
