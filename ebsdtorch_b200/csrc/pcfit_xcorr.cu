@@ -26,21 +26,23 @@
 //     with y' = y - H/2, x' = x - W/2 (the fftshift) and a_kx = 1 for the
 //     DC and Nyquist columns, 2 otherwise (the c2r Hermitian fold).
 //
-// Each stage is D[128 lanes, N] = A[128 rows, K] B[N rows, K]^T with the
-// constant DFT matrix as B (copied once per CTA into shared memory) and the
-// data as A, written by the CTA's threads into shared memory in the
-// 128-byte-swizzled K-major layout the MMA descriptors read. Between the
-// stages the TMEM result is read back (tcgen05.ld) and written transposed as
-// the next stage's A operand.
+// Each stage is D[128 lanes, N] = A[128 rows, K] B[N rows, K]^T. The
+// constant DFT matrices are built once per detector size and copied by each
+// CTA into shared memory; data operands are written by the CTA's threads in
+// the 128-byte-swizzled K-major layout the MMA descriptors read.
 //
-// k_xc_max: a CTA owns one experimental pattern and a slice of the batch;
-// per pass it correlates PP simulated patterns with it (PP * 2 WF rows in
-// stage A, PP * H rows in stage B), then the passes' maps (staged in shared
-// memory) are max-reduced per shift into registers (the first maximum wins
-// on ties, i.e. the smaller index). At the end each (shift, max, index) is
-// merged into a 64-bit key (ordered float bits, inverted index) with
-// atomicMax; ebsd_pcfit_fold applies the reference's running-best rule
+// The inverse kernels: a CTA owns one experimental pattern and a slice of
+// the batch and correlates PP simulated patterns with it per pass; the max
+// over pairs and passes is kept per shift in registers (the first maximum
+// wins on ties, i.e. the smaller index), and at the end each (shift, max,
+// index) is merged into a 64-bit key (ordered float bits, inverted index)
+// with atomicMax; ebsd_pcfit_fold applies the reference's running-best rule
 // (fitting.py:498-507) per batch and clears the keys.
+//   k_xc_max_tm (used when its operands fit shared memory, up to about
+//     96 x 96): stage A leaves its output in TMEM laid out as stage B's A
+//     operand (lanes y, K along the columns); passes are software-pipelined.
+//   k_xc_max (larger detectors): stage A's output is written transposed
+//     through shared memory and the pass's maps are staged there.
 //
 // Supported: enlarged detectors up to 127 x 127 (one 128-row tile per
 // image, K <= 128). Every wait is bounded; a timeout is reported in *status.
@@ -708,8 +710,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_xc_max(const XcParams p) {
   if (warp == 0) tmem_dealloc(tmem, 512);
 }
 
-// k_xc_max_tm: k_xc_max with stage A's output kept in TMEM as stage B's A
-// operand (no shared-memory transpose, no staged maps):
+// k_xc_max_tm: the inverse transforms with stage A's output kept in TMEM as
+// stage B's A operand (no shared-memory transpose, no staged maps):
 //   stage A  D_A[y, (pair, part, kx)] = CA[y, K] . Data[(pair, part, kx), K]^T
 //            with the constant (128 rows y) as the A operand and the pass's
 //            [E | O] rows as B (N = pairs * RW);
