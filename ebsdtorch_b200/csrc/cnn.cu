@@ -59,6 +59,41 @@ __global__ void k_im2col(const __nv_bfloat16* __restrict__ x, int H, int W, int 
   }
 }
 
+// The same for C % 8 == 0 with 16-byte aligned input: one thread per
+// (output pixel, tap) pair copies the tap's C channels in 16-byte chunks
+// (the pixel's coordinates decoded once per pair instead of once per chunk);
+// tap 9 writes the zero padding of K from 9 C to ld.
+__global__ void k_im2col_taps(const __nv_bfloat16* __restrict__ x, int H, int W, int C, int Ho, int Wo, int M,
+                              int r0, int n_rows, int ld, int ntap, __nv_bfloat16* __restrict__ cols) {
+  const unsigned total = (unsigned)n_rows * (unsigned)ntap;
+  const int hw = Ho * Wo, nc = C >> 3;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const int rl = (int)(t / (unsigned)ntap);
+    const int tap = (int)(t - (unsigned)rl * (unsigned)ntap);
+    const int r = r0 + rl;
+    uint4* dst = reinterpret_cast<uint4*>(cols + (int64_t)r * ld);
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    if (tap == 9) {  // K padding
+      for (int j = (9 * C) >> 3; j < (ld >> 3); ++j) dst[j] = zero;
+      continue;
+    }
+    const uint4* src = nullptr;
+    if (r < M) {
+      const int b = r / hw, rem = r - b * hw;
+      const int oy = rem / Wo, ox = rem - oy * Wo;
+      const int iy = 2 * oy - 1 + tap / 3, ix = 2 * ox - 1 + tap % 3;
+      if (iy >= 0 && iy < H && ix >= 0 && ix < W)
+        src = reinterpret_cast<const uint4*>(x + (((int64_t)b * H + iy) * W + ix) * C);
+    }
+    uint4* d = dst + tap * nc;
+    if (src) {
+      for (int j = 0; j < nc; ++j) d[j] = __ldg(src + j);
+    } else {
+      for (int j = 0; j < nc; ++j) d[j] = zero;
+    }
+  }
+}
+
 // Direct convolution of a single-channel input (the first layer):
 // out[(b, oy, ox), c] = act(sum_{ky,kx} x[b, 2 oy - 1 + ky, 2 ox - 1 + kx] w[c, 3 ky + kx] + bias[c]),
 // one thread per output pixel and all COUT channels, weights (bf16, as the
@@ -303,11 +338,18 @@ extern "C" int ebsd_cnn_im2col(const void* x, int B, int H, int W, int C, int64_
   const int vec = (C % 8 == 0) && (((uintptr_t)x & 15) == 0);
   const int64_t nj = ld / 8;
   const int64_t rows_per = std::max<int64_t>(1, (INT32_MAX / 2) / nj);
+  const int ntap = ld > 9 * C ? 10 : 9;
   for (int64_t r0 = 0; r0 < m_pad; r0 += rows_per) {
     const int n_rows = (int)std::min(rows_per, m_pad - r0);
-    k_im2col<<<nblocks((int64_t)n_rows * nj), 256, 0, CNN_STREAM>>>(
-        reinterpret_cast<const __nv_bfloat16*>(x), H, W, C, Ho, Wo, (int)M, (int)r0, n_rows, ld, vec,
-        reinterpret_cast<__nv_bfloat16*>(cols));
+    if (vec) {
+      k_im2col_taps<<<nblocks((int64_t)n_rows * ntap), 256, 0, CNN_STREAM>>>(
+          reinterpret_cast<const __nv_bfloat16*>(x), H, W, C, Ho, Wo, (int)M, (int)r0, n_rows, ld, ntap,
+          reinterpret_cast<__nv_bfloat16*>(cols));
+    } else {
+      k_im2col<<<nblocks((int64_t)n_rows * nj), 256, 0, CNN_STREAM>>>(
+          reinterpret_cast<const __nv_bfloat16*>(x), H, W, C, Ho, Wo, (int)M, (int)r0, n_rows, ld, vec,
+          reinterpret_cast<__nv_bfloat16*>(cols));
+    }
     EBSD_LAUNCH_CHECK();
   }
   return 0;

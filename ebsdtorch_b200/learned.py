@@ -125,12 +125,23 @@ class _Dense:
         self.gw = torch.zeros_like(self.w)
         self.gb = torch.zeros_like(self.b)
 
-    def forward(self, x: torch.Tensor, keep: dict):
+    def forward(self, x: torch.Tensor, keep: dict, tf32: bool = False):
+        """y = act(x W^T + b). tf32 (inference): the product on the tensor
+        cores (ebsd_gemm_f32) when the layer is wide, then bias and ReLU;
+        training keeps the FP32 SIMT kernel."""
         B = x.shape[0]
         y = torch.empty((B, self.nout), dtype=torch.float32, device=x.device)
         y16 = torch.empty((B, self.nout), dtype=torch.bfloat16, device=x.device) if self.relu else None
-        call("ebsd_cnn_dense_fwd", ptr(x), x.stride(0), ptr(self.w), ptr(self.b), B, self.nout, self.nin,
-             int(self.relu), ptr(y), ptr(y16), _stream(x))
+        if tf32 and self.nin >= 512 and self.nin % 4 == 0 and x.stride(1) == 1 and x.stride(0) % 4 == 0:
+            kernels.gemm_f32(x, self.w, y)
+            if self.relu:
+                call("ebsd_cnn_bias_act", ptr(y), self.nout, ptr(self.b), B, self.nout, 1, ptr(y16), self.nout,
+                     ptr(y), _stream(x))
+            else:
+                y += self.b
+        else:
+            call("ebsd_cnn_dense_fwd", ptr(x), x.stride(0), ptr(self.w), ptr(self.b), B, self.nout, self.nin,
+                 int(self.relu), ptr(y), ptr(y16), _stream(x))
         keep.update(x=x, y16=y16)
         return y
 
@@ -191,7 +202,7 @@ class OrientationCNN:
             if keep:
                 self._keep.append(saved)
         k1, k2 = {}, {}
-        hid = self.fc1.forward(a32.view(B, -1), k1)
+        hid = self.fc1.forward(a32.view(B, -1), k1, tf32=not keep)
         out = self.fc2.forward(hid, k2)
         if keep:
             self._keep += [k1, k2]

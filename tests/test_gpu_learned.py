@@ -90,11 +90,13 @@ def test_cnn_gradients_match_oracle():
     assert report["fc2.b"][1] < 1e-5  # FP32 head: exact
 
 
-@pytest.mark.parametrize("cin,cout,hw,batch", [(1, 32, 64, 1024), (64, 128, 16, 256), (256, 256, 8, 128)])
+@pytest.mark.parametrize("cin,cout,hw,batch", [(1, 32, 64, 1024), (64, 128, 16, 256), (256, 256, 8, 128),
+                                                (32, 64, 32, 256), (64, 128, 15, 64)])
 def test_conv_forward_matches_fp32_convolution(cin, cout, hw, batch):
     """Fused im2col GEMM + bias + ReLU (ebsd_cnn_conv_fwd) against an FP32
     convolution of the same bf16-rounded input and weights; the first case
-    streams ~14 pixel tiles per work unit, the last uses two channel tiles."""
+    streams ~14 pixel tiles per work unit, the third uses two channel tiles,
+    the fourth pads K (288 -> 320), the last has an odd input size."""
     from ebsdtorch_b200.learned import _Conv
 
     gen = torch.Generator().manual_seed(cin + cout)
