@@ -662,7 +662,10 @@ def run_ours(args, wl):
         companions = {"pca": pca_block(args, wl, mp, geom, truth, pats, dev),
                       "refine": refine_block(args, wl, mp, geom, truth, pats, di_ori, dev, min(args.steps, 3))}
         del di_ori
-        short = argparse.Namespace(**{**vars(args), "no_cpu_baseline": True})
+        # the companions' CPU baselines only where the reference itself runs
+        # (bounded samples of a few seconds each)
+        short = argparse.Namespace(**{**vars(args), "no_cpu_baseline": args.no_cpu_baseline or
+                                      not _reference_staged()})
         companions["preprocess"] = run_preprocess(short)
         companions["pcfit"] = run_pcfit(short)
 
@@ -929,6 +932,12 @@ def refine_block(args, wl, mp, geom, truth, pats, di_ori, dev, steps) -> dict:
                                         "refined_within_0.5": float((after < 0.5).float().mean())},
         "clocks": clocks.summary(),
     }
+    if not args.no_cpu_baseline and _reference_staged():
+        from oracle import ref_baselines as RB
+
+        m = 256  # a bounded sample of the same patterns and starting orientations
+        line["cpu_baseline"] = RB.refine_cpu(mp.master_pattern.cpu(), wl["det"], pats[:m].float().cpu(),
+                                             di_ori[:m].float().cpu(), wl["res"])
     del exp
     return line
 
@@ -1108,7 +1117,12 @@ def run_preprocess(args):
                               "average_frac": pairs / (kern["nlpar_average"] / 1e3) / smem_pairs_peak},
         "clocks": clocks.summary(),
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and _reference_staged():
+        from oracle import ref_baselines as RB
+
+        # a 64 x 64 crop of the same scan (4,096 patterns)
+        line["cpu_baseline"] = RB.preprocess_cpu(host_in[:64, :64].float(), cfg["k_rad"], 0.375)
+    elif not args.no_cpu_baseline:
         r, csecs = preprocess_cpu_rate(cfg)
         line["cpu_baseline"] = {"value": r, "unit": UNIT, "cores": 1, "kind": "port",
                                 "sample": "oracle (NumPy float64) standard_clean + nlpar k_rad 3 on a 24 x 24 crop "
@@ -1254,7 +1268,16 @@ def run_pcfit(args):
                      "flops": "bf16 tensor FLOPs of the 3-term split, unpadded: 6 (4 WF H H2 + 2 H W WF) per pair"},
         "clocks": clocks.summary(),
     }
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and _reference_staged():
+        from oracle import ref_baselines as RB
+
+        kw_ref = dict(pc_x_min=cfg["x"][0], pc_x_max=cfg["x"][1], pc_y_min=cfg["y"][0], pc_y_max=cfg["y"][1],
+                      pc_z_min=cfg["z"][0], pc_z_max=cfg["z"][1], pc_z_steps=cfg["z"][2], primary_tilt_deg=70.0,
+                      secondary_tilt_deg=0.0, dictionary_resolution_deg=cfg["res"],
+                      dictionary_indexing_batch_size=cfg["bs"])
+        torch.manual_seed(0)
+        line["cpu_baseline"] = RB.pcfit_cpu(mp_t.cpu(), pats.cpu(), kw_ref, z_steps)
+    elif not args.no_cpu_baseline:
         from oracle import di_oracle as O
 
         q64 = quats[:64].double().cpu().numpy()

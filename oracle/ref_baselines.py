@@ -5,9 +5,12 @@ arm, the ``cpu_baseline`` object and the plain-FP32-GPU-DI comparison). The
 product path never imports it. The reference is loaded from ``oracle/_ref``
 (staged by ``oracle/stage_ref.py``) through ``oracle/ref_loader.py``.
 
-Both baselines call the reference's public ``dictionary_index_orientations``
-(ebsdtorch/ebsd/indexing.py:14-211) unmodified, with its own MasterPattern,
-EBSDGeometry and ExperimentPatterns objects.
+The indexing baselines call the reference's public
+``dictionary_index_orientations`` (ebsdtorch/ebsd/indexing.py:14-211)
+unmodified, with its own MasterPattern, EBSDGeometry and ExperimentPatterns
+objects; the baselines of the steps either side of indexing (pattern-centre
+fitting, preprocessing, grid refinement; end of this file) call the
+reference's own functions for those steps the same way, on bounded samples.
 
 The reference's cost of one call is affine in the query count at a fixed
 dictionary: T(Q) = alpha + beta * Q, where alpha is the dictionary projection
@@ -222,3 +225,108 @@ def fp32_gpu_di(mp_tensor, det, pats, res: float, k: int, q_full: int,
     return {"rate": rate, "best_chunks": {"dictionary_chunk_size": best[0], "experiment_chunk_size": best[1]},
             "sweep_at": qa, "sweep": rows, "second_point": {"patterns": qb, "seconds": t_b},
             "projection_s": alpha, "per_pattern_s": beta, "top1_quats": top1}
+
+
+# ---------------------------------------------------------------------------
+# host-CPU baselines of the steps either side of indexing, each a bounded
+# sample of the bench's workload run through the reference's own function
+# ---------------------------------------------------------------------------
+
+def _all_threads() -> int:
+    import torch
+
+    n = host_threads()
+    torch.set_num_threads(n)
+    return n
+
+
+def fitting_module():
+    """The reference's ebsd/fitting.py. It imports matplotlib (for a plotting
+    helper) and, through io/read_master_pattern.py, h5py; the fitter uses
+    neither, so empty stand-in modules are registered when they are absent."""
+    import sys
+    import types
+
+    ref_loader.import_reference()
+    for name in ("matplotlib", "matplotlib.pyplot", "h5py"):
+        try:
+            __import__(name)
+        except ImportError:
+            sys.modules[name] = types.ModuleType(name)
+    sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
+    from ebsdtorch.ebsd import fitting
+
+    return fitting
+
+
+def pcfit_cpu(mp_tensor_cpu, pats_cpu, kw: Dict, z_steps: int) -> Dict:
+    """The reference's spatial_fft_pc_fitter (fitting.py:359-540) on the
+    host's threads for one pc_z step over the whole dictionary; a fit visits
+    z_steps such steps, so the rate is 1 / (seconds * z_steps)."""
+    import contextlib
+    import io
+
+    F = fitting_module()
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+
+    cores = _all_threads()
+    kw1 = dict(kw, pc_z_steps=1, pc_z_max=kw["pc_z_min"])
+    mp = MasterPattern(mp_tensor_cpu.clone(), laue_group=11)
+    with ref_loader.quiet_stdout(), contextlib.redirect_stderr(io.StringIO()):
+        t0 = time.perf_counter()
+        F.spatial_fft_pc_fitter(mp, pats_cpu.clone(), **kw1)
+        secs = time.perf_counter() - t0
+    return {"value": 1.0 / (secs * z_steps), "unit": "fits/s", "cores": cores, "kind": "reference",
+            "cpu_model": cpu_model(),
+            "sample": "the reference's spatial_fft_pc_fitter on the host CPU (%d threads), one pc_z step over the "
+                      "whole dictionary (%.1f s), times %d steps" % (cores, secs, z_steps)}
+
+
+def preprocess_cpu(counts_cpu, k_rad: int, coeff: float) -> Dict:
+    """The reference's standard_clean (experiment_pats.py:285-295) and nlpar
+    (nlpar.py:21-192) on the host's threads, on a (scan_h, scan_w, h, w)
+    crop of detector counts; rate in patterns/s."""
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.preprocessing.nlpar import nlpar
+
+    ref_loader.import_reference()
+    cores = _all_threads()
+    sh, sw, h, w = counts_cpu.shape
+    t0 = time.perf_counter()
+    e = ExperimentPatterns(counts_cpu.reshape(sh * sw, h, w).float().clone())
+    e.standard_clean()
+    nlpar(e.patterns.view(sh, sw, h, w), k_rad=k_rad, coeff=coeff)
+    secs = time.perf_counter() - t0
+    return {"value": sh * sw / secs, "unit": "patterns/s", "cores": cores, "kind": "reference",
+            "cpu_model": cpu_model(),
+            "sample": "the reference's standard_clean + nlpar (k_rad %d) on the host CPU (%d threads), a %d x %d "
+                      "crop of the scan (%.1f s)" % (k_rad, cores, sh, sw, secs)}
+
+
+def refine_cpu(mp_tensor_cpu, det, pats_cpu, start_cpu, semi_edge_deg: float, n_iter: int = 3,
+               radius: int = 1) -> Dict:
+    """The reference's orientation_grid_refinement (refining.py:71-244) on
+    the host's threads, FP32 matching, on the given patterns; patterns/s."""
+    import contextlib
+    import io
+
+    import torch
+
+    ref_loader.import_reference()
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.ebsd.refining import orientation_grid_refinement
+
+    cores = _all_threads()
+    mp, geom = _reference_objects(mp_tensor_cpu, det)
+    n = pats_cpu.shape[0]
+    exp = ExperimentPatterns(pats_cpu.clone())
+    exp.set_orientations(start_cpu.clone())
+    exp.phases = torch.zeros(n, dtype=torch.int64)
+    with ref_loader.quiet_stdout(), contextlib.redirect_stderr(io.StringIO()):
+        t0 = time.perf_counter()
+        orientation_grid_refinement(mp, geom, exp, grid_semi_edge_in_degrees=semi_edge_deg, batch_size=n,
+                                    n_iter=n_iter, kernel_radius_in_steps=radius, match_dtype=torch.float32)
+        secs = time.perf_counter() - t0
+    return {"value": n / secs, "unit": "patterns/s", "cores": cores, "kind": "reference", "cpu_model": cpu_model(),
+            "sample": "the reference's orientation_grid_refinement on the host CPU (%d threads, FP32), %d patterns "
+                      "(%.1f s)" % (cores, n, secs)}
