@@ -286,10 +286,10 @@ def preprocess_cpu(counts_cpu, k_rad: int, coeff: float) -> Dict:
     """The reference's standard_clean (experiment_pats.py:285-295) and nlpar
     (nlpar.py:21-192) on the host's threads, on a (scan_h, scan_w, h, w)
     crop of detector counts; rate in patterns/s."""
+    ref_loader.import_reference()
     from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
     from ebsdtorch.preprocessing.nlpar import nlpar
 
-    ref_loader.import_reference()
     cores = _all_threads()
     sh, sw, h, w = counts_cpu.shape
     t0 = time.perf_counter()
