@@ -19,7 +19,9 @@ outputs of one case (``--refinement-only`` / ``--preprocessing-only`` /
 pcfit.npz / emsoft_reader.npz; ``--config0-only`` writes config0.npz, the
 reference's own plain DI at the small configuration on inputs rebuilt by
 ``config0_inputs.py``; ``--euclidean-only`` writes di_euclid.npz, plain DI with
-the euclidean distance). The files are small (< 1 MB each) and committed.
+the euclidean distance; ``--pca-config0-only`` writes pca_config0.npz, the
+reference's own PCA DI on the config-0 inputs). The files are small (< 1 MB
+each) and committed.
 """
 
 from __future__ import annotations
@@ -325,6 +327,55 @@ def config0_goldens(root=None):
         case=np.array(repr(sorted(c.items()))))
 
 
+PCA_CONFIG0 = dict(n_components=256, learn_res=2.0)
+
+
+def pca_config0_goldens(root=None):
+    """The reference's own PCA DI at the small configuration: the inputs of
+    config0_inputs.py, the 256 leading components (indexing.py:355 with the
+    "top" slice) learned on the m-3m 2.0 deg dictionary (4,344 rows),
+    indexing the 1.0 deg dictionary (36,829 rows), top-4, FP32 matching.
+    Commits the per-pattern top-4 indices (into the permuted index
+    dictionary) and metrics."""
+    import config0_inputs as C
+
+    _, ref_top = load_reference(root)
+    from ebsdtorch.ebsd.experiment_pats import ExperimentPatterns
+    from ebsdtorch.ebsd.geometry import EBSDGeometry
+    from ebsdtorch.ebsd.master_pattern import MasterPattern
+    from ebsdtorch.s2_and_so3.laue_fz_ori import sample_ori_fz_laue_angle
+
+    c, pc = C.CASE, PCA_CONFIG0
+    inp = C.make_inputs(c)
+    mp = MasterPattern(torch.from_numpy(inp["master_pattern"]).clone(), laue_group=11)
+    geom = EBSDGeometry(c["det"], tilts_degrees=c["tilts"], proj_center=c["pc"])
+    exp = ExperimentPatterns(torch.from_numpy(inp["counts"].astype(np.float32)))
+    torch.manual_seed(c["perm_seed"])
+    with ref_loader.quiet_stdout():
+        ref_top.pca_dictionary_index_orientations(
+            mp, geom, exp, n_pca_components=pc["n_components"], dictionary_resolution_learn_deg=pc["learn_res"],
+            dictionary_resolution_index_deg=c["res"], top_k_matches=c["k"],
+            dictionary_chunk_size=c["dictionary_chunk_size"], experiment_chunk_size=c["experiment_chunk_size"],
+            match_dtype=torch.float32, quantized_via_ao=False)
+    quats_k, metrics_k = exp.raw_indexing_results[0]
+    # the same draws: the learning dictionary's permutation, then the index dictionary's
+    torch.manual_seed(c["perm_seed"])
+    sample_ori_fz_laue_angle(11, pc["learn_res"], torch.device("cpu"), permute=True)
+    dictionary = sample_ori_fz_laue_angle(11, c["res"], torch.device("cpu"), permute=True).numpy()
+    lookup = {row.tobytes(): i for i, row in enumerate(dictionary)}
+    q = quats_k.numpy()
+    idx = np.array([[lookup[q[i, j].tobytes()] for j in range(q.shape[1])] for i in range(q.shape[0])],
+                   dtype=np.int32)
+    np.savez_compressed(
+        os.path.join(HERE, "pca_config0.npz"),
+        indices=idx, metrics=metrics_k.numpy().astype(np.float32),
+        n_dictionary=np.array([dictionary.shape[0]]), n_components=np.array([pc["n_components"]]),
+        learn_res=np.array([pc["learn_res"]]),
+        sha256_master_pattern=np.array(inp["sha256_master_pattern"]),
+        sha256_counts=np.array(inp["sha256_counts"]),
+        case=np.array(repr(sorted(c.items()))))
+
+
 def euclidean_goldens(root=None):
     """The reference's plain DI with distance_metric="euclidean" (knn.py:85-91,
     squared distance of the zero-mean rows) and "manhattan" (:92-93, L1
@@ -614,6 +665,8 @@ if __name__ == "__main__":
         config0_goldens(*args[1:])
     elif args and args[0] == "--euclidean-only":
         euclidean_goldens(*args[1:])
+    elif args and args[0] == "--pca-config0-only":
+        pca_config0_goldens(*args[1:])
     else:
         main(*args)
         refinement_goldens(*args)
