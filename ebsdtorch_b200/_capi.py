@@ -38,6 +38,8 @@ SIGNATURES = {
     "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
     "ebsd_match_auto_splits": (i32, [i64, i64]),
     "ebsd_set_wait_limit_ns": (i64, [i64]),
+    "ebsd_set_match_pairs": (i32, [i32]),
+    "ebsd_match_pair_max_clusters": (i32, []),
     "ebsd_manhattan_topk": (i32, [vp, i64, i64, i64, vp, i64, i64, i32, i32, i32, vp, vp, i32, i32, i32, vp]),
     "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
     "ebsd_match_topk_tiled": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, vp, vp, i32, i32, vp, vp, i32, i32, i32,
@@ -134,6 +136,10 @@ def load() -> C.CDLL:
                 fn = getattr(lib, name)
                 fn.restype = res
                 fn.argtypes = args
+            # EBSD_MATCH_PAIRS=0/1 sets the match kernels' CTA-pair mode
+            pairs = os.environ.get("EBSD_MATCH_PAIRS")
+            if pairs is not None:
+                lib.ebsd_set_match_pairs(0 if pairs.strip() in ("", "0") else 1)
             _lib = lib
     return _lib
 

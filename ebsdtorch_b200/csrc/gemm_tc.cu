@@ -49,6 +49,7 @@ struct Tile {
 };
 
 struct GemmParams {
+  int m_tiles;  // query tiles with rows (the pair kernel's odd CTA may have none)
   int n_tiles;
   int splits;
   int units;  // m_tiles * splits; a CTA takes units blockIdx.x, + gridDim.x, ...
@@ -459,6 +460,310 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Pair variant of the top-k match (angular ranking, 256-row dictionary
+// tiles, non-persistent). The two CTAs of a cluster take two consecutive
+// query tiles and the same dictionary range; the even CTA issues
+// tcgen05.mma.cta_group::2 with M = 256 (the two query tiles) and N = 256.
+// Each CTA stages its own 128 query rows and HALF of each 256-row dictionary
+// tile (rows rank * 128 ...), so a CTA moves 32 KB per K step instead of
+// 48 KB (the dictionary tile is read once per pair, not once per CTA), and
+// each CTA's TMEM receives its 128 query rows x 256 dictionary columns for
+// the same top-k epilogue as k_tc_gemm.
+//
+// Barriers (every wait bounded; per CTA unless noted):
+//   full[s]       even CTA: stage s of BOTH CTAs landed. The even CTA's
+//                 producer expects both CTAs' bytes; both CTAs' copies
+//                 (cp.async.bulk.tensor .cta_group::2) signal this barrier.
+//   empty[s]      the even CTA's MMA commit, multicast to both CTAs
+//   accf[a]       accumulator a complete: commit multicast to both CTAs
+//   acce[a]       even CTA: accumulator a drained, 8 arrivals (4 epilogue
+//                 warps x 2 CTAs)
+// The MMA thread's waits are CTA-scoped waits on its own barriers. The pair
+// ends with a cluster barrier so that neither CTA exits (and frees its
+// shared memory or TMEM) while the other may still reach it.
+// ---------------------------------------------------------------------------
+constexpr int PAIR_STAGES = 6;
+constexpr int PAIR_B_BYTES = 128 * BKB;
+constexpr int PAIR_STAGE_BYTES = A_BYTES + PAIR_B_BYTES;
+constexpr int PAIR_BAR_BYTES = 8 * (2 * PAIR_STAGES + 4 + 1) + 16;
+constexpr int PAIR_SMEM_BYTES = 1024 + PAIR_STAGES * PAIR_STAGE_BYTES + SCRATCH_BYTES + PAIR_BAR_BYTES;
+constexpr uint32_t PAIR_TMEM_COLS = 512;  // two 128 x 256 FP32 accumulators per CTA
+static_assert(PAIR_SMEM_BYTES <= 232448, "shared memory budget");
+
+template <int KIND>
+__host__ __device__ constexpr uint32_t make_idesc_pair() {
+  // as make_idesc, with M = 256 (both CTAs' query tiles) and N = 256
+  return (1u << 4) | (KIND == 0 ? ((1u << 7) | (1u << 10)) : 0u) | ((uint32_t)(256 >> 3) << 17) |
+         ((uint32_t)(256 >> 4) << 24);
+}
+
+template <int KIND, int KC>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
+    k_tc_gemm_pair(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const GemmParams p) {
+  constexpr int STAGES = PAIR_STAGES;
+  constexpr int STAGE_BYTES = PAIR_STAGE_BYTES;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_s = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
+  const uint32_t sbase = smem_u32(smem);
+  float* scratch = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + SCRATCH_BYTES);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+  auto accf_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + a); };
+  auto acce_bar = [&](int a) { return bar0 + 8u * (2 * STAGES + 2 + a); };
+  const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 5);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const bool leader = rank == 0;
+  // unit of this pair -> (pair of query tiles, dictionary tile range)
+  const int u = (int)(blockIdx.x >> 1);
+  const int n_splits = p.splits;
+  const int pair_tile = u / n_splits;
+  const int split = u - pair_tile * n_splits;
+  const int m_tile = 2 * pair_tile + (int)rank;
+  const int n_begin = (int)((int64_t)split * p.n_tiles / n_splits);
+  const int n_end = (int)((int64_t)(split + 1) * p.n_tiles / n_splits);
+  const int k_iters = p.k_iters;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(accf_bar(a), 1);
+      mbar_init(acce_bar(a), 8);
+    }
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) tmem_alloc_pair(smem_u32(tmem_slot), PAIR_TMEM_COLS);
+  __syncwarp();
+  tc_fence_before();
+  // both CTAs' barriers are initialised before any arrival from the peer
+  cluster_sync_all();
+  tc_fence_after();
+  const uint32_t tmem_base = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+  const uint64_t wait_ns = p.wait_ns;
+  uint32_t prod_stage = 0, prod_phase = 0;
+  int64_t issued = 0;
+  bool prod_ok = true, any_mma = false;
+
+  if (warp == 0) {
+    // ---------------- TMA producer (both CTAs) ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      const int a_row = m_tile * BM;
+      const uint32_t full0 = mapa_shared(full_bar(0), 0);  // the even CTA's full[0]
+      for (int n = n_begin; n < n_end && prod_ok; ++n) {
+        const int b_row = n * 256 + (int)rank * 128;
+        for (int k = 0; k < k_iters; ++k) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, wait_ns)) {
+            prod_ok = false;
+            break;
+          }
+          const uint32_t a_dst = sbase + stage * STAGE_BYTES;
+          if (leader) mbar_arrive_expect_tx(full_bar(stage), 2 * STAGE_BYTES);
+          const int kx = k * (BKB / kind_elem_bytes<KIND>());
+          tma_load_2d_pair(a_dst, &tmA, kx, a_row, full0 + 8u * stage);
+          tma_load_2d_pair(a_dst + A_BYTES, &tmB, kx, b_row, full0 + 8u * stage);
+          ++issued;
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (!prod_ok) report_timeout(p, abort_flag);
+      prod_stage = stage;
+      prod_phase = phase;
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0 && leader) {
+      // ---------------- MMA issuer (even CTA) ----------------
+      uint32_t stage = 0, phase = 0;
+      bool ok = true;
+      {
+        int acc = 0;
+        uint32_t acc_phase = 0;
+        constexpr uint32_t idesc = make_idesc_pair<KIND>();
+        for (int n = n_begin; n < n_end && ok; ++n) {
+          if (!mbar_wait_cluster(acce_bar(acc), acc_phase ^ 1u, abort_flag, wait_ns)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t d_tmem = tmem_base + (uint32_t)(acc * 256);
+          for (int k = 0; k < k_iters; ++k) {
+            if (!mbar_wait(full_bar(stage), phase, abort_flag, wait_ns)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t a_addr = sbase + stage * STAGE_BYTES;
+            const uint32_t b_addr = a_addr + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < BKB / 32; ++kk) {
+              tc_mma_pair<KIND>(d_tmem, smem_desc_sw128(a_addr + kk * 32), smem_desc_sw128(b_addr + kk * 32), idesc,
+                                (k | kk) != 0 ? 1u : 0u);
+            }
+            any_mma = true;
+            tc_commit_pair_mc(empty_bar(stage), 0x3);
+            if (++stage == STAGES) {
+              stage = 0;
+              phase ^= 1u;
+            }
+          }
+          if (!ok) break;
+          tc_commit_pair_mc(accf_bar(acc), 0x3);
+          if (++acc == 2) {
+            acc = 0;
+            acc_phase ^= 1u;
+          }
+        }
+      }
+      if (!ok) report_timeout(p, abort_flag);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue (both CTAs) ----------------
+    const int wq = warp & 3;
+    const int etid = threadIdx.x - 64;
+    const int row = wq * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(wq * 32) << 16;
+    const uint32_t acce0 = mapa_shared(acce_bar(0), 0);
+    float bv[KC];
+    int bi[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      bv[j] = -INFINITY;
+      bi[j] = -1;
+    }
+    int acc = 0;
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    for (int n = n_begin; n < n_end; ++n) {
+      bool got = mbar_wait_sleep(accf_bar(acc), acc_phase, abort_flag, wait_ns);
+      got = __all_sync(0xffffffffu, got);
+      if (!got) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t tile_col = (int64_t)n * 256;
+#pragma unroll 1
+      for (int c = 0; c < 256 / 32; ++c) {
+        __syncwarp();
+        float v[32];
+        tmem_ld32(tmem_base + lane_addr + (uint32_t)(acc * 256 + c * 32), v);
+        const int64_t col0 = tile_col + c * 32;
+        uint32_t mask = 0;
+        const float thr = bv[KC - 1];
+        if (col0 + 32 <= p.n_valid) {
+          if (p.col_scale) {
+            const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
+#pragma unroll
+            for (int j4 = 0; j4 < 8; ++j4) {
+              const float4 s4 = __ldg(cs + j4);
+              v[4 * j4 + 0] *= s4.x;
+              v[4 * j4 + 1] *= s4.y;
+              v[4 * j4 + 2] *= s4.z;
+              v[4 * j4 + 3] *= s4.w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const bool valid = col0 + j < p.n_valid;
+            const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
+            v[j] = valid ? v[j] * sc : -INFINITY;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
+        if (mask) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) scratch[j * EPI_THREADS + etid] = v[j];
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const float sc = scratch[j * EPI_THREADS + etid];
+            if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
+          }
+        }
+      }
+      // this warp's TMEM reads are complete: one arrival per warp on the
+      // even CTA's acce[acc]
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive_cluster(acce0 + 8u * acc);
+      if (++acc == 2) {
+        acc = 0;
+        acc_phase ^= 1u;
+      }
+    }
+    if (ok && m_tile < p.m_tiles) {
+      const int64_t q = (int64_t)m_tile * BM + row;
+      const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        p.part_val[base + j] = bv[j];
+        p.part_idx[base + j] = bi[j];
+      }
+    }
+    if (!ok && lane == 0) report_timeout(p, abort_flag);
+  }
+
+  __syncthreads();
+  if (warp == 0 && lane == 0) {
+    // On the normal path: wait for the even CTA's last commits to this CTA's
+    // empty barriers, so that no arrival reaches this CTA's shared memory
+    // after the cluster barrier below. After a give-up: the even CTA waits
+    // for the pair's copies still in flight (they all signal its full
+    // barriers; a phase whose copies were never all issued ends the drain at
+    // the default limit), and the odd CTA, which cannot observe its copies,
+    // is held at the cluster barrier until then.
+    volatile int never = 0;
+    const bool aborted = *abort_flag != 0;
+    const int64_t last = issued < STAGES ? issued : (int64_t)STAGES;
+    uint32_t s = prod_stage, ph = prod_phase;
+    for (int64_t i = 0; i < last && (leader || !aborted); ++i) {
+      if (s == 0) {
+        s = STAGES - 1;
+        ph ^= 1u;
+      } else {
+        --s;
+      }
+      if (!mbar_wait(aborted ? full_bar(s) : empty_bar(s), ph, &never)) break;
+    }
+  } else if (warp == 1 && lane == 0 && leader && any_mma && *abort_flag) {
+    tc_commit_pair(drain_bar);
+    volatile int never = 0;
+    mbar_wait(drain_bar, 0, &never);
+  }
+  __syncwarp();
+  tc_fence_before();
+  cluster_sync_all();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, PAIR_TMEM_COLS);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 
@@ -552,6 +857,37 @@ static int launch(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& 
   return 0;
 }
 
+template <int KIND, int KC>
+static int launch_pair_kc(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p_in, int grid,
+                          cudaStream_t s) {
+  auto kern = k_tc_gemm_pair<KIND, KC>;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM_BYTES));
+  GemmParams p = p_in;
+  p.wait_ns = wait_limit_ns();
+  kern<<<grid, THREADS, PAIR_SMEM_BYTES, s>>>(a, b, p);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int KIND>
+static int launch_pair(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
+                       cudaStream_t s) {
+  switch (kc) {
+    case 1: return launch_pair_kc<KIND, 1>(a, b, p, grid, s);
+    case 2: return launch_pair_kc<KIND, 2>(a, b, p, grid, s);
+    case 4: return launch_pair_kc<KIND, 4>(a, b, p, grid, s);
+    case 8: return launch_pair_kc<KIND, 8>(a, b, p, grid, s);
+    case 16: return launch_pair_kc<KIND, 16>(a, b, p, grid, s);
+    case 32: return launch_pair_kc<KIND, 32>(a, b, p, grid, s);
+    case 64: return launch_pair_kc<KIND, 64>(a, b, p, grid, s);
+  }
+  set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
+  return EBSD_ERR_ARG;
+}
+
+// Whether eligible top-k matches run as CTA pairs (ebsd_set_match_pairs).
+static std::atomic<int> g_match_pairs{0};
+
 template <int KIND, int BN, bool PERSIST, bool BIAS = false>
 static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
                        int grid, cudaStream_t s) {
@@ -610,6 +946,31 @@ extern "C" int64_t ebsd_set_wait_limit_ns(int64_t ns) {
   return prev ? (int64_t)prev : (int64_t)kWaitLimitNs;
 }
 
+extern "C" int ebsd_set_match_pairs(int on) {
+  if (on < 0) return g_match_pairs.load();
+  return g_match_pairs.exchange(on ? 1 : 0);
+}
+
+extern "C" int ebsd_match_pair_max_clusters(void) {
+  // every instantiation has the same block, cluster and shared-memory size
+  auto kern = k_tc_gemm_pair<0, 32>;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, PAIR_SMEM_BYTES));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * 1024);
+  cfg.blockDim = dim3(THREADS);
+  cfg.dynamicSmemBytes = PAIR_SMEM_BYTES;
+  cudaLaunchAttribute attr;
+  attr.id = cudaLaunchAttributeClusterDimension;
+  attr.val.clusterDim.x = 2;
+  attr.val.clusterDim.y = 1;
+  attr.val.clusterDim.z = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  EBSD_CUDA_CHECK(cudaOccupancyMaxActiveClusters(&n, kern, &cfg));
+  return n;
+}
+
 extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
   // One wave: query tiles x dictionary ranges ~= number of SMs, so all units
   // start and finish together. Measured on B200 at 128^2 px x 328,720 rows:
@@ -648,10 +1009,18 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
                  "part_slots (%d) < slot_base (%d) + splits (%d)", part_slots, slot_base, splits);
   const int64_t m_tiles = n_queries_pad / BM;
   EBSD_ARG_CHECK(m_tiles * splits < INT32_MAX, "too many work units");
+  // max_ctas > 0 and fewer CTAs than units: persistent launch, each CTA
+  // loops over its units. Otherwise, with pairs switched on, 256-row tiles,
+  // the angular ranking and an even number of query tiles, one cluster of
+  // two CTAs takes two query tiles and a dictionary range.
+  const bool persist = max_ctas > 0 && max_ctas < m_tiles * splits;
+  const bool pair = g_match_pairs.load(std::memory_order_relaxed) && !persist && tile_n == 256 && !col_bias &&
+                    m_tiles % 2 == 0;
   CUtensorMap ta, tb;
   if (int rc = make_tmap(&ta, queries_lp, lp_dtype, n_queries_pad, k_pad, BM)) return rc;
-  if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, tile_n)) return rc;
+  if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, pair ? tile_n / 2 : tile_n)) return rc;
   GemmParams p{};
+  p.m_tiles = (int)m_tiles;
   p.n_tiles = n_tiles;
   p.splits = splits;
   p.units = (int)(m_tiles * splits);
@@ -666,11 +1035,13 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   p.slot_base = slot_base;
   p.index_base = index_base;
   p.status = d_status;
-  // max_ctas > 0 and fewer CTAs than units: persistent launch, each CTA
-  // loops over its units
-  const bool persist = max_ctas > 0 && max_ctas < p.units;
-  const int grid = persist ? max_ctas : p.units;
   cudaStream_t s = as_stream(stream);
+  if (pair) {
+    p.units = (int)(m_tiles / 2 * splits);
+    return lp_dtype == EBSD_DT_BF16 ? launch_pair<0>(n_cand, ta, tb, p, 2 * p.units, s)
+                                    : launch_pair<1>(n_cand, ta, tb, p, 2 * p.units, s);
+  }
+  const int grid = persist ? max_ctas : p.units;
   return lp_dtype == EBSD_DT_BF16 ? launch_topk_shape<0>(n_cand, tile_n, persist, ta, tb, p, grid, s)
                                   : launch_topk_shape<1>(n_cand, tile_n, persist, ta, tb, p, grid, s);
 }

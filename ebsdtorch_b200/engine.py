@@ -219,9 +219,12 @@ def wave_query_tiles(device, row_bytes: int = 0) -> int:
     sms = props.multi_processor_count
     l2 = getattr(props, "L2_cache_size", 0) or (126 << 20)
     quarter = max(1, sms // 4)
-    if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2) // 3:
-        return quarter
-    return max(1, sms // 8)
+    tiles = quarter if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2) // 3 else max(1, sms // 8)
+    # CTA-pair launches take query tiles two at a time (an odd count runs the
+    # one-CTA kernel)
+    if tiles > 1 and tiles % 2 and kernels.match_pairs():
+        tiles -= 1
+    return tiles
 
 
 def default_budget(device) -> int:

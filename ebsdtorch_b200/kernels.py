@@ -157,6 +157,18 @@ def avg_pool(x: torch.Tensor, binning: int) -> torch.Tensor:
 # ---------------------------------------------------------- A9/A10 matching
 
 
+def set_match_pairs(on: bool) -> bool:
+    """Run the eligible top-k matches that follow as CTA pairs (two CTAs of
+    a cluster share one M = 256 tcgen05.mma.cta_group::2 and each stages half
+    of every dictionary tile); returns the previous setting."""
+    return bool(_capi.load().ebsd_set_match_pairs(1 if on else 0))
+
+
+def match_pairs() -> bool:
+    """Whether eligible top-k matches run as CTA pairs."""
+    return bool(_capi.load().ebsd_set_match_pairs(-1))
+
+
 def auto_splits(n_queries_pad: int, n_dict_pad: int) -> int:
     return int(_capi.load().ebsd_match_auto_splits(n_queries_pad, n_dict_pad))
 

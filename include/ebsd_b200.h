@@ -182,6 +182,18 @@ int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad);
  * Meant for tests and for callers that want a tighter watchdog. */
 int64_t ebsd_set_wait_limit_ns(int64_t ns);
 
+/* No counterpart in the reference: on != 0 runs the top-k matches launched
+ * after the call as CTA pairs where they can (256-row dictionary tiles, the
+ * angular ranking, an even number of 128-row query tiles and no persistent
+ * launch): the two CTAs of a cluster share one tcgen05.mma.cta_group::2 of
+ * M = 256 query rows, and each stages half of every dictionary tile. Results
+ * and the partial-result layout are the same as the one-CTA kernel's.
+ * Returns the previous setting (0 by default); on < 0 only returns it. */
+int ebsd_set_match_pairs(int on);
+/* Clusters of the pair kernel that fit on the current device at once (one
+ * wave), or a negative CUDA error. */
+int ebsd_match_pair_max_clusters(void);
+
 
 int ebsd_match_topk(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
                     int64_t n_dict_pad, int64_t n_dict_valid, int64_t k_pad, int lp_dtype,

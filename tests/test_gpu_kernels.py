@@ -237,6 +237,46 @@ def test_match_launch_shapes_give_identical_results(lp, shape):
     assert torch.equal(base_v, v2)
 
 
+@pytest.mark.parametrize("lp,shape,rescore_k", [
+    ("bf16", {}, 0),
+    ("bf16", {}, 32),
+    ("fp8", {}, 0),
+    ("bf16", dict(wave_tiles=4, splits=3), 32),
+    ("bf16", dict(wave_tiles=3), 0),
+    ("fp8", dict(wave_tiles=6, splits=5), 32),
+])
+def test_match_pairs_give_identical_results(lp, shape, rescore_k):
+    """CTA-pair launches (two query tiles per tcgen05.mma.cta_group::2, half
+    of each dictionary tile staged per CTA) return exactly the one-CTA
+    kernel's top-k, raw low-precision scores included; launches with an odd
+    number of query tiles (wave_tiles=3) fall back to the one-CTA kernel."""
+    from ebsdtorch_b200 import kernels
+    from ebsdtorch_b200.engine import Searcher, SearchConfig
+
+    p, nd, nq, k = 320, 5000, 2300, 6
+    d = _rows(nd, p, 21)
+    q = d[np.arange(nq) * 2] + 0.4 * _rows(nq, p, 22)
+    dt, qt = torch.from_numpy(d).float().to(DEV), torch.from_numpy(q).float().to(DEV)
+
+    def fill_d(d0, d1, bufs):
+        kernels.prep_patterns(dt[d0:d1].reshape(d1 - d0, 1, p), bufs, subtract_mean=False)
+
+    def fill_q(q0, q1, bufs):
+        kernels.prep_patterns(qt[q0:q1].reshape(q1 - q0, 1, p), bufs, subtract_mean=False)
+
+    cfg = SearchConfig(precision=lp, rescore_k=rescore_k, **shape)
+    prev = kernels.set_match_pairs(False)
+    try:
+        base_i, base_v = Searcher(nd, nq, p, k, cfg, DEV).run(fill_d, fill_q)
+        kernels.set_match_pairs(True)
+        i2, v2 = Searcher(nd, nq, p, k, cfg, DEV).run(fill_d, fill_q)
+    finally:
+        kernels.set_match_pairs(prev)
+    torch.cuda.synchronize()
+    assert torch.equal(base_i, i2)
+    assert torch.equal(base_v, v2)
+
+
 def test_prep_patterns_integer_counts():
     """uint16 / uint8 / fp16 detector counts prepare to the same rows as the
     same values in float32."""
