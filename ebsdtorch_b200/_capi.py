@@ -37,8 +37,10 @@ SIGNATURES = {
     "ebsd_sample_master_pattern": (i32, [vp, i32, i32, vp, i64, i32, vp, vp]),
     "ebsd_avg_pool": (i32, [vp, i64, i32, i32, i32, vp, vp]),
     "ebsd_match_auto_splits": (i32, [i64, i64]),
+    "ebsd_match_auto_splits_typed": (i32, [i64, i64, i32]),
     "ebsd_set_wait_limit_ns": (i64, [i64]),
     "ebsd_set_match_pairs": (i32, [i32]),
+    "ebsd_set_match_dual": (i32, [i32]),
     "ebsd_match_pair_max_clusters": (i32, []),
     "ebsd_manhattan_topk": (i32, [vp, i64, i64, i64, vp, i64, i64, i32, i32, i32, vp, vp, i32, i32, i32, vp]),
     "ebsd_match_topk": (i32, [vp, i64, vp, i64, i64, i64, i32, vp, i32, i32, vp, vp, i32, i32, i32, vp, vp]),
@@ -140,6 +142,11 @@ def load() -> C.CDLL:
             pairs = os.environ.get("EBSD_MATCH_PAIRS")
             if pairs is not None:
                 lib.ebsd_set_match_pairs(0 if pairs.strip() in ("", "0") else 1)
+            # EBSD_MATCH_DUAL=0/1/2: two query tiles per match CTA for no, all or
+            # e4m3 (the default) launches
+            dual = os.environ.get("EBSD_MATCH_DUAL")
+            if dual is not None:
+                lib.ebsd_set_match_dual({"": 0, "0": 0, "2": 2}.get(dual.strip(), 1))
             _lib = lib
     return _lib
 

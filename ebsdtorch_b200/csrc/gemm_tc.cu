@@ -764,6 +764,274 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
+// Dual variant of the top-k match (angular ranking, 256-row dictionary
+// tiles, non-persistent): one CTA takes TWO consecutive query tiles and one
+// dictionary range, and every K step issues two M = 128, N = 256 MMAs (one
+// per query tile) against the same staged dictionary tile. Per K step a CTA
+// stages 64 KB for twice the MMA work of k_tc_gemm's 48 KB, i.e. a third
+// less L2 -> SM operand traffic per FLOP, with no operand exchange between
+// SMs (which the CTA-pair variant pays for in power).
+//   warp 0      TMA producer (A0, A1: 128 rows x 128 B; B: 256 rows x 128 B
+//               per stage; 3 stages of 64 KB)
+//   warp 1      TMEM (512 columns: query tile h accumulates in columns
+//               h * 256 ...) and the MMAs
+//   warps 2-9   epilogue: warps 2-5 read query tile 0's accumulator, 6-9
+//               tile 1's; each thread owns one query row's top-k
+// The two accumulators fill TMEM, so they are single-buffered: the MMAs of
+// dictionary tile n + 1 wait until the epilogue has read tile n (the
+// epilogue takes about 1 % of a tile's MMA time at 128^2 px).
+// ---------------------------------------------------------------------------
+constexpr int DUAL_EPI = 256;
+constexpr int DUAL_THREADS = 64 + DUAL_EPI;
+constexpr int DUAL_STAGES = 3;
+constexpr int DUAL_STAGE_BYTES = 2 * A_BYTES + 256 * BKB;
+constexpr int DUAL_SCRATCH_BYTES = 32 * DUAL_EPI * 4;
+constexpr int DUAL_BAR_BYTES = 8 * (2 * DUAL_STAGES + 2 + 1) + 16;
+constexpr int DUAL_SMEM_BYTES = 1024 + DUAL_STAGES * DUAL_STAGE_BYTES + DUAL_SCRATCH_BYTES + DUAL_BAR_BYTES;
+static_assert(DUAL_SMEM_BYTES <= 232448, "shared memory budget");
+
+template <int KIND, int KC>
+__global__ void __launch_bounds__(DUAL_THREADS, 1)
+    k_tc_gemm_dual(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                   const GemmParams p) {
+  constexpr int STAGES = DUAL_STAGES;
+  constexpr int STAGE_BYTES = DUAL_STAGE_BYTES;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t raw_s = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024u - (raw_s & 1023u)) & 1023u);
+  const uint32_t sbase = smem_u32(smem);
+  float* scratch = reinterpret_cast<float*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES + DUAL_SCRATCH_BYTES);
+  const uint32_t bar0 = smem_u32(bars);
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (STAGES + s); };
+  const uint32_t accf_bar = bar0 + 8u * (2 * STAGES);
+  const uint32_t acce_bar = bar0 + 8u * (2 * STAGES + 1);
+  const uint32_t drain_bar = bar0 + 8u * (2 * STAGES + 2);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * STAGES + 3);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // unit -> (pair of query tiles, dictionary tile range)
+  const int u = (int)blockIdx.x;
+  const int n_splits = p.splits;
+  const int pair_tile = u / n_splits;
+  const int split = u - pair_tile * n_splits;
+  const int n_begin = (int)((int64_t)split * p.n_tiles / n_splits);
+  const int n_end = (int)((int64_t)(split + 1) * p.n_tiles / n_splits);
+  const int k_iters = p.k_iters;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(full_bar(s), 1);
+      mbar_init(empty_bar(s), 1);
+    }
+    mbar_init(accf_bar, 1);
+    mbar_init(acce_bar, DUAL_EPI);
+    mbar_init(drain_bar, 1);
+    *abort_flag = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&tmA);
+    prefetch_tmap(&tmB);
+  }
+  if (warp == 1) tmem_alloc(smem_u32(tmem_slot), 512);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *reinterpret_cast<volatile uint32_t*>(tmem_slot);
+
+  const uint64_t wait_ns = p.wait_ns;
+  uint32_t prod_stage = 0, prod_phase = 0;
+  int64_t issued = 0;
+  bool any_mma = false;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      bool ok = true;
+      const int a_row = 2 * pair_tile * BM;
+      for (int n = n_begin; n < n_end && ok; ++n) {
+        for (int k = 0; k < k_iters; ++k) {
+          if (!mbar_wait(empty_bar(stage), phase ^ 1u, abort_flag, wait_ns)) {
+            ok = false;
+            break;
+          }
+          const uint32_t dst = sbase + stage * STAGE_BYTES;
+          mbar_arrive_expect_tx(full_bar(stage), STAGE_BYTES);
+          const int kx = k * (BKB / kind_elem_bytes<KIND>());
+          tma_load_2d(dst, &tmA, kx, a_row, full_bar(stage));
+          tma_load_2d(dst + A_BYTES, &tmA, kx, a_row + BM, full_bar(stage));
+          tma_load_2d(dst + 2 * A_BYTES, &tmB, kx, n * 256, full_bar(stage));
+          ++issued;
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      if (!ok) report_timeout(p, abort_flag);
+      prod_stage = stage;
+      prod_phase = phase;
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0, acc_phase = 0;
+      bool ok = true;
+      constexpr uint32_t idesc = make_idesc<KIND, 256>();
+      for (int n = n_begin; n < n_end && ok; ++n) {
+        if (!mbar_wait(acce_bar, acc_phase ^ 1u, abort_flag, wait_ns)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        for (int k = 0; k < k_iters; ++k) {
+          if (!mbar_wait(full_bar(stage), phase, abort_flag, wait_ns)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a_addr = sbase + stage * STAGE_BYTES;
+          const uint32_t b_addr = a_addr + 2 * A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < BKB / 32; ++kk) {
+            const uint64_t bdesc = smem_desc_sw128(b_addr + kk * 32);
+            const uint32_t accum = (k | kk) != 0 ? 1u : 0u;
+            tc_mma<KIND>(tmem_base, smem_desc_sw128(a_addr + kk * 32), bdesc, idesc, accum);
+            tc_mma<KIND>(tmem_base + 256u, smem_desc_sw128(a_addr + A_BYTES + kk * 32), bdesc, idesc, accum);
+          }
+          any_mma = true;
+          tc_commit(empty_bar(stage));
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) break;
+        tc_commit(accf_bar);
+        acc_phase ^= 1u;
+      }
+      if (!ok) report_timeout(p, abort_flag);
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue ----------------
+    const int h = (warp - 2) >> 2;        // query tile of the pair
+    const int wq = warp & 3;              // TMEM lane quarter this warp may access
+    const int etid = threadIdx.x - 64;    // 0..255, scratch column
+    const int row = wq * 32 + lane;
+    const uint32_t lane_addr = (uint32_t)(wq * 32) << 16;
+    const int m_tile = 2 * pair_tile + h;
+    float bv[KC];
+    int bi[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+      bv[j] = -INFINITY;
+      bi[j] = -1;
+    }
+    uint32_t acc_phase = 0;
+    bool ok = true;
+    for (int n = n_begin; n < n_end; ++n) {
+      bool got = mbar_wait_sleep(accf_bar, acc_phase, abort_flag, wait_ns);
+      got = __all_sync(0xffffffffu, got);
+      if (!got) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int64_t tile_col = (int64_t)n * 256;
+#pragma unroll 1
+      for (int c = 0; c < 256 / 32; ++c) {
+        __syncwarp();
+        float v[32];
+        tmem_ld32(tmem_base + lane_addr + (uint32_t)(h * 256 + c * 32), v);
+        const int64_t col0 = tile_col + c * 32;
+        uint32_t mask = 0;
+        const float thr = bv[KC - 1];
+        if (col0 + 32 <= p.n_valid) {
+          if (p.col_scale) {
+            const float4* cs = reinterpret_cast<const float4*>(p.col_scale + col0);
+#pragma unroll
+            for (int j4 = 0; j4 < 8; ++j4) {
+              const float4 s4 = __ldg(cs + j4);
+              v[4 * j4 + 0] *= s4.x;
+              v[4 * j4 + 1] *= s4.y;
+              v[4 * j4 + 2] *= s4.z;
+              v[4 * j4 + 3] *= s4.w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const bool valid = col0 + j < p.n_valid;
+            const float sc = (valid && p.col_scale) ? __ldg(p.col_scale + col0 + j) : 1.0f;
+            v[j] = valid ? v[j] * sc : -INFINITY;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) mask |= (v[j] > thr) ? (1u << j) : 0u;
+        if (mask) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) scratch[j * DUAL_EPI + etid] = v[j];
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const float sc = scratch[j * DUAL_EPI + etid];
+            if (sc > bv[KC - 1]) topk_insert<KC>(bv, bi, sc, (int)(col0 + j) + p.index_base);
+          }
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(acce_bar);
+      acc_phase ^= 1u;
+    }
+    if (ok && m_tile < p.m_tiles) {
+      const int64_t q = (int64_t)m_tile * BM + row;
+      const int64_t base = (q * p.part_slots + p.slot_base + split) * KC;
+#pragma unroll
+      for (int j = 0; j < KC; ++j) {
+        p.part_val[base + j] = bv[j];
+        p.part_idx[base + j] = bi[j];
+      }
+    }
+    if (!ok && lane == 0) report_timeout(p, abort_flag);
+  }
+
+  // As in k_tc_gemm: after a give-up, let this CTA's copies and MMAs finish
+  // before shared memory and TMEM are released.
+  __syncthreads();
+  if (*abort_flag) {
+    volatile int never = 0;
+    if (warp == 0 && lane == 0) {
+      const int64_t inflight = issued < STAGES ? issued : (int64_t)STAGES;
+      uint32_t s = prod_stage, ph = prod_phase;
+      for (int64_t i = 0; i < inflight; ++i) {
+        if (s == 0) {
+          s = STAGES - 1;
+          ph ^= 1u;
+        } else {
+          --s;
+        }
+        mbar_wait(full_bar(s), ph, &never);
+      }
+    } else if (warp == 1 && lane == 0 && any_mma) {
+      tc_commit(drain_bar);
+      mbar_wait(drain_bar, 0, &never);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 
@@ -888,6 +1156,53 @@ static int launch_pair(int kc, const CUtensorMap& a, const CUtensorMap& b, const
 // Whether eligible top-k matches run as CTA pairs (ebsd_set_match_pairs).
 static std::atomic<int> g_match_pairs{0};
 
+template <int KIND, int KC>
+static int launch_dual_kc(const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p_in, int grid,
+                          cudaStream_t s) {
+  auto kern = k_tc_gemm_dual<KIND, KC>;
+  EBSD_CUDA_CHECK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, DUAL_SMEM_BYTES));
+  GemmParams p = p_in;
+  p.wait_ns = wait_limit_ns();
+  kern<<<grid, DUAL_THREADS, DUAL_SMEM_BYTES, s>>>(a, b, p);
+  EBSD_LAUNCH_CHECK();
+  return 0;
+}
+
+template <int KIND>
+static int launch_dual(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p, int grid,
+                       cudaStream_t s) {
+  switch (kc) {
+    case 1: return launch_dual_kc<KIND, 1>(a, b, p, grid, s);
+    case 2: return launch_dual_kc<KIND, 2>(a, b, p, grid, s);
+    case 4: return launch_dual_kc<KIND, 4>(a, b, p, grid, s);
+    case 8: return launch_dual_kc<KIND, 8>(a, b, p, grid, s);
+    case 16: return launch_dual_kc<KIND, 16>(a, b, p, grid, s);
+    case 32: return launch_dual_kc<KIND, 32>(a, b, p, grid, s);
+    case 64: return launch_dual_kc<KIND, 64>(a, b, p, grid, s);
+  }
+  set_error("n_cand %d not in {1,2,4,8,16,32,64}", kc);
+  return EBSD_ERR_ARG;
+}
+
+// Which eligible top-k matches take two query tiles per CTA
+// (ebsd_set_match_dual): 0 none, 1 all, 2 those of e4m3 rows (default).
+// Measured on a B200 under the 1 kW power cap (full bench, two alternating
+// pairs of runs): e4m3 190,500 vs 182,000 patterns/s; bf16 within the noise
+// (about 8 % more work per clock, about 8 % less clock).
+static std::atomic<int> g_match_dual{2};
+
+// The variant an eligible launch (256-row tiles, angular ranking, not
+// persistent) of m_tiles query tiles of lp_dtype rows runs: 1 CTA pairs, 2
+// two query tiles per CTA, 0 the one-tile kernel (always for an odd tile
+// count).
+static int match_variant(int64_t m_tiles, int lp_dtype) {
+  if (m_tiles % 2) return 0;
+  if (g_match_pairs.load(std::memory_order_relaxed)) return 1;
+  const int dual = g_match_dual.load(std::memory_order_relaxed);
+  if (dual == 1 || (dual == 2 && lp_dtype == EBSD_DT_E4M3)) return 2;
+  return 0;
+}
+
 template <int KIND, int BN, bool PERSIST, bool BIAS = false>
 static int launch_topk(int kc, const CUtensorMap& a, const CUtensorMap& b, const GemmParams& p,
                        int grid, cudaStream_t s) {
@@ -951,6 +1266,11 @@ extern "C" int ebsd_set_match_pairs(int on) {
   return g_match_pairs.exchange(on ? 1 : 0);
 }
 
+extern "C" int ebsd_set_match_dual(int mode) {
+  if (mode < 0) return g_match_dual.load();
+  return g_match_dual.exchange(mode == 0 ? 0 : mode == 2 ? 2 : 1);
+}
+
 extern "C" int ebsd_match_pair_max_clusters(void) {
   // every instantiation has the same block, cluster and shared-memory size
   auto kern = k_tc_gemm_pair<0, 32>;
@@ -971,19 +1291,25 @@ extern "C" int ebsd_match_pair_max_clusters(void) {
   return n;
 }
 
-extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
+extern "C" int ebsd_match_auto_splits_typed(int64_t n_queries_pad, int64_t n_dict_pad, int lp_dtype) {
   // One wave: query tiles x dictionary ranges ~= number of SMs, so all units
   // start and finish together. Measured on B200 at 128^2 px x 328,720 rows:
   // one-wave shapes with 16-37 query tiles x 4-9 ranges run at ~1.26 PFLOP/s
   // and ~1.3 GHz under the power cap (18 x 8 fastest: its query tiles stay
   // in L2); multi-wave or 1-range shapes that keep many more operand tiles in
   // flight settle at 0.68-1.1 PFLOP/s.
+  // (with two query tiles per CTA, the CTAs of a range are half as many)
   const int64_t m_tiles = std::max<int64_t>(1, n_queries_pad / BM);
   const int64_t n_tiles = std::max<int64_t>(1, n_dict_pad / 256);
   const int64_t sms = device_sm_count();
-  int64_t splits = std::max<int64_t>(1, sms / m_tiles);
+  const int64_t ctas_per_range = match_variant(m_tiles, lp_dtype) == 2 ? m_tiles / 2 : m_tiles;
+  int64_t splits = std::max<int64_t>(1, sms / ctas_per_range);
   splits = std::min(splits, n_tiles);
   return (int)splits;
+}
+
+extern "C" int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad) {
+  return ebsd_match_auto_splits_typed(n_queries_pad, n_dict_pad, EBSD_DT_BF16);
 }
 
 extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_pad, const void* dict_lp,
@@ -1003,7 +1329,7 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   EBSD_ARG_CHECK(!col_bias || ((uintptr_t)col_bias & 15) == 0, "col_bias must be 16-byte aligned");
   EBSD_ARG_CHECK(!col_bias == !row_scale, "col_bias and row_scale must be given together");
   const int n_tiles = (int)(n_dict_pad / tile_n);
-  if (splits <= 0) splits = ebsd_match_auto_splits(n_queries_pad, n_dict_pad);
+  if (splits <= 0) splits = ebsd_match_auto_splits_typed(n_queries_pad, n_dict_pad, lp_dtype);
   splits = std::min(splits, n_tiles);
   EBSD_ARG_CHECK(slot_base >= 0 && slot_base + splits <= part_slots,
                  "part_slots (%d) < slot_base (%d) + splits (%d)", part_slots, slot_base, splits);
@@ -1014,8 +1340,8 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
   // the angular ranking and an even number of query tiles, one cluster of
   // two CTAs takes two query tiles and a dictionary range.
   const bool persist = max_ctas > 0 && max_ctas < m_tiles * splits;
-  const bool pair = g_match_pairs.load(std::memory_order_relaxed) && !persist && tile_n == 256 && !col_bias &&
-                    m_tiles % 2 == 0;
+  const int variant = (!persist && tile_n == 256 && !col_bias) ? match_variant(m_tiles, lp_dtype) : 0;
+  const bool pair = variant == 1;
   CUtensorMap ta, tb;
   if (int rc = make_tmap(&ta, queries_lp, lp_dtype, n_queries_pad, k_pad, BM)) return rc;
   if (int rc = make_tmap(&tb, dict_lp, lp_dtype, n_dict_pad, k_pad, pair ? tile_n / 2 : tile_n)) return rc;
@@ -1040,6 +1366,11 @@ extern "C" int ebsd_match_topk_tiled(const void* queries_lp, int64_t n_queries_p
     p.units = (int)(m_tiles / 2 * splits);
     return lp_dtype == EBSD_DT_BF16 ? launch_pair<0>(n_cand, ta, tb, p, 2 * p.units, s)
                                     : launch_pair<1>(n_cand, ta, tb, p, 2 * p.units, s);
+  }
+  if (variant == 2) {
+    p.units = (int)(m_tiles / 2 * splits);
+    return lp_dtype == EBSD_DT_BF16 ? launch_dual<0>(n_cand, ta, tb, p, p.units, s)
+                                    : launch_dual<1>(n_cand, ta, tb, p, p.units, s);
   }
   const int grid = persist ? max_ctas : p.units;
   return lp_dtype == EBSD_DT_BF16 ? launch_topk_shape<0>(n_cand, tile_n, persist, ta, tb, p, grid, s)

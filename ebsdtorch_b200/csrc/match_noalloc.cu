@@ -74,7 +74,7 @@ extern "C" int ebsd_match_topk_noalloc(const void* queries_lp, int64_t n_queries
                  "the fixed scratch holds %zu (at most %zu padded queries for this k)",
                  (long long)n_queries_pad, n_cand, (size_t)n_queries_pad * per_query_slot, cap,
                  cap / per_query_slot);
-  int splits = std::min(ebsd_match_auto_splits(n_queries_pad, n_dict_pad), 4096 / n_cand);
+  int splits = std::min(ebsd_match_auto_splits_typed(n_queries_pad, n_dict_pad, lp_dtype), 4096 / n_cand);
   while (splits > 1 && (size_t)n_queries_pad * splits * per_query_slot > cap) --splits;
 
   void* base = nullptr;

@@ -219,12 +219,9 @@ def wave_query_tiles(device, row_bytes: int = 0) -> int:
     sms = props.multi_processor_count
     l2 = getattr(props, "L2_cache_size", 0) or (126 << 20)
     quarter = max(1, sms // 4)
-    tiles = quarter if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2) // 3 else max(1, sms // 8)
-    # CTA-pair launches take query tiles two at a time (an odd count runs the
-    # one-CTA kernel)
-    if tiles > 1 and tiles % 2 and kernels.match_pairs():
-        tiles -= 1
-    return tiles
+    if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2) // 3:
+        return quarter
+    return max(1, sms // 8)
 
 
 def default_budget(device) -> int:
@@ -321,7 +318,12 @@ class Searcher:
         else:
             # launches of one wave of (query tile, dictionary range) units
             row_bytes = q_rows.k_pad * q_rows.lp.element_size()
-            qm, max_ctas = (cfg.wave_tiles or wave_query_tiles(dev, row_bytes)) * TILE_Q, 0
+            tiles = cfg.wave_tiles or wave_query_tiles(dev, row_bytes)
+            # launch variants that take query tiles two at a time get an even
+            # count (an odd one runs the one-tile kernel)
+            if not cfg.wave_tiles and tiles > 1 and tiles % 2 and kernels.takes_tile_pairs(self.lp_dtype):
+                tiles -= 1
+            qm, max_ctas = tiles * TILE_Q, 0
             max_splits = min(cfg.splits or max(1, sms), split_cap)
         part_val = torch.empty((min(qm, round_up(qc, TILE_Q)) * max_splits * self.n_cand,), dtype=torch.float32,
                                device=dev)
@@ -360,7 +362,7 @@ class Searcher:
                     ns = s1 - s0
                     ns_pad = round_up(ns, TILE_Q)
                     tile = cfg.tile_n or 256
-                    auto = max_splits if cfg.persistent else kernels.auto_splits(ns_pad, nd_pad)
+                    auto = max_splits if cfg.persistent else kernels.auto_splits(ns_pad, nd_pad, self.lp_dtype)
                     splits = max(1, min(cfg.splits or auto, max_splits, split_cap, nd_pad // tile))
                     timers = MATCH_TIMERS
                     if timers is not None:

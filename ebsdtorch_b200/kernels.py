@@ -169,8 +169,28 @@ def match_pairs() -> bool:
     return bool(_capi.load().ebsd_set_match_pairs(-1))
 
 
-def auto_splits(n_queries_pad: int, n_dict_pad: int) -> int:
-    return int(_capi.load().ebsd_match_auto_splits(n_queries_pad, n_dict_pad))
+def set_match_dual(mode) -> int:
+    """Which eligible top-k matches that follow take two query tiles per CTA
+    (two MMAs per K step share one staged dictionary tile): 0 / False none,
+    1 / True all, 2 those of e4m3 rows (the default). Returns the previous
+    mode."""
+    return int(_capi.load().ebsd_set_match_dual(int(mode)))
+
+
+def match_dual() -> int:
+    """The current two-tile mode (see set_match_dual)."""
+    return int(_capi.load().ebsd_set_match_dual(-1))
+
+
+def takes_tile_pairs(lp_dtype: int) -> bool:
+    """Whether match launches of lp_dtype rows with an even number of query
+    tiles run a variant that takes the tiles two at a time."""
+    mode = match_dual()
+    return match_pairs() or mode == 1 or (mode == 2 and lp_dtype == DT_E4M3)
+
+
+def auto_splits(n_queries_pad: int, n_dict_pad: int, lp_dtype: int = DT_BF16) -> int:
+    return int(_capi.load().ebsd_match_auto_splits_typed(n_queries_pad, n_dict_pad, lp_dtype))
 
 
 def match_topk(q_lp, d_lp, n_dict_valid: int, lp_dtype: int, col_scale, n_cand: int, splits: int,

@@ -171,6 +171,10 @@ int ebsd_avg_pool(const float* in, int64_t n, int height, int width, int binning
  *   part_val/part_idx[(q * part_slots + slot_base + range) * n_cand + j].
  * part_slots >= slot_base + splits. */
 int ebsd_match_auto_splits(int64_t n_queries_pad, int64_t n_dict_pad);
+/* The automatic number of dictionary ranges for rows of lp_dtype (the launch
+ * variant, and so the plan, may depend on the element type: see
+ * ebsd_set_match_dual); ebsd_match_auto_splits plans for bf16 rows. */
+int ebsd_match_auto_splits_typed(int64_t n_queries_pad, int64_t n_dict_pad, int lp_dtype);
 
 /* No counterpart in the reference (which has no device-side waits): sets the
  * limit, in nanoseconds, of every bounded wait inside the tensor-core kernels
@@ -190,6 +194,15 @@ int64_t ebsd_set_wait_limit_ns(int64_t ns);
  * and the partial-result layout are the same as the one-CTA kernel's.
  * Returns the previous setting (0 by default); on < 0 only returns it. */
 int ebsd_set_match_pairs(int on);
+/* No counterpart in the reference: which eligible top-k matches that follow
+ * (as for ebsd_set_match_pairs) take TWO query tiles per CTA: two M = 128
+ * MMAs per K step share one staged 256-row dictionary tile, a third less
+ * operand traffic from L2 per FLOP. mode 0: none; 1: all; 2 (default): those
+ * of e4m3 rows. ebsd_match_auto_splits_typed then plans twice the dictionary
+ * ranges. Results and the partial-result layout are the same as the one-tile
+ * kernel's. CTA pairs, when on, take precedence. Returns the previous mode;
+ * mode < 0 only returns it. */
+int ebsd_set_match_dual(int mode);
 /* Clusters of the pair kernel that fit on the current device at once (one
  * wave), or a negative CUDA error. */
 int ebsd_match_pair_max_clusters(void);

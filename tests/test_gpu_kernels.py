@@ -237,6 +237,7 @@ def test_match_launch_shapes_give_identical_results(lp, shape):
     assert torch.equal(base_v, v2)
 
 
+@pytest.mark.parametrize("variant", ["pairs", "dual"])
 @pytest.mark.parametrize("lp,shape,rescore_k", [
     ("bf16", {}, 0),
     ("bf16", {}, 32),
@@ -245,11 +246,13 @@ def test_match_launch_shapes_give_identical_results(lp, shape):
     ("bf16", dict(wave_tiles=3), 0),
     ("fp8", dict(wave_tiles=6, splits=5), 32),
 ])
-def test_match_pairs_give_identical_results(lp, shape, rescore_k):
+def test_match_pairs_give_identical_results(lp, shape, rescore_k, variant):
     """CTA-pair launches (two query tiles per tcgen05.mma.cta_group::2, half
-    of each dictionary tile staged per CTA) return exactly the one-CTA
-    kernel's top-k, raw low-precision scores included; launches with an odd
-    number of query tiles (wave_tiles=3) fall back to the one-CTA kernel."""
+    of each dictionary tile staged per CTA) and two-tile launches (two MMAs
+    per K step sharing one staged dictionary tile) return exactly the
+    one-tile kernel's top-k, raw low-precision scores included; launches with
+    an odd number of query tiles (wave_tiles=3) fall back to the one-tile
+    kernel."""
     from ebsdtorch_b200 import kernels
     from ebsdtorch_b200.engine import Searcher, SearchConfig
 
@@ -265,13 +268,15 @@ def test_match_pairs_give_identical_results(lp, shape, rescore_k):
         kernels.prep_patterns(qt[q0:q1].reshape(q1 - q0, 1, p), bufs, subtract_mean=False)
 
     cfg = SearchConfig(precision=lp, rescore_k=rescore_k, **shape)
-    prev = kernels.set_match_pairs(False)
+    switch = kernels.set_match_pairs if variant == "pairs" else kernels.set_match_dual
+    prev = (kernels.set_match_pairs(False), kernels.set_match_dual(False))
     try:
         base_i, base_v = Searcher(nd, nq, p, k, cfg, DEV).run(fill_d, fill_q)
-        kernels.set_match_pairs(True)
+        switch(True)
         i2, v2 = Searcher(nd, nq, p, k, cfg, DEV).run(fill_d, fill_q)
     finally:
-        kernels.set_match_pairs(prev)
+        kernels.set_match_pairs(prev[0])
+        kernels.set_match_dual(prev[1])
     torch.cuda.synchronize()
     assert torch.equal(base_i, i2)
     assert torch.equal(base_v, v2)

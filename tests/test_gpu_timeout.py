@@ -34,10 +34,25 @@ def _match(lib, q, d, col_scale, k, status):
     return idx, val
 
 
-def test_wait_limit_runs_out_and_the_next_call_succeeds():
-    from ebsdtorch_b200 import _capi
+@pytest.mark.parametrize("variant", ["one_tile", "pairs", "dual"])
+def test_wait_limit_runs_out_and_the_next_call_succeeds(variant):
+    """For each match kernel: the one-tile kernel, CTA pairs (whose even CTA
+    drains both CTAs' copies before the cluster barrier) and two query tiles
+    per CTA."""
+    from ebsdtorch_b200 import _capi, kernels
 
     lib = _capi.load()
+    prev_modes = (kernels.set_match_pairs(variant == "pairs"), kernels.set_match_dual(variant == "dual"))
+    try:
+        _run_timeout_case(lib)
+    finally:
+        kernels.set_match_pairs(prev_modes[0])
+        kernels.set_match_dual(prev_modes[1])
+
+
+def _run_timeout_case(lib):
+    from ebsdtorch_b200 import _capi
+
     g = torch.Generator(device=DEV).manual_seed(3)
     # 256 queries x 16,384 rows of 16,384 bf16 values: every accumulator
     # takes far longer than a wait's spin, so a 1 ns limit always runs out
