@@ -29,6 +29,9 @@ q = synthetic.random_quaternions(300, 2).to("cuda")
 pats = synthetic.synthetic_patterns(mp_t, geom, q, mean_counts=200.0, seed=3)
 exp = ExperimentPatterns(pats)
 dictionary_index_orientations(mp, geom, exp, dictionary_resolution_degrees=4.0, top_k_matches=4)
+# e4m3 rows, two 128-row query tiles: the two-query-tile match kernel
+exp8 = ExperimentPatterns(pats[:256].clone())
+dictionary_index_orientations(mp, geom, exp8, dictionary_resolution_degrees=4.0, top_k_matches=4, precision="fp8")
 spatial_fft_pc_fitter(mp, pats[:4].reshape(4, 1, 32, 32).clone(), pc_x_min=0.4, pc_x_max=0.6, pc_y_min=0.4,
                       pc_y_max=0.6, pc_z_min=0.55, pc_z_max=0.65, pc_z_steps=2, dictionary_resolution_deg=8.0)
 torch.cuda.synchronize()
