@@ -158,3 +158,30 @@ def test_check_build_query_without_checks_needs_no_gpu():
     if _capi.LIB_PATH.endswith("_check.so"):
         return
     assert _capi.debug_check() == (-1, "")
+
+
+def test_match_variant_switches_need_no_gpu():
+    """The match-variant switches: CTA pairs off and two query tiles per CTA
+    for e4m3 rows by default; a negative argument only reads the mode; the
+    setters return the previous mode."""
+    from ebsdtorch_b200 import kernels
+
+    lib = _capi.load()
+    pairs0, dual0 = lib.ebsd_set_match_pairs(-1), lib.ebsd_set_match_dual(-1)
+    if os.environ.get("EBSD_MATCH_PAIRS") is None:
+        assert pairs0 == 0
+    if os.environ.get("EBSD_MATCH_DUAL") is None:
+        assert dual0 == 2
+    try:
+        assert lib.ebsd_set_match_pairs(1) == pairs0 and lib.ebsd_set_match_pairs(-1) == 1
+        assert kernels.takes_tile_pairs(_capi.DT_BF16) and kernels.takes_tile_pairs(_capi.DT_E4M3)
+        lib.ebsd_set_match_pairs(0)
+        for mode, bf16, e4m3 in ((0, False, False), (1, True, True), (2, False, True)):
+            kernels.set_match_dual(mode)
+            assert kernels.match_dual() == mode
+            assert kernels.takes_tile_pairs(_capi.DT_BF16) == bf16
+            assert kernels.takes_tile_pairs(_capi.DT_E4M3) == e4m3
+        assert kernels.set_match_dual(True) == 2 and kernels.match_dual() == 1
+    finally:
+        lib.ebsd_set_match_pairs(pairs0)
+        lib.ebsd_set_match_dual(dual0)
