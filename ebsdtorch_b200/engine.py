@@ -216,12 +216,26 @@ def wave_query_tiles(device, row_bytes: int = 0) -> int:
     (16 KB, 76 MB for 37 tiles) were ~2 % slower with 18 tiles (no traffic
     to save). row_bytes 0 (unknown) takes the smaller count."""
     props = torch.cuda.get_device_properties(device)
-    sms = props.multi_processor_count
-    l2 = getattr(props, "L2_cache_size", 0) or (126 << 20)
+    return wave_tiles_for(props.multi_processor_count, getattr(props, "L2_cache_size", 0) or (126 << 20), row_bytes)
+
+
+def wave_tiles_for(sms: int, l2_bytes: int, row_bytes: int = 0, tile_pairs: bool = False) -> int:
+    """The rule of wave_query_tiles for a device of `sms` SMs and `l2_bytes`
+    of L2. tile_pairs: the launch variant takes query tiles two at a time
+    (two-tile CTAs or CTA pairs), so an odd count is rounded down to an even
+    one (an odd count runs the one-tile kernel)."""
     quarter = max(1, sms // 4)
-    if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2) // 3:
-        return quarter
-    return max(1, sms // 8)
+    if row_bytes > 0 and quarter * TILE_Q * row_bytes <= (2 * l2_bytes) // 3:
+        tiles = quarter
+    else:
+        tiles = max(1, sms // 8)
+    return even_tiles(tiles, tile_pairs)
+
+
+def even_tiles(tiles: int, tile_pairs: bool) -> int:
+    """An odd query-tile count rounded down to an even one for launch
+    variants that take the tiles two at a time."""
+    return tiles - 1 if tile_pairs and tiles > 1 and tiles % 2 else tiles
 
 
 def default_budget(device) -> int:
@@ -318,11 +332,10 @@ class Searcher:
         else:
             # launches of one wave of (query tile, dictionary range) units
             row_bytes = q_rows.k_pad * q_rows.lp.element_size()
-            tiles = cfg.wave_tiles or wave_query_tiles(dev, row_bytes)
             # launch variants that take query tiles two at a time get an even
             # count (an odd one runs the one-tile kernel)
-            if not cfg.wave_tiles and tiles > 1 and tiles % 2 and kernels.takes_tile_pairs(self.lp_dtype):
-                tiles -= 1
+            tiles = cfg.wave_tiles or even_tiles(wave_query_tiles(dev, row_bytes),
+                                                 kernels.takes_tile_pairs(self.lp_dtype))
             qm, max_ctas = tiles * TILE_Q, 0
             max_splits = min(cfg.splits or max(1, sms), split_cap)
         part_val = torch.empty((min(qm, round_up(qc, TILE_Q)) * max_splits * self.n_cand,), dtype=torch.float32,

@@ -78,3 +78,18 @@ def test_match_traffic_model_reproduces_its_captures():
     # the 18-query-tile launches read each dictionary row about twice
     operands = (328960 + bench.MATCH_WAVE_QUERIES) * 16384 * 2
     assert 1.5 * operands < bench.match_traffic_estimate(328720) < 2.5 * operands
+
+
+def test_wave_shape_rule():
+    """One-wave query-tile counts on a 148-SM, 126 MB-L2 device: bf16 rows of
+    128^2 px (32 KB) take 18 tiles, e4m3 rows (16 KB) 37, or 36 when the
+    launch takes query tiles two at a time; unknown row sizes take 18."""
+    from ebsdtorch_b200.engine import even_tiles, wave_tiles_for
+
+    l2 = 126 << 20
+    assert wave_tiles_for(148, l2, 32768) == 18
+    assert wave_tiles_for(148, l2, 16384) == 37
+    assert wave_tiles_for(148, l2, 16384, tile_pairs=True) == 36
+    assert wave_tiles_for(148, l2, 32768, tile_pairs=True) == 18
+    assert wave_tiles_for(148, l2) == 18
+    assert even_tiles(1, True) == 1 and even_tiles(7, False) == 7 and even_tiles(7, True) == 6
